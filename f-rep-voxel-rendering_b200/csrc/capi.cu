@@ -1,0 +1,558 @@
+// C-ABI of the library (include/frep.h): tapes, device contexts, trees,
+// voxelization and rendering. Host code only; kernels live in voxelizer.cu and
+// raytracer.cu.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "device_common.cuh"
+#include "frep.h"
+#include "kernels.h"
+#include "tape_compiler.h"
+
+using frep::CompiledTape;
+
+namespace {
+
+thread_local std::string g_error;
+
+frep_status fail(frep_status s, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_error = buf;
+    return s;
+}
+
+frep_status cuda_fail(cudaError_t e, const char* what) {
+    return fail(FREP_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define FREP_CUDA(call)                                              \
+    do {                                                             \
+        cudaError_t e_ = (call);                                     \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call);          \
+    } while (0)
+
+uint64_t align_up(uint64_t v, uint64_t a) { return (v + a - 1) / a * a; }
+
+}  // namespace
+
+struct frep_tape {
+    CompiledTape ct;
+    std::vector<uint64_t> record;  // [n_instr][instrs...] padded to 16 words
+    void build_record() {
+        record.assign(align_up(1 + ct.instrs.size(), frep::dev::TAPE_ALIGN_WORDS), 0);
+        record[0] = ct.instrs.size();
+        std::memcpy(&record[1], ct.instrs.data(), ct.instrs.size() * 8);
+    }
+};
+
+struct frep_ctx {
+    int device = 0;
+    uint64_t budget = 0;
+    uint64_t used = 0;
+    int sm_count = 0;
+};
+
+struct frep_tree {
+    frep_ctx* ctx = nullptr;
+    frep_grid grid{};
+    frep_voxelize_opts opts{};
+    float cell_size[FREP_MAX_LEVELS] = {};
+    uint32_t node_size[FREP_MAX_LEVELS] = {};
+    frep::dev::TreeHeader* hdr = nullptr;
+    uint32_t* nodes = nullptr;
+    uint64_t* tapes = nullptr;
+    uint64_t node_cap = 0, tape_cap = 0;
+    uint32_t* keep = nullptr;
+    uint64_t keep_words = 0;
+    uint64_t bytes = 0;
+    // staging for the root tape upload
+    uint64_t* staging = nullptr;
+    uint64_t staging_words = 0;
+    cudaEvent_t upload_done = nullptr;
+    // the root tape of the last voxelization
+    uint32_t n_slots = 4, mm_cap = 0, root_n = 0, root_words = 0;
+    bool plan_valid = false;
+    uint32_t plan_slots = 0, plan_mm = 0, plan_round = 0;
+    frep::LevelPlan plan{};
+    cudaStream_t stream = nullptr;
+    bool voxelized = false;
+    bool profile = false;
+    cudaEvent_t ev[FREP_MAX_LEVELS + 1] = {};
+};
+
+extern "C" {
+
+const char* frep_last_error(void) { return g_error.c_str(); }
+const char* frep_version(void) { return "frep-b200 0.1 (sm_100a)"; }
+
+// ---- tapes -------------------------------------------------------------------
+
+frep_status frep_tape_compile(const frep_dag* dag, frep_tape** out) {
+    if (!dag || !out || !dag->ops || !dag->in0 || !dag->in1 || !dag->consts)
+        return fail(FREP_ERR_INVALID_ARG, "frep_tape_compile: null argument");
+    std::vector<frep::DagNode> nodes(dag->n_nodes);
+    for (uint32_t i = 0; i < dag->n_nodes; i++)
+        nodes[i] = {dag->ops[i], dag->in0[i], dag->in1[i], dag->consts[i]};
+    auto* t = new frep_tape();
+    std::string err = frep::compile_tape(nodes.data(), dag->n_nodes, dag->root, &t->ct);
+    if (!err.empty()) {
+        delete t;
+        return fail(FREP_ERR_COMPILE, "frep_tape_compile: %s", err.c_str());
+    }
+    t->build_record();
+    *out = t;
+    return FREP_OK;
+}
+
+frep_status frep_tape_from_reference(const uint32_t* instrs, uint32_t n_instr, const float* consts,
+                                     uint32_t n_consts, frep_tape** out) {
+    if (!instrs || !out || (n_consts && !consts))
+        return fail(FREP_ERR_INVALID_ARG, "frep_tape_from_reference: null argument");
+    auto* t = new frep_tape();
+    std::string err = frep::import_reference_tape(instrs, n_instr, consts, n_consts, &t->ct);
+    if (!err.empty()) {
+        delete t;
+        return fail(FREP_ERR_INVALID_ARG, "frep_tape_from_reference: %s", err.c_str());
+    }
+    t->build_record();
+    *out = t;
+    return FREP_OK;
+}
+
+frep_status frep_tape_get_info(const frep_tape* tape, frep_tape_info* info) {
+    if (!tape || !info) return fail(FREP_ERR_INVALID_ARG, "frep_tape_get_info: null argument");
+    info->n_instr = (uint32_t)tape->ct.instrs.size();
+    info->n_slots = tape->ct.n_slots;
+    info->n_consts = (uint32_t)tape->ct.const_pool.size();
+    info->n_minmax = tape->ct.n_minmax;
+    info->fits_reference = tape->ct.fits_reference ? 1u : 0u;
+    info->uses_time = tape->ct.uses_time ? 1u : 0u;
+    return FREP_OK;
+}
+
+frep_status frep_tape_get_instrs(const frep_tape* tape, uint64_t* out, uint32_t cap) {
+    if (!tape || !out) return fail(FREP_ERR_INVALID_ARG, "frep_tape_get_instrs: null argument");
+    if (cap < tape->ct.instrs.size()) return fail(FREP_ERR_INVALID_ARG, "frep_tape_get_instrs: capacity too small");
+    std::memcpy(out, tape->ct.instrs.data(), tape->ct.instrs.size() * 8);
+    return FREP_OK;
+}
+
+frep_status frep_tape_get_reference(const frep_tape* tape, uint32_t* instrs, float* consts) {
+    if (!tape || !instrs || !consts) return fail(FREP_ERR_INVALID_ARG, "frep_tape_get_reference: null argument");
+    if (!tape->ct.fits_reference)
+        return fail(FREP_ERR_UNSUPPORTED, "tape has %u slots / %zu constants; the 8-bit encoding holds 256",
+                    tape->ct.n_slots, tape->ct.const_pool.size());
+    std::memcpy(instrs, tape->ct.ref_instrs.data(), tape->ct.ref_instrs.size() * 4);
+    if (!tape->ct.const_pool.empty())
+        std::memcpy(consts, tape->ct.const_pool.data(), tape->ct.const_pool.size() * 4);
+    return FREP_OK;
+}
+
+frep_status frep_tape_eval(const frep_tape* tape, const float* xyzt, uint32_t n, float* out) {
+    if (!tape || (n && (!xyzt || !out))) return fail(FREP_ERR_INVALID_ARG, "frep_tape_eval: null argument");
+    for (uint32_t i = 0; i < n; i++)
+        out[i] = frep::eval_point_host(tape->ct.instrs, tape->ct.n_slots, xyzt[4 * i], xyzt[4 * i + 1],
+                                       xyzt[4 * i + 2], xyzt[4 * i + 3]);
+    return FREP_OK;
+}
+
+void frep_tape_destroy(frep_tape* tape) { delete tape; }
+
+// ---- context -----------------------------------------------------------------
+
+frep_status frep_ctx_create(int device, uint64_t hbm_budget_bytes, frep_ctx** out) {
+    if (!out) return fail(FREP_ERR_INVALID_ARG, "frep_ctx_create: null argument");
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) return fail(FREP_ERR_CUDA, "frep_ctx_create: no CUDA device (%s)", cudaGetErrorString(e));
+    if (device < 0 || device >= n) return fail(FREP_ERR_INVALID_ARG, "frep_ctx_create: device %d of %d", device, n);
+    FREP_CUDA(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    FREP_CUDA(cudaGetDeviceProperties(&prop, device));
+    if (prop.major < 10) return fail(FREP_ERR_UNSUPPORTED, "frep_ctx_create: device is sm_%d%d; this build is sm_100a", prop.major, prop.minor);
+    size_t free_b = 0, total_b = 0;
+    FREP_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    auto* c = new frep_ctx();
+    c->device = device;
+    c->budget = hbm_budget_bytes ? hbm_budget_bytes : (uint64_t)(free_b * 0.9);
+    c->sm_count = prop.multiProcessorCount;
+    *out = c;
+    return FREP_OK;
+}
+
+void frep_ctx_destroy(frep_ctx* ctx) { delete ctx; }
+
+frep_status frep_ctx_memory(const frep_ctx* ctx, uint64_t* used, uint64_t* budget) {
+    if (!ctx) return fail(FREP_ERR_INVALID_ARG, "frep_ctx_memory: null argument");
+    if (used) *used = ctx->used;
+    if (budget) *budget = ctx->budget;
+    return FREP_OK;
+}
+
+// ---- trees -------------------------------------------------------------------
+
+static frep_status validate_grid(const frep_grid* g) {
+    if (g->levels == 0 || g->levels > FREP_MAX_LEVELS)
+        return fail(FREP_ERR_INVALID_ARG, "grid: levels must be 1..8 (got %u)", g->levels);
+    for (uint32_t l = 0; l < g->levels; l++) {
+        const uint32_t d = g->dims[l];
+        // Masks are whole 32-bit words and a warp owns one word (voxelizer.cpp:270 asserts dim^3 % 64).
+        if (d < 4 || d > 32 || d % 4 != 0)
+            return fail(FREP_ERR_INVALID_ARG, "grid: dims[%u] = %u must be a multiple of 4 in 4..32", l, d);
+    }
+    if (!(g->world_size > 0.0f)) return fail(FREP_ERR_INVALID_ARG, "grid: world_size must be > 0");
+    return FREP_OK;
+}
+
+frep_status frep_tree_create(frep_ctx* ctx, const frep_grid* grid, const frep_voxelize_opts* opts,
+                             frep_tree** out) {
+    if (!ctx || !grid || !out) return fail(FREP_ERR_INVALID_ARG, "frep_tree_create: null argument");
+    frep_status s = validate_grid(grid);
+    if (s != FREP_OK) return s;
+    FREP_CUDA(cudaSetDevice(ctx->device));
+    auto* t = new frep_tree();
+    t->ctx = ctx;
+    t->grid = *grid;
+    if (opts) t->opts = *opts;
+    else { t->opts.rounding = FREP_ROUND_OUTWARD; t->opts.shorten = 1; }
+    if (t->opts.rounding > 1) { delete t; return fail(FREP_ERR_INVALID_ARG, "opts.rounding must be 0 or 1"); }
+    // Cell sizes by successive division (voxelizer.cpp:209-216).
+    float cs = grid->world_size;
+    uint64_t dense_nodes = 1, dense_words = 0;
+    for (uint32_t l = 0; l < grid->levels; l++) {
+        cs /= (float)grid->dims[l];
+        t->cell_size[l] = cs;
+        t->node_size[l] = frep::dev::node_words(grid->dims[l], l == grid->levels - 1);
+        dense_words += dense_nodes * t->node_size[l];
+        const uint64_t d3 = (uint64_t)grid->dims[l] * grid->dims[l] * grid->dims[l];
+        dense_nodes = std::min<uint64_t>(dense_nodes * d3, 1ull << 40);
+        dense_words = std::min<uint64_t>(dense_words, 1ull << 44);
+    }
+    const uint64_t avail = ctx->budget > ctx->used ? ctx->budget - ctx->used : 0;
+    t->node_cap = t->opts.node_words ? t->opts.node_words : std::min<uint64_t>(dense_words, avail / 4 / 4);
+    t->tape_cap = t->opts.tape_words ? t->opts.tape_words : avail / 4 / 8;
+    t->tape_cap = std::min<uint64_t>(t->tape_cap, 0xFFFFFFF0ull);  // tape indices are u32
+    const uint64_t bytes = t->node_cap * 4 + t->tape_cap * 8 + sizeof(frep::dev::TreeHeader);
+    if (t->node_cap < t->node_size[0] || bytes > avail) {
+        delete t;
+        return fail(FREP_ERR_OOM, "frep_tree_create: %llu bytes requested, %llu left in the budget",
+                    (unsigned long long)bytes, (unsigned long long)avail);
+    }
+    cudaError_t e = cudaMalloc(&t->hdr, sizeof(frep::dev::TreeHeader));
+    if (e == cudaSuccess) e = cudaMalloc(&t->nodes, t->node_cap * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&t->tapes, t->tape_cap * 8);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&t->upload_done, cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(t->hdr);
+        cudaFree(t->nodes);
+        cudaFree(t->tapes);
+        delete t;
+        return fail(FREP_ERR_OOM, "frep_tree_create: cudaMalloc failed (%s)", cudaGetErrorString(e));
+    }
+    cudaMemset(t->hdr, 0, sizeof(frep::dev::TreeHeader));
+    t->bytes = bytes;
+    ctx->used += bytes;
+    *out = t;
+    return FREP_OK;
+}
+
+void frep_tree_destroy(frep_tree* t) {
+    if (!t) return;
+    cudaSetDevice(t->ctx->device);
+    if (t->stream) cudaStreamSynchronize(t->stream);
+    else cudaDeviceSynchronize();
+    cudaFree(t->hdr);
+    cudaFree(t->nodes);
+    cudaFree(t->tapes);
+    cudaFree(t->keep);
+    if (t->staging) cudaFreeHost(t->staging);
+    if (t->upload_done) cudaEventDestroy(t->upload_done);
+    for (auto& e : t->ev)
+        if (e) cudaEventDestroy(e);
+    t->ctx->used -= std::min(t->ctx->used, t->bytes);
+    delete t;
+}
+
+frep_status frep_voxelize(frep_ctx* ctx, frep_tree* tree, const frep_tape* tape, float tape_time,
+                          void* stream_ptr) {
+    if (!ctx || !tree || !tape) return fail(FREP_ERR_INVALID_ARG, "frep_voxelize: null argument");
+    if (tree->ctx != ctx) return fail(FREP_ERR_INVALID_ARG, "frep_voxelize: tree belongs to another context");
+    cudaStream_t stream = (cudaStream_t)stream_ptr;
+    FREP_CUDA(cudaSetDevice(ctx->device));
+    const uint32_t n = (uint32_t)tape->ct.instrs.size();
+    const uint32_t n_slots = std::max<uint32_t>(tape->ct.n_slots, 4);
+    const uint64_t root_words = tape->record.size();
+    if (root_words > tree->tape_cap)
+        return fail(FREP_ERR_CAPACITY, "frep_voxelize: root tape (%llu words) exceeds the tape pool", (unsigned long long)root_words);
+
+    // Launch plan for this slot / MIN-MAX count.
+    if (!tree->plan_valid || tree->plan_slots != n_slots || tree->plan_mm != tape->ct.n_minmax ||
+        tree->plan_round != tree->opts.rounding) {
+        cudaError_t e = frep::plan_levels(n_slots, tape->ct.n_minmax, (int)tree->opts.rounding, &tree->plan);
+        if (e == cudaErrorInvalidValue)
+            return fail(FREP_ERR_UNSUPPORTED, "frep_voxelize: %u slots / %u min-max ops exceed shared memory", n_slots, tape->ct.n_minmax);
+        if (e != cudaSuccess) return cuda_fail(e, "plan_levels");
+        tree->plan_valid = true;
+        tree->plan_slots = n_slots;
+        tree->plan_mm = tape->ct.n_minmax;
+        tree->plan_round = tree->opts.rounding;
+    }
+    // Per-warp keep-ballot scratch: one word per instruction of the longest tape.
+    const uint32_t keep_stride = (uint32_t)align_up(std::max<uint32_t>(n, 1), 32);
+    const uint64_t keep_words = (uint64_t)tree->plan.blocks * tree->plan.warps_per_block * keep_stride;
+    if (keep_words > tree->keep_words) {
+        if (tree->keep) {
+            cudaStreamSynchronize(tree->stream);
+            cudaFree(tree->keep);
+            tree->ctx->used -= std::min<uint64_t>(tree->ctx->used, tree->keep_words * 4);
+            tree->bytes -= tree->keep_words * 4;
+        }
+        tree->keep = nullptr;
+        tree->keep_words = 0;
+        if (ctx->used + keep_words * 4 > ctx->budget)
+            return fail(FREP_ERR_OOM, "frep_voxelize: scratch of %llu bytes exceeds the budget", (unsigned long long)keep_words * 4);
+        FREP_CUDA(cudaMalloc(&tree->keep, keep_words * 4));
+        tree->keep_words = keep_words;
+        tree->bytes += keep_words * 4;
+        ctx->used += keep_words * 4;
+    }
+    // Root tape upload through pinned staging (reused once the previous copy is done).
+    if (root_words > tree->staging_words) {
+        if (tree->staging) {
+            cudaEventSynchronize(tree->upload_done);
+            cudaFreeHost(tree->staging);
+        }
+        FREP_CUDA(cudaMallocHost(&tree->staging, root_words * 8));
+        tree->staging_words = root_words;
+    } else {
+        FREP_CUDA(cudaEventSynchronize(tree->upload_done));
+    }
+    std::memcpy(tree->staging, tape->record.data(), root_words * 8);
+    FREP_CUDA(cudaMemcpyAsync(tree->tapes, tree->staging, root_words * 8, cudaMemcpyHostToDevice, stream));
+    FREP_CUDA(cudaEventRecord(tree->upload_done, stream));
+
+    tree->n_slots = n_slots;
+    tree->mm_cap = tape->ct.n_minmax;
+    tree->root_n = n;
+    tree->root_words = (uint32_t)root_words;
+    tree->stream = stream;
+
+    cudaError_t e = frep::launch_tree_init(tree->hdr, tree->nodes, n, (uint32_t)root_words, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "tree_init_kernel");
+    const frep_grid& g = tree->grid;
+    if (tree->profile) FREP_CUDA(cudaEventRecord(tree->ev[0], stream));
+    for (uint32_t l = 0; l < g.levels; l++) {
+        const bool last = l == g.levels - 1;
+        frep::LevelArgs a{};
+        a.hdr = tree->hdr;
+        a.nodes = tree->nodes;
+        a.node_cap = tree->node_cap;
+        a.tapes = tree->tapes;
+        a.tape_cap = tree->tape_cap;
+        a.keep_scratch = tree->keep;
+        a.keep_stride = keep_stride;
+        a.level = l;
+        a.levels = g.levels;
+        a.dim = g.dims[l];
+        a.dim_next = last ? 0 : g.dims[l + 1];
+        a.node_size = tree->node_size[l];
+        a.node_size_next = last ? 1 : tree->node_size[l + 1];
+        a.cell_size = tree->cell_size[l];
+        a.low[0] = g.low_vertex[0];
+        a.low[1] = g.low_vertex[1];
+        a.low[2] = g.low_vertex[2];
+        a.tape_time = tape_time;
+        a.n_slots = n_slots;
+        a.mm_cap = std::max<uint32_t>(tape->ct.n_minmax, 1);
+        a.shorten = tree->opts.shorten;
+        e = frep::launch_level(a, tree->plan, (int)tree->opts.rounding, last, stream);
+        if (e != cudaSuccess) return cuda_fail(e, "level kernel");
+        if (tree->profile) FREP_CUDA(cudaEventRecord(tree->ev[l + 1], stream));
+    }
+    tree->voxelized = true;
+    return FREP_OK;
+}
+
+frep_status frep_tree_sync(frep_tree* tree, frep_tree_info* info) {
+    if (!tree) return fail(FREP_ERR_INVALID_ARG, "frep_tree_sync: null argument");
+    FREP_CUDA(cudaSetDevice(tree->ctx->device));
+    FREP_CUDA(cudaStreamSynchronize(tree->stream));
+    frep::dev::TreeHeader h;
+    FREP_CUDA(cudaMemcpy(&h, tree->hdr, sizeof(h), cudaMemcpyDeviceToHost));
+    frep_tree_info local;
+    frep_tree_info& I = info ? *info : local;
+    std::memset(&I, 0, sizeof(I));
+    const frep_grid& g = tree->grid;
+    I.levels = g.levels;
+    uint64_t end = 0;
+    for (uint32_t l = 0; l < g.levels; l++) {
+        I.dims[l] = g.dims[l];
+        I.node_size[l] = tree->node_size[l];
+        I.node_offset[l] = h.node_ofs[l];
+        const uint64_t cap = tree->node_cap > h.node_ofs[l] ? (tree->node_cap - h.node_ofs[l]) / tree->node_size[l] : 0;
+        I.node_count[l] = (uint32_t)std::min<uint64_t>(h.node_count[l], cap);
+        I.tape_size_sum[l] = h.tape_size_sum[l];
+        I.tape_size_max[l] = h.tape_size_max[l];
+        end = h.node_ofs[l] + (uint64_t)I.node_count[l] * tree->node_size[l];
+    }
+    I.node_words_used = end;
+    I.node_words_cap = tree->node_cap;
+    I.tape_words_used = std::min<uint64_t>(h.tape_top, tree->tape_cap);
+    I.tape_words_cap = tree->tape_cap;
+    I.overflow = h.overflow;
+    I.root_tape_words = tree->root_words;
+    if (h.overflow)
+        return fail(FREP_ERR_CAPACITY, "tree pools overflowed (flags %u: 1 = nodes, 2 = tapes)", h.overflow);
+    return FREP_OK;
+}
+
+frep_status frep_tree_set_profiling(frep_tree* tree, int enable) {
+    if (!tree) return fail(FREP_ERR_INVALID_ARG, "frep_tree_set_profiling: null argument");
+    FREP_CUDA(cudaSetDevice(tree->ctx->device));
+    if (enable && !tree->ev[0])
+        for (auto& e : tree->ev) FREP_CUDA(cudaEventCreate(&e));
+    tree->profile = enable != 0;
+    return FREP_OK;
+}
+
+frep_status frep_tree_timings(frep_tree* tree, float ms[FREP_MAX_LEVELS]) {
+    if (!tree || !ms) return fail(FREP_ERR_INVALID_ARG, "frep_tree_timings: null argument");
+    if (!tree->profile || !tree->voxelized) return fail(FREP_ERR_INVALID_ARG, "frep_tree_timings: profiling is off");
+    for (uint32_t l = 0; l < FREP_MAX_LEVELS; l++) ms[l] = 0.0f;
+    FREP_CUDA(cudaEventSynchronize(tree->ev[tree->grid.levels]));
+    for (uint32_t l = 0; l < tree->grid.levels; l++)
+        FREP_CUDA(cudaEventElapsedTime(&ms[l], tree->ev[l], tree->ev[l + 1]));
+    return FREP_OK;
+}
+
+frep_status frep_tree_work(frep_tree* tree, uint64_t* cell_instr) {
+    if (!tree || !cell_instr) return fail(FREP_ERR_INVALID_ARG, "frep_tree_work: null argument");
+    FREP_CUDA(cudaStreamSynchronize(tree->stream));
+    frep::dev::TreeHeader h;
+    FREP_CUDA(cudaMemcpy(&h, tree->hdr, sizeof(h), cudaMemcpyDeviceToHost));
+    for (int l = 0; l < FREP_MAX_LEVELS; l++) cell_instr[l] = h.cell_instr[l];
+    return FREP_OK;
+}
+
+frep_status frep_tree_copy_nodes(frep_tree* tree, uint32_t* dst, uint64_t n_words) {
+    if (!tree || !dst) return fail(FREP_ERR_INVALID_ARG, "frep_tree_copy_nodes: null argument");
+    if (n_words > tree->node_cap) return fail(FREP_ERR_INVALID_ARG, "frep_tree_copy_nodes: beyond the pool");
+    FREP_CUDA(cudaStreamSynchronize(tree->stream));
+    FREP_CUDA(cudaMemcpy(dst, tree->nodes, n_words * 4, cudaMemcpyDeviceToHost));
+    return FREP_OK;
+}
+
+frep_status frep_tree_copy_tapes(frep_tree* tree, uint64_t* dst, uint64_t n_words) {
+    if (!tree || !dst) return fail(FREP_ERR_INVALID_ARG, "frep_tree_copy_tapes: null argument");
+    if (n_words > tree->tape_cap) return fail(FREP_ERR_INVALID_ARG, "frep_tree_copy_tapes: beyond the pool");
+    FREP_CUDA(cudaStreamSynchronize(tree->stream));
+    FREP_CUDA(cudaMemcpy(dst, tree->tapes, n_words * 8, cudaMemcpyDeviceToHost));
+    return FREP_OK;
+}
+
+// ---- rendering ---------------------------------------------------------------
+
+frep_status frep_lights_default(frep_lights* L) {
+    if (!L) return fail(FREP_ERR_INVALID_ARG, "frep_lights_default: null argument");
+    std::memset(L, 0, sizeof(*L));
+    // raytracer.cpp:183-192 (directions normalised at render time)
+    L->count = 2;
+    L->direction[0][0] = -1.0f; L->direction[0][1] = -1.0f; L->direction[0][2] = -0.2f;
+    L->color[0][0] = 1.0f;
+    L->direction[1][0] = 1.0f; L->direction[1][1] = -1.0f; L->direction[1][2] = -0.2f;
+    L->color[1][2] = 2.0f;
+    L->ambient[0] = L->ambient[1] = L->ambient[2] = 0.2f;  // main.comp:136
+    L->ambient[3] = 1.0f;
+    L->background[3] = 1.0f;  // glm::vec4(black, 1)
+    L->shadow_mask = 0;
+    return FREP_OK;
+}
+
+namespace {
+struct H3 {
+    float x, y, z;
+};
+H3 cross3(H3 a, H3 b) { return {a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y}; }
+float dot3(H3 a, H3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+H3 normalize3(H3 v) {
+    const float inv = 1.0f / std::sqrt(dot3(v, v));
+    return {v.x * inv, v.y * inv, v.z * inv};
+}
+}  // namespace
+
+frep_status frep_render(frep_ctx* ctx, const frep_tree* tree, const frep_camera* cam,
+                        const frep_lights* lights, float tape_time, const frep_image* out,
+                        void* stream_ptr) {
+    if (!ctx || !tree || !cam || !lights || !out) return fail(FREP_ERR_INVALID_ARG, "frep_render: null argument");
+    if (!tree->voxelized) return fail(FREP_ERR_INVALID_ARG, "frep_render: the tree has not been voxelized");
+    if (cam->width == 0 || cam->height == 0 || cam->projection > 1)
+        return fail(FREP_ERR_INVALID_ARG, "frep_render: bad camera");
+    if (lights->count > FREP_MAX_LIGHTS) return fail(FREP_ERR_INVALID_ARG, "frep_render: too many lights");
+    if (((uintptr_t)out->rgba8 & 3) || ((uintptr_t)out->hits & 3))
+        return fail(FREP_ERR_INVALID_ARG, "frep_render: output buffers must be 4-byte aligned");
+    FREP_CUDA(cudaSetDevice(ctx->device));
+    frep::RenderArgs a{};
+    a.hdr = tree->hdr;
+    a.nodes = tree->nodes;
+    a.tapes = tree->tapes;
+    a.levels = tree->grid.levels;
+    for (uint32_t l = 0; l < a.levels; l++) {
+        a.dims[l] = tree->grid.dims[l];
+        a.node_size[l] = tree->node_size[l];
+        a.cell_size[l] = tree->cell_size[l];
+    }
+    for (int k = 0; k < 3; k++) a.low[k] = tree->grid.low_vertex[k];
+    a.world_size = tree->grid.world_size;
+    a.tape_time = tape_time;
+    // Camera::Init, Right(), Up() (camera.cpp:8-27); raytracer.cpp:177-181.
+    const H3 fwd = normalize3({cam->forward[0], cam->forward[1], cam->forward[2]});
+    const H3 up0 = normalize3({cam->up[0], cam->up[1], cam->up[2]});
+    const H3 right = normalize3(cross3(fwd, up0));
+    const H3 up = cross3(right, fwd);
+    for (int k = 0; k < 3; k++) a.pos[k] = cam->position[k];
+    a.fwd[0] = fwd.x; a.fwd[1] = fwd.y; a.fwd[2] = fwd.z;
+    a.right[0] = right.x; a.right[1] = right.y; a.right[2] = right.z;
+    a.up[0] = up.x; a.up[1] = up.y; a.up[2] = up.z;
+    a.sws_x = 2.0f * std::tan((cam->fov_deg * 0.01745329251994329577f) / 2.0f);
+    const float aspect = (float)cam->height / (float)cam->width;
+    a.sws_y = a.sws_x * aspect;
+    a.half_w = cam->ortho_width / 2.0f;
+    a.half_h = (cam->ortho_width * aspect) / 2.0f;
+    a.projection = cam->projection;
+    a.width = cam->width;
+    a.height = cam->height;
+    a.jitter = cam->jitter;
+    a.jitter_seed = cam->jitter_seed;
+    a.n_lights = lights->count;
+    for (uint32_t i = 0; i < lights->count; i++) {
+        const H3 d = normalize3({lights->direction[i][0], lights->direction[i][1], lights->direction[i][2]});
+        a.light_dir[i][0] = d.x; a.light_dir[i][1] = d.y; a.light_dir[i][2] = d.z;
+        for (int c = 0; c < 4; c++) a.light_color[i][c] = lights->color[i][c];
+    }
+    for (int c = 0; c < 4; c++) {
+        a.ambient[c] = lights->ambient[c];
+        a.background[c] = lights->background[c];
+    }
+    a.shadow_mask = lights->shadow_mask;
+    a.n_slots = tree->n_slots;
+    a.rgba8 = out->rgba8;
+    a.hits = out->hits;
+    cudaError_t e = frep::launch_render(a, (cudaStream_t)stream_ptr);
+    if (e == cudaErrorInvalidValue) return fail(FREP_ERR_UNSUPPORTED, "frep_render: more than 1024 slots");
+    if (e != cudaSuccess) return cuda_fail(e, "render_kernel");
+    return FREP_OK;
+}
+
+}  // extern "C"

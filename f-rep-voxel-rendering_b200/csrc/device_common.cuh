@@ -1,0 +1,187 @@
+// Device-side definitions shared by the voxelizer and raytracer kernels.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "frep/frep_math.h"
+
+namespace frep {
+namespace dev {
+
+constexpr uint32_t OP_CONST = 0, OP_SIN = 1, OP_COS = 2, OP_ADD = 3, OP_SUB = 4, OP_MUL = 5,
+                   OP_DIV = 6, OP_MIN = 7, OP_MAX = 8, OP_EXP = 9, OP_NEG = 10, OP_SQRT = 11,
+                   OP_COPY = 12;
+constexpr uint32_t MM_FIRST = 1, MM_SECOND = 2, MM_BOTH = 3;
+constexpr float EPS = 0.0001f;                    // utils.comp:19
+constexpr float PI_F = 3.141592653589793238f;     // utils.comp:2
+constexpr uint32_t MAX_LEVELS = 8;
+constexpr uint32_t MAX_DDA_STEPS = 1u << 16;      // bound on every DDA loop
+constexpr uint32_t TAPE_ALIGN_WORDS = 16;         // tape records start on 128-byte lines
+
+// Device-resident state of one tree (one per frep_tree). Counters are reset by
+// the init kernel at the start of every voxelization.
+struct TreeHeader {
+    uint32_t node_count[MAX_LEVELS];           // interiorNodeCount
+    unsigned long long work_cursor[MAX_LEVELS]; // dynamic work fetch per level
+    unsigned long long node_ofs[MAX_LEVELS];   // u32 words
+    unsigned long long tape_top;               // u64 words
+    unsigned long long tape_size_sum[MAX_LEVELS];
+    uint32_t tape_size_max[MAX_LEVELS];
+    unsigned long long cell_instr[MAX_LEVELS]; // cell-instructions evaluated per level
+    uint32_t overflow;                         // bit 0 node pool, bit 1 tape pool
+    uint32_t status;                           // reserved for bounded-wait failures
+};
+
+__host__ __device__ inline uint32_t node_words(uint32_t dim, bool last) {
+    const uint32_t c3 = dim * dim * dim;       // node.comp:4-15
+    return last ? 4 + (c3 >> 4) : 4 + 17 * (c3 >> 4);
+}
+
+__device__ __forceinline__ uint32_t w_op(uint64_t w) { return (uint32_t)w & 0xFFu; }
+__device__ __forceinline__ uint32_t w_out(uint64_t w) { return ((uint32_t)w >> 16) & 0xFFFFu; }
+__device__ __forceinline__ uint32_t w_a(uint64_t w) { return (uint32_t)(w >> 32) & 0xFFFFu; }
+__device__ __forceinline__ uint32_t w_b(uint64_t w) { return (uint32_t)(w >> 48); }
+__device__ __forceinline__ float w_const(uint64_t w) { return __uint_as_float((uint32_t)(w >> 32)); }
+__device__ __forceinline__ bool is_mm(uint32_t op) { return op == OP_MIN || op == OP_MAX; }
+
+// glm's min/max selection rules (the oracle uses the same selects).
+__device__ __forceinline__ float min_sel(float a, float b) { return (b < a) ? b : a; }
+__device__ __forceinline__ float max_sel(float a, float b) { return (a < b) ? b : a; }
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// ---- interval arithmetic (interval.comp:8-111) --------------------------------
+// ROUND = 0: the reference's round-to-nearest; ROUND = 1: outward (directed
+// rounding intrinsics), conservative.
+template <int ROUND>
+__device__ __forceinline__ float2 iv_mul(float2 a, float2 b) {
+    if (ROUND) {
+        const float l0 = __fmul_rd(a.x, b.x), l1 = __fmul_rd(a.x, b.y), l2 = __fmul_rd(a.y, b.x),
+                    l3 = __fmul_rd(a.y, b.y);
+        const float h0 = __fmul_ru(a.x, b.x), h1 = __fmul_ru(a.x, b.y), h2 = __fmul_ru(a.y, b.x),
+                    h3 = __fmul_ru(a.y, b.y);
+        return make_float2(min_sel(min_sel(l0, l1), min_sel(l2, l3)),
+                           max_sel(max_sel(h0, h1), max_sel(h2, h3)));
+    } else {
+        const float p0 = __fmul_rn(a.x, b.x), p1 = __fmul_rn(a.x, b.y), p2 = __fmul_rn(a.y, b.x),
+                    p3 = __fmul_rn(a.y, b.y);
+        return make_float2(min_sel(min_sel(p0, p1), min_sel(p2, p3)),
+                           max_sel(max_sel(p0, p1), max_sel(p2, p3)));
+    }
+}
+
+__device__ __forceinline__ bool contains_multiple(float lo, float hi, float x) {
+    const float ql = __fdiv_rn(lo, x), qh = __fdiv_rn(hi, x);
+    const float fl = floorf(ql), fh = floorf(qh);
+    return fl < fh || fl == ql || fh == qh;
+}
+
+static __device__ __noinline__ float2 iv_sincos_rn(float2 a, bool is_cos) {
+    const float two_pi = 2.0f * PI_F, half_pi = PI_F / 2.0f;
+    if (!is_cos) {
+        const float s_lo = frep_sinf(a.x), s_hi = frep_sinf(a.y);
+        const float lo = contains_multiple(__fadd_rn(a.x, half_pi), __fadd_rn(a.y, half_pi), two_pi)
+                             ? -1.0f : min_sel(s_lo, s_hi);
+        const float hi = contains_multiple(__fsub_rn(a.x, half_pi), __fsub_rn(a.y, half_pi), two_pi)
+                             ? 1.0f : max_sel(s_lo, s_hi);
+        return make_float2(lo, hi);
+    }
+    const float c_lo = frep_cosf(a.x), c_hi = frep_cosf(a.y);
+    const float lo = contains_multiple(__fsub_rn(a.x, PI_F), __fsub_rn(a.y, PI_F), two_pi)
+                         ? -1.0f : min_sel(c_lo, c_hi);
+    const float hi = contains_multiple(a.x, a.y, two_pi) ? 1.0f : max_sel(c_lo, c_hi);
+    return make_float2(lo, hi);
+}
+
+__device__ __forceinline__ bool critical_in(double lo, double hi, double phase) {
+    const double two_pi = 6.283185307179586;
+    const double kl = ceil(__dsub_rn(__ddiv_rn(__dsub_rn(lo, phase), two_pi), 1e-9));
+    const double kh = floor(__dadd_rn(__ddiv_rn(__dsub_rn(hi, phase), two_pi), 1e-9));
+    return kl <= kh;
+}
+
+static __device__ __noinline__ float2 iv_sincos_out(float2 a, bool is_cos) {
+    const double lo = a.x, hi = a.y;
+    if (!(__dsub_rn(hi, lo) < 6.0) || !(fabs(lo) < 1048576.0) || !(fabs(hi) < 1048576.0))
+        return make_float2(-1.0f, 1.0f);
+    const double ph_max = is_cos ? 0.0 : 1.5707963267948966;
+    const double ph_min = is_cos ? 3.141592653589793 : -1.5707963267948966;
+    const float f_lo = is_cos ? frep_cosf(a.x) : frep_sinf(a.x);
+    const float f_hi = is_cos ? frep_cosf(a.y) : frep_sinf(a.y);
+    const float l = critical_in(lo, hi, ph_min) ? -1.0f : max_sel(-1.0f, frep_next_down(min_sel(f_lo, f_hi)));
+    const float h = critical_in(lo, hi, ph_max) ? 1.0f : min_sel(1.0f, frep_next_up(max_sel(f_lo, f_hi)));
+    return make_float2(l, h);
+}
+
+template <int ROUND>
+__device__ __noinline__ float2 iv_div(float2 a, float2 b) {
+    const float inf = __int_as_float(0x7f800000);
+    if ((b.x == 0.0f && b.y == 0.0f) || (b.x < 0.0f && b.y > 0.0f)) return make_float2(-inf, inf);
+    float2 r;
+    if (b.x == 0.0f) r = make_float2(ROUND ? __fdiv_rd(1.0f, b.y) : __fdiv_rn(1.0f, b.y), inf);
+    else if (b.y == 0.0f) r = make_float2(-inf, ROUND ? __fdiv_ru(1.0f, b.x) : __fdiv_rn(1.0f, b.x));
+    else r = make_float2(ROUND ? __fdiv_rd(1.0f, b.y) : __fdiv_rn(1.0f, b.y),
+                         ROUND ? __fdiv_ru(1.0f, b.x) : __fdiv_rn(1.0f, b.x));
+    return iv_mul<ROUND>(a, r);
+}
+
+template <int ROUND>
+__device__ __noinline__ float2 iv_exp(float2 a) {
+    const float el = frep_expf(a.x), eh = frep_expf(a.y);
+    if (ROUND) return make_float2(max_sel(0.0f, frep_next_down(el)), frep_next_up(eh));
+    return make_float2(el, eh);
+}
+
+// One interval instruction (INTERVAL_UPDATE_SLOTS, interval.comp:36-111).
+template <int ROUND>
+__device__ __forceinline__ float2 iv_apply(uint32_t op, uint64_t w, float2 a, float2 b) {
+    switch (op) {
+        case OP_CONST: { const float c = w_const(w); return make_float2(c, c); }
+        case OP_ADD:
+            return ROUND ? make_float2(__fadd_rd(a.x, b.x), __fadd_ru(a.y, b.y))
+                         : make_float2(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y));
+        case OP_SUB:
+            return ROUND ? make_float2(__fsub_rd(a.x, b.y), __fsub_ru(a.y, b.x))
+                         : make_float2(__fsub_rn(a.x, b.y), __fsub_rn(a.y, b.x));
+        case OP_MUL: return iv_mul<ROUND>(a, b);
+        case OP_MIN: return make_float2(min_sel(a.x, b.x), min_sel(a.y, b.y));
+        case OP_MAX: return make_float2(max_sel(a.x, b.x), max_sel(a.y, b.y));
+        case OP_NEG: return make_float2(-a.y, -a.x);
+        case OP_SQRT: {
+            const float l = max_sel(0.0f, a.x), h = max_sel(0.0f, a.y);
+            return ROUND ? make_float2(__fsqrt_rd(l), __fsqrt_ru(h))
+                         : make_float2(__fsqrt_rn(l), __fsqrt_rn(h));
+        }
+        case OP_DIV: return iv_div<ROUND>(a, b);
+        case OP_EXP: return iv_exp<ROUND>(a);
+        case OP_SIN: return ROUND ? iv_sincos_out(a, false) : iv_sincos_rn(a, false);
+        case OP_COS: return ROUND ? iv_sincos_out(a, true) : iv_sincos_rn(a, true);
+        default: return a;  // COPY
+    }
+}
+
+// Point evaluation of one instruction (point.comp:41-81).
+__device__ __forceinline__ float pt_apply(uint32_t op, uint64_t w, float a, float b) {
+    switch (op) {
+        case OP_CONST: return w_const(w);
+        case OP_ADD: return __fadd_rn(a, b);
+        case OP_SUB: return __fsub_rn(a, b);
+        case OP_MUL: return __fmul_rn(a, b);
+        case OP_MIN: return min_sel(a, b);
+        case OP_MAX: return max_sel(a, b);
+        case OP_NEG: return -a;
+        case OP_SQRT: return __fsqrt_rn(a);
+        case OP_DIV: return __fdiv_rn(a, b);
+        case OP_EXP: return frep_expf(a);
+        case OP_SIN: return frep_sinf(a);
+        case OP_COS: return frep_cosf(a);
+        default: return a;  // COPY
+    }
+}
+
+}  // namespace dev
+}  // namespace frep

@@ -1,0 +1,378 @@
+"""frep — B200-native F-rep voxelize-and-raytrace (host-side Python mirror).
+
+The classes follow the reference's host interface for this path so that code
+written against it reads the same:
+
+* ``csg`` (``frep.csg``)       — ``csg::Expr`` / ``csg::lib`` scene construction
+* ``Tape``                     — ``csg::Tape`` (vulkan/include/csg/tape.h:12-83)
+* ``VoxelStorage``             — ``VoxelStorage`` (vulkan/include/engine/voxel_storage.h:9-89)
+* ``Voxelizer.voxelize``       — ``Voxelizer::Voxelize`` (vulkan/src/engine/voxelizer.cpp:429-440)
+* ``Camera`` / ``Raytracer.trace`` — ``Camera`` (camera.h) / ``Raytracer::Trace`` (raytracer.cpp:243-272)
+
+Everything below calls the C-ABI in include/frep.h (libfrep.so); the compute
+runs in the sm_100a kernels. Device buffers and streams are torch's.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import csg
+from . import _lib as L
+from ._lib import FrepError
+
+__all__ = ["csg", "Tape", "Context", "VoxelStorage", "Voxelizer", "Camera", "Lights", "Raytracer",
+           "FrepError", "ROUND_NEAREST", "ROUND_OUTWARD", "TreeExport"]
+
+ROUND_NEAREST = 0
+ROUND_OUTWARD = 1
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _dag_struct(expr: csg.Expr):
+    ops, in0, in1, consts, root = expr.flatten()
+    d = L.Dag(len(ops), ops.ctypes.data_as(C.POINTER(C.c_uint8)), in0.ctypes.data_as(C.POINTER(C.c_uint32)),
+              in1.ctypes.data_as(C.POINTER(C.c_uint32)), consts.ctypes.data_as(C.POINTER(C.c_float)), root)
+    return d, (ops, in0, in1, consts)
+
+
+class Tape:
+    """A compiled tape (csg::Tape). ``Tape(expr)`` runs the library's compiler
+    (simplify, topological sort, constant pool, slot allocation)."""
+
+    def __init__(self, expr: csg.Expr | None = None, *, _handle=None):
+        self._h = C.c_void_p()
+        if _handle is not None:
+            self._h = _handle
+        elif expr is not None:
+            d, keep = _dag_struct(expr)
+            L.check(L.lib().frep_tape_compile(C.byref(d), C.byref(self._h)))
+        else:
+            raise ValueError("Tape needs an expression")
+        info = L.TapeInfo()
+        L.check(L.lib().frep_tape_get_info(self._h, C.byref(info)))
+        self.n_instr = info.n_instr
+        self.n_slots = info.n_slots
+        self.n_consts = info.n_consts
+        self.n_minmax = info.n_minmax
+        self.fits_reference = bool(info.fits_reference)
+        self.uses_time = bool(info.uses_time)
+
+    @classmethod
+    def from_reference(cls, instrs, consts) -> "Tape":
+        """Imports a tape in the reference's 8-bit upload format + constant pool."""
+        instrs = np.ascontiguousarray(instrs, np.uint32)
+        consts = np.ascontiguousarray(consts, np.float32)
+        h = C.c_void_p()
+        L.check(L.lib().frep_tape_from_reference(_ptr(instrs), len(instrs), _ptr(consts), len(consts), C.byref(h)))
+        return cls(_handle=h)
+
+    @classmethod
+    def from_dag(cls, ops, in0, in1, consts, root) -> "Tape":
+        ops = np.ascontiguousarray(ops, np.uint8)
+        in0 = np.ascontiguousarray(in0, np.uint32)
+        in1 = np.ascontiguousarray(in1, np.uint32)
+        consts = np.ascontiguousarray(consts, np.float32)
+        d = L.Dag(len(ops), ops.ctypes.data_as(C.POINTER(C.c_uint8)), in0.ctypes.data_as(C.POINTER(C.c_uint32)),
+                  in1.ctypes.data_as(C.POINTER(C.c_uint32)), consts.ctypes.data_as(C.POINTER(C.c_float)), int(root))
+        h = C.c_void_p()
+        L.check(L.lib().frep_tape_compile(C.byref(d), C.byref(h)))
+        return cls(_handle=h)
+
+    def __del__(self):
+        if getattr(self, "_h", None) and self._h.value:
+            L.lib().frep_tape_destroy(self._h)
+            self._h = C.c_void_p()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def wide(self) -> np.ndarray:
+        """Instruction words of the library's wide encoding (include/frep.h)."""
+        out = np.zeros(self.n_instr, np.uint64)
+        L.check(L.lib().frep_tape_get_instrs(self._h, _ptr(out), self.n_instr))
+        return out
+
+    @property
+    def instructions(self) -> np.ndarray:
+        """csg::Tape::instructions packed as the reference uploads them."""
+        instrs = np.zeros(self.n_instr, np.uint32)
+        consts = np.zeros(max(self.n_consts, 1), np.float32)
+        L.check(L.lib().frep_tape_get_reference(self._h, _ptr(instrs), _ptr(consts)))
+        return instrs
+
+    @property
+    def constant_pool(self) -> np.ndarray:
+        instrs = np.zeros(self.n_instr, np.uint32)
+        consts = np.zeros(max(self.n_consts, 1), np.float32)
+        L.check(L.lib().frep_tape_get_reference(self._h, _ptr(instrs), _ptr(consts)))
+        return consts[: self.n_consts]
+
+    def slot_count(self) -> int:
+        return self.n_slots
+
+    def eval_points(self, xyzt) -> np.ndarray:
+        xyzt = np.ascontiguousarray(xyzt, np.float32).reshape(-1, 4)
+        out = np.zeros(len(xyzt), np.float32)
+        L.check(L.lib().frep_tape_eval(self._h, _ptr(xyzt), len(xyzt), _ptr(out)))
+        return out
+
+    def eval(self, x, y, z, t=0.0) -> float:
+        return float(self.eval_points(np.array([[x, y, z, t]], np.float32))[0])
+
+
+class Context:
+    """One device and its HBM budget (frep_ctx)."""
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0):
+        self._h = C.c_void_p()
+        L.check(L.lib().frep_ctx_create(device, hbm_budget_bytes, C.byref(self._h)))
+        self.device = device
+
+    def memory(self):
+        used, budget = C.c_uint64(), C.c_uint64()
+        L.check(L.lib().frep_ctx_memory(self._h, C.byref(used), C.byref(budget)))
+        return used.value, budget.value
+
+    def close(self):
+        if self._h is not None and self._h.value and L is not None and L._lib is not None:
+            L.lib().frep_ctx_destroy(self._h)
+        self._h = C.c_void_p()
+
+    def __del__(self):
+        self.close()
+
+
+@dataclass
+class TreeExport:
+    """A tree copied to the host: its header (frep_tree_info fields), the node
+    pool (reference layout, u32) and the tape pool (u64)."""
+
+    levels: int
+    dims: list
+    node_count: list
+    node_offset: list
+    node_size: list
+    tape_size_sum: list
+    tape_size_max: list
+    tape_words_used: int
+    nodes: np.ndarray
+    tapes: np.ndarray
+
+
+class VoxelStorage:
+    """Grid description + device tree (VoxelStorage, voxel_storage.h:9-89).
+    Fill grid_dims / low_vertex / world_size, then call init(ctx, shape)."""
+
+    def __init__(self, grid_dims=(16, 4), low_vertex=(-1.5, -1.5, -1.5), world_size=3.0,
+                 rounding: int = ROUND_OUTWARD, shorten: bool = True, node_words: int = 0,
+                 tape_words: int = 0):
+        self.grid_dims = list(grid_dims)
+        self.low_vertex = tuple(float(v) for v in low_vertex)
+        self.world_size = float(world_size)
+        self.rounding = rounding
+        self.shorten = shorten
+        self.node_words = node_words
+        self.tape_words = tape_words
+        self.tape: Tape | None = None
+        self.ctx: Context | None = None
+        self._tree = C.c_void_p()
+        self.interior_node_count: list[int] = []
+
+    @property
+    def grid_levels(self) -> int:
+        return len(self.grid_dims)
+
+    @property
+    def fine_grid_dim(self) -> int:
+        return int(np.prod(self.grid_dims))
+
+    def grid_struct(self) -> L.Grid:
+        g = L.Grid()
+        g.levels = len(self.grid_dims)
+        for i, d in enumerate(self.grid_dims):
+            g.dims[i] = d
+        for i in range(3):
+            g.low_vertex[i] = self.low_vertex[i]
+        g.world_size = self.world_size
+        return g
+
+    def init(self, ctx: Context, shape) -> "VoxelStorage":
+        self.ctx = ctx
+        self.tape = shape if isinstance(shape, Tape) else Tape(shape)
+        opts = L.VoxelizeOpts(self.rounding, 1 if self.shorten else 0, self.node_words, self.tape_words)
+        g = self.grid_struct()
+        L.check(L.lib().frep_tree_create(ctx._h, C.byref(g), C.byref(opts), C.byref(self._tree)))
+        self.interior_node_count = [0] * self.grid_levels
+        return self
+
+    @property
+    def tree(self):
+        return self._tree
+
+    def cleanup(self):
+        if self._tree.value:
+            L.lib().frep_tree_destroy(self._tree)
+            self._tree = C.c_void_p()
+
+    def __del__(self):
+        self.cleanup()
+
+    def sync(self, raise_on_overflow: bool = True) -> L.TreeInfo:
+        info = L.TreeInfo()
+        st = L.lib().frep_tree_sync(self._tree, C.byref(info))
+        if st != L.OK and (raise_on_overflow or st != L.ERR_CAPACITY):
+            L.check(st)
+        self.interior_node_count = list(info.node_count[: self.grid_levels])
+        return info
+
+    def work(self) -> list[int]:
+        arr = (C.c_uint64 * L.MAX_LEVELS)()
+        L.check(L.lib().frep_tree_work(self._tree, arr))
+        return list(arr[: self.grid_levels])
+
+    def set_profiling(self, enable: bool = True) -> None:
+        L.check(L.lib().frep_tree_set_profiling(self._tree, 1 if enable else 0))
+
+    def level_timings(self) -> list[float]:
+        """Device milliseconds of each level pass of the last voxelization."""
+        arr = (C.c_float * L.MAX_LEVELS)()
+        L.check(L.lib().frep_tree_timings(self._tree, arr))
+        return list(arr[: self.grid_levels])
+
+    def export(self) -> TreeExport:
+        info = self.sync()
+        nodes = np.zeros(max(info.node_words_used, 1), np.uint32)
+        tapes = np.zeros(max(info.tape_words_used, 1), np.uint64)
+        L.check(L.lib().frep_tree_copy_nodes(self._tree, _ptr(nodes), info.node_words_used))
+        L.check(L.lib().frep_tree_copy_tapes(self._tree, _ptr(tapes), info.tape_words_used))
+        n = self.grid_levels
+        return TreeExport(n, list(info.dims[:n]), list(info.node_count[:n]), list(info.node_offset[:n]),
+                          list(info.node_size[:n]), list(info.tape_size_sum[:n]),
+                          list(info.tape_size_max[:n]), info.tape_words_used, nodes, tapes)
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        try:
+            import torch
+            return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+        except Exception:
+            return C.c_void_p(0)
+    if hasattr(stream, "cuda_stream"):
+        return C.c_void_p(stream.cuda_stream)
+    return C.c_void_p(int(stream))
+
+
+class Voxelizer:
+    """Builds the sparse tree on the device (Voxelizer, voxelizer.h:12-113)."""
+
+    def __init__(self, ctx: Context, voxels: VoxelStorage):
+        self.ctx = ctx
+        self.voxels = voxels
+
+    def voxelize(self, tape_time: float = 0.0, stream=None) -> None:
+        """Enqueues every level pass on `stream`; no host round trip per level."""
+        L.check(L.lib().frep_voxelize(self.ctx._h, self.voxels.tree, self.voxels.tape.handle,
+                                      float(tape_time), _stream_ptr(stream)))
+
+    def print_stats(self) -> None:
+        info = self.voxels.sync()
+        total = sum(info.node_count[: self.voxels.grid_levels])
+        print(f"[+] Total interior nodes :\n\tcount={total}\tnode buf words={info.node_words_used}")
+        print(f"[+] Total tapes :\n\ttape buf bytes={8 * info.tape_words_used}")
+        for i in range(self.voxels.grid_levels):
+            cnt = max(info.node_count[i], 1)
+            print(f"\t{i}: nodes={info.node_count[i]}  avg tape={info.tape_size_sum[i] / cnt:.1f}"
+                  f"  max tape={info.tape_size_max[i]}")
+
+
+@dataclass
+class Camera:
+    """Camera (camera.h:6-41). forward / initial_up are normalised by the
+    library; fov_deg is the horizontal field of view."""
+
+    position: tuple = (0.0, 0.0, 40.0)
+    forward: tuple = (0.0, 0.0, -1.0)
+    initial_up: tuple = (0.0, 1.0, 0.0)
+    fov_deg: float = 45.0
+    orthographic: bool = False
+    ortho_width: float = 2.0
+    jitter: bool = False
+    jitter_seed: float = 0.0
+
+    def struct(self, width: int, height: int) -> L.CameraStruct:
+        c = L.CameraStruct()
+        for i in range(3):
+            c.position[i] = self.position[i]
+            c.forward[i] = self.forward[i]
+            c.up[i] = self.initial_up[i]
+        c.fov_deg = self.fov_deg
+        c.ortho_width = self.ortho_width
+        c.projection = 1 if self.orthographic else 0
+        c.width, c.height = width, height
+        c.jitter = 1 if self.jitter else 0
+        c.jitter_seed = self.jitter_seed
+        return c
+
+
+@dataclass
+class Lights:
+    """Directional lights, ambient and background (raytracer.cpp:183-192).
+    Defaults are the reference's two hard-coded lights."""
+
+    directions: list = field(default_factory=lambda: [(-1.0, -1.0, -0.2), (1.0, -1.0, -0.2)])
+    colors: list = field(default_factory=lambda: [(1.0, 0.0, 0.0, 0.0), (0.0, 0.0, 2.0, 0.0)])
+    ambient: tuple = (0.2, 0.2, 0.2, 1.0)
+    background: tuple = (0.0, 0.0, 0.0, 1.0)
+    shadow_mask: int = 0
+
+    def struct(self) -> L.LightsStruct:
+        s = L.LightsStruct()
+        s.count = len(self.directions)
+        for i, (d, c) in enumerate(zip(self.directions, self.colors)):
+            for k in range(3):
+                s.direction[i][k] = d[k]
+            for k in range(4):
+                s.color[i][k] = c[k]
+        for k in range(4):
+            s.ambient[k] = self.ambient[k]
+            s.background[k] = self.background[k]
+        s.shadow_mask = self.shadow_mask
+        return s
+
+
+class Raytracer:
+    """Renders a voxelized tree (Raytracer, raytracer.h:15-121) into device
+    buffers (torch tensors): an rgba8 image and optionally hit records."""
+
+    def __init__(self, ctx: Context, voxels: VoxelStorage):
+        self.ctx = ctx
+        self.voxels = voxels
+        self.lights = Lights()
+
+    def set_background_color(self, rgb) -> None:
+        self.lights.background = (float(rgb[0]), float(rgb[1]), float(rgb[2]), 1.0)
+
+    def trace(self, camera: Camera, tape_time: float = 0.0, width: int = 256, height: int = 256,
+              hits: bool = False, out=None, stream=None):
+        import torch
+        dev = torch.device("cuda", self.ctx.device)
+        if out is None:
+            rgba = torch.empty((height, width, 4), dtype=torch.uint8, device=dev)
+            hit_buf = torch.empty((height, width, 8), dtype=torch.int32, device=dev) if hits else None
+        else:
+            rgba, hit_buf = out
+        img = L.Image(rgba.data_ptr() if rgba is not None else None,
+                      hit_buf.data_ptr() if hit_buf is not None else None)
+        cam = camera.struct(width, height)
+        lights = self.lights.struct()
+        L.check(L.lib().frep_render(self.ctx._h, self.voxels.tree, C.byref(cam), C.byref(lights),
+                                    float(tape_time), C.byref(img), _stream_ptr(stream)))
+        return rgba, hit_buf

@@ -1,0 +1,268 @@
+/* frep.h — C-ABI of the B200 F-rep voxelize-and-raytrace library.
+ *
+ * This is the drop-in boundary for the reference's hot path
+ * (MathisBD/f-rep-voxel-rendering, vulkan/): every entry point below names the
+ * reference interface it replaces. Plain pointers and sizes only; CUDA streams
+ * are passed as `void*` (a cudaStream_t, NULL = the legacy default stream).
+ *
+ * Conventions
+ *   - Every function returns frep_status. The reference has no status codes (it
+ *     prints and asserts: vulkan/include/vk_wrapper/vk_check.h:8-18, tape.cpp:
+ *     223-227); here each of those failure points returns an error instead.
+ *   - Handles are opaque and owned by the library; *_destroy releases them.
+ *   - A frep_ctx owns one device's memory arena with an explicit HBM budget.
+ *     It is thread-compatible (one host thread at a time), not thread-safe.
+ *   - frep_last_error() returns a message for the most recent failure on the
+ *     calling thread.
+ */
+#ifndef FREP_H
+#define FREP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum frep_status {
+    FREP_OK = 0,
+    FREP_ERR_INVALID_ARG = 1,   /* bad pointer, size or enum value                */
+    FREP_ERR_OOM = 2,           /* the context's HBM budget or cudaMalloc refused */
+    FREP_ERR_CAPACITY = 3,      /* a tree's node or tape pool filled up           */
+    FREP_ERR_TIMEOUT = 4,       /* a bounded device loop gave up                  */
+    FREP_ERR_CUDA = 5,          /* a CUDA runtime call failed                     */
+    FREP_ERR_UNSUPPORTED = 6,   /* valid request outside this build's limits      */
+    FREP_ERR_COMPILE = 7        /* the expression could not be compiled to a tape */
+} frep_status;
+
+const char* frep_last_error(void);
+const char* frep_version(void);
+
+/* ---------------------------------------------------------------------------
+ * Expressions and tapes
+ * ------------------------------------------------------------------------- */
+
+/* csg::Operator numbering (vulkan/include/csg/expression.h:14-22). */
+enum {
+    FREP_OP_X = 0, FREP_OP_Y, FREP_OP_Z, FREP_OP_T, FREP_OP_CONST,
+    FREP_OP_SIN, FREP_OP_COS, FREP_OP_EXP, FREP_OP_NEG, FREP_OP_SQRT,
+    FREP_OP_ADD, FREP_OP_SUB, FREP_OP_MUL, FREP_OP_DIV, FREP_OP_MIN, FREP_OP_MAX
+};
+
+/* Tape opcodes (vulkan/include/csg/tape.h:15-30). */
+enum {
+    FREP_TAPE_CONST = 0, FREP_TAPE_SIN, FREP_TAPE_COS, FREP_TAPE_ADD, FREP_TAPE_SUB,
+    FREP_TAPE_MUL, FREP_TAPE_DIV, FREP_TAPE_MIN, FREP_TAPE_MAX, FREP_TAPE_EXP,
+    FREP_TAPE_NEG, FREP_TAPE_SQRT, FREP_TAPE_COPY
+};
+
+/* A flattened csg::Expr DAG: node i = (ops[i], in0[i], in1[i], consts[i]);
+ * inputs refer to earlier nodes; unused inputs are ignored. This is how a
+ * csg::Expr (shared_ptr DAG, expression.h:29-100) crosses the boundary. */
+typedef struct frep_dag {
+    uint32_t n_nodes;
+    const uint8_t* ops;
+    const uint32_t* in0;
+    const uint32_t* in1;
+    const float* consts;
+    uint32_t root;
+} frep_dag;
+
+typedef struct frep_tape frep_tape;
+
+typedef struct frep_tape_info {
+    uint32_t n_instr;         /* csg::Tape::instructions.size()                 */
+    uint32_t n_slots;         /* csg::Tape::GetSlotCount()                      */
+    uint32_t n_consts;        /* csg::Tape::constantPool.size()                 */
+    uint32_t n_minmax;        /* MIN/MAX instructions (pruning choice points)   */
+    uint32_t fits_reference;  /* 1 if the 8-bit reference encoding can hold it  */
+    uint32_t uses_time;       /* 1 if slot 3 (T) is read                        */
+} frep_tape_info;
+
+/* Replaces csg::Tape::Tape(Expr) (vulkan/src/csg/tape.cpp:14-228): simplify,
+ * topologically sort, pool constants, allocate slots. Same instruction stream
+ * as the reference; wide encoding so that large scenes compile. */
+frep_status frep_tape_compile(const frep_dag* dag, frep_tape** out);
+
+/* Accepts a tape in the reference's own upload format
+ * (vulkan/src/engine/voxelizer.cpp:385-398: op | out<<8 | inA<<16 | inB<<24)
+ * with its constant pool. */
+frep_status frep_tape_from_reference(const uint32_t* instrs, uint32_t n_instr, const float* consts,
+                                     uint32_t n_consts, frep_tape** out);
+
+frep_status frep_tape_get_info(const frep_tape* tape, frep_tape_info* info);
+
+/* Wide instruction words (8 bytes each): op bits 0-7, out 16-31, inA 32-47,
+ * inB 48-63; for CONST bits 32-63 hold the float. cap = capacity of `out`. */
+frep_status frep_tape_get_instrs(const frep_tape* tape, uint64_t* out, uint32_t cap);
+
+/* csg::Tape::instructions / constantPool in the reference's 8-bit encoding;
+ * FREP_ERR_UNSUPPORTED when the tape does not fit it (fits_reference == 0). */
+frep_status frep_tape_get_reference(const frep_tape* tape, uint32_t* instrs, float* consts);
+
+/* Replaces csg::Tape::Eval (tape.cpp:274-302) on the host: n points, 4 floats
+ * (x, y, z, t) each. */
+frep_status frep_tape_eval(const frep_tape* tape, const float* xyzt, uint32_t n, float* out);
+
+void frep_tape_destroy(frep_tape* tape);
+
+/* ---------------------------------------------------------------------------
+ * Device context
+ * ------------------------------------------------------------------------- */
+
+typedef struct frep_ctx frep_ctx;
+
+/* Opens `device` with an HBM budget in bytes (0 = 90% of free memory). Replaces
+ * the Vulkan device/VMA set-up of EngineBase::Init (engine_base.cpp:45-160). */
+frep_status frep_ctx_create(int device, uint64_t hbm_budget_bytes, frep_ctx** out);
+void frep_ctx_destroy(frep_ctx* ctx);
+/* Bytes of the budget currently held by trees and scratch. */
+frep_status frep_ctx_memory(const frep_ctx* ctx, uint64_t* used, uint64_t* budget);
+
+/* ---------------------------------------------------------------------------
+ * Voxelization (sparse tree build)
+ * ------------------------------------------------------------------------- */
+
+#define FREP_MAX_LEVELS 8
+
+/* VoxelStorage's inputs (vulkan/include/engine/voxel_storage.h:15-22):
+ * gridDims (children per axis per level; each a multiple of 4, 4..32),
+ * lowVertex and worldSize. */
+typedef struct frep_grid {
+    uint32_t levels;
+    uint32_t dims[FREP_MAX_LEVELS];
+    float low_vertex[3];
+    float world_size;
+} frep_grid;
+
+enum {
+    FREP_ROUND_NEAREST = 0,   /* the reference's round-to-nearest intervals       */
+    FREP_ROUND_OUTWARD = 1    /* directed rounding: every interval is conservative */
+};
+
+typedef struct frep_voxelize_opts {
+    uint32_t rounding;        /* FREP_ROUND_*                                        */
+    uint32_t shorten;         /* 1 = prune min/max into shortened child tapes (ref.) */
+    uint64_t node_words;      /* node pool capacity in u32 words (0 = automatic)     */
+    uint64_t tape_words;      /* tape pool capacity in u64 words (0 = automatic)     */
+} frep_voxelize_opts;
+
+typedef struct frep_tree frep_tree;
+
+/* Creates an empty tree for `grid` with its own node and tape pools (carved
+ * from the context's budget). The tree can be re-voxelized many times. */
+frep_status frep_tree_create(frep_ctx* ctx, const frep_grid* grid, const frep_voxelize_opts* opts,
+                             frep_tree** out);
+void frep_tree_destroy(frep_tree* tree);
+
+/* Replaces Voxelizer::Voxelize(waitSem, tapeTime) (vulkan/src/engine/
+ * voxelizer.cpp:429-440, with VoxelizeLevel :295-329). Builds the whole tree
+ * level by level on `stream` WITHOUT a host round trip per level; returns when
+ * the work is enqueued. Overflow of the pools is reported by frep_tree_sync. */
+frep_status frep_voxelize(frep_ctx* ctx, frep_tree* tree, const frep_tape* tape, float tape_time,
+                          void* stream);
+
+/* Waits for the tree's stream and reads its header. Replaces the per-level
+ * childCount readback (voxelizer.cpp:326-328) and PrintStats (:442-478). */
+typedef struct frep_tree_info {
+    uint32_t levels;
+    uint32_t dims[FREP_MAX_LEVELS];
+    uint32_t node_count[FREP_MAX_LEVELS];      /* interiorNodeCount              */
+    uint64_t node_offset[FREP_MAX_LEVELS];     /* in u32 words                   */
+    uint32_t node_size[FREP_MAX_LEVELS];       /* in u32 words                   */
+    uint64_t tape_size_sum[FREP_MAX_LEVELS];   /* stats_buf.tape_size_sum        */
+    uint32_t tape_size_max[FREP_MAX_LEVELS];   /* stats_buf.max_tape_size        */
+    uint64_t node_words_used, node_words_cap;
+    uint64_t tape_words_used, tape_words_cap;
+    uint32_t overflow;                          /* bit 0 node pool, bit 1 tapes   */
+    uint32_t root_tape_words;
+} frep_tree_info;
+frep_status frep_tree_sync(frep_tree* tree, frep_tree_info* info);
+
+/* Copies the device buffers to the host (for export and parity checks). The
+ * node layout is the reference's (node.comp:1-72, voxel_storage.h:57-88):
+ * per level contiguous; node = [tapeIdx, cx, cy, cz, leafMask[dim^3/32],
+ * interiorMask[dim^3/32], childList[dim^3]], last level = [tapeIdx, cx, cy, cz,
+ * leafMask, unused]. tapeIdx indexes the tape pool in u64 words; a tape is
+ * [header: n_instr (u32) | reserved (u32)] followed by n_instr wide words. */
+frep_status frep_tree_copy_nodes(frep_tree* tree, uint32_t* dst, uint64_t n_words);
+
+/* Profiling: when enabled, frep_voxelize records a CUDA event pair around each
+ * level pass on its stream; frep_tree_timings waits for them and returns the
+ * device time of every level pass of the last voxelization, in milliseconds. */
+frep_status frep_tree_set_profiling(frep_tree* tree, int enable);
+frep_status frep_tree_timings(frep_tree* tree, float ms[FREP_MAX_LEVELS]);
+/* Cell-instructions evaluated per level by the last voxelization: the number
+ * of (cell, tape instruction) pairs the interval and point passes executed. */
+frep_status frep_tree_work(frep_tree* tree, uint64_t cell_instr[FREP_MAX_LEVELS]);
+frep_status frep_tree_copy_tapes(frep_tree* tree, uint64_t* dst, uint64_t n_words);
+
+/* ---------------------------------------------------------------------------
+ * Rendering
+ * ------------------------------------------------------------------------- */
+
+enum { FREP_PERSPECTIVE = 0, FREP_ORTHOGRAPHIC = 1 };
+
+/* Camera (vulkan/include/engine/camera.h:6-41). forward/up need not be
+ * normalised or orthogonal: right = normalize(forward x up), up' = right x forward
+ * (camera.cpp:16-27). Perspective uses the horizontal fov_deg
+ * (raytracer.cpp:177-181); orthographic uses ortho_width world units across. */
+typedef struct frep_camera {
+    float position[3];
+    float forward[3];
+    float up[3];
+    float fov_deg;
+    float ortho_width;
+    uint32_t projection;
+    uint32_t width, height;
+    uint32_t jitter;          /* 0 = ray through pixel corner (parity), 1 = jittered */
+    float jitter_seed;        /* the reference seeds rand() with the wall clock      */
+} frep_camera;
+
+#define FREP_MAX_LIGHTS 8
+/* Directional lights and background (raytracer.cpp:183-192). Directions are
+ * the direction the light travels; the library normalises them. shadow_mask
+ * bit i = cast a shadow ray toward light i (the reference's shadow ray is
+ * commented out at raytracer/main.comp:125-133). */
+typedef struct frep_lights {
+    uint32_t count;
+    float direction[FREP_MAX_LIGHTS][3];
+    float color[FREP_MAX_LIGHTS][4];
+    float ambient[4];
+    float background[4];
+    uint32_t shadow_mask;
+} frep_lights;
+
+/* Fills `lights` with the reference's two hard-coded lights, 0.2 ambient and a
+ * black background, no shadows. */
+frep_status frep_lights_default(frep_lights* lights);
+
+/* Output buffers (device pointers; any may be NULL):
+ *   rgba8 : width*height*4 bytes, row-major, the reference's rgba8 image layer
+ *   hits  : width*height frep_hit records (for parity and debugging) */
+typedef struct frep_hit {
+    float t;                  /* ray parameter of the hit (Hit.t)               */
+    float normal[3];          /* normalised gradient at the hit point           */
+    uint32_t level;           /* tree level of the hit cell, 0xFFFFFFFF = miss  */
+    uint32_t node;            /* node id at that level                          */
+    uint32_t cell;            /* bit index z + dim*y + dim^2*x inside the node  */
+    uint32_t steps;           /* DDA iterations spent                           */
+} frep_hit;
+
+typedef struct frep_image {
+    uint8_t* rgba8;
+    frep_hit* hits;
+} frep_image;
+
+/* Replaces Raytracer::Trace(waitSem, camera, tapeTime) (vulkan/src/engine/
+ * raytracer.cpp:243-272 and raytracer/main.comp:161-183). Enqueued on `stream`. */
+frep_status frep_render(frep_ctx* ctx, const frep_tree* tree, const frep_camera* camera,
+                        const frep_lights* lights, float tape_time, const frep_image* out,
+                        void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FREP_H */
