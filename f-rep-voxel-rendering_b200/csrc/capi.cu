@@ -300,7 +300,8 @@ frep_status frep_voxelize(frep_ctx* ctx, frep_tree* tree, const frep_tape* tape,
     // Launch plan for this slot / MIN-MAX count.
     if (!tree->plan_valid || tree->plan_slots != n_slots || tree->plan_mm != tape->ct.n_minmax ||
         tree->plan_round != tree->opts.rounding) {
-        cudaError_t e = frep::plan_levels(n_slots, tape->ct.n_minmax, (int)tree->opts.rounding, &tree->plan);
+        cudaError_t e = frep::plan_levels(n_slots, tape->ct.n_minmax, tree->grid.dims[tree->grid.levels - 1],
+                                          (int)tree->opts.rounding, &tree->plan);
         if (e == cudaErrorInvalidValue)
             return fail(FREP_ERR_UNSUPPORTED, "frep_voxelize: %u slots / %u min-max ops exceed shared memory", n_slots, tape->ct.n_minmax);
         if (e != cudaSuccess) return cuda_fail(e, "plan_levels");
@@ -443,6 +444,25 @@ frep_status frep_tree_work(frep_tree* tree, uint64_t* cell_instr) {
     frep::dev::TreeHeader h;
     FREP_CUDA(cudaMemcpy(&h, tree->hdr, sizeof(h), cudaMemcpyDeviceToHost));
     for (int l = 0; l < FREP_MAX_LEVELS; l++) cell_instr[l] = h.cell_instr[l];
+    return FREP_OK;
+}
+
+frep_status frep_tree_fp32_ops(frep_tree* tree, uint64_t* ops) {
+    if (!tree || !ops) return fail(FREP_ERR_INVALID_ARG, "frep_tree_fp32_ops: null argument");
+    if (!tree->voxelized) return fail(FREP_ERR_INVALID_ARG, "frep_tree_fp32_ops: the tree has not been voxelized");
+    FREP_CUDA(cudaSetDevice(tree->ctx->device));
+    const frep_grid& g = tree->grid;
+    FREP_CUDA(cudaMemsetAsync(&tree->hdr->fp32_ops[0], 0, sizeof(tree->hdr->fp32_ops), tree->stream));
+    for (uint32_t l = 0; l < g.levels; l++) {
+        cudaError_t e = frep::launch_count_ops(tree->hdr, tree->nodes, tree->tapes, tree->node_cap, l,
+                                               tree->node_size[l], g.dims[l] * g.dims[l] * g.dims[l],
+                                               l == g.levels - 1, tree->stream);
+        if (e != cudaSuccess) return cuda_fail(e, "count_ops_kernel");
+    }
+    FREP_CUDA(cudaStreamSynchronize(tree->stream));
+    frep::dev::TreeHeader h;
+    FREP_CUDA(cudaMemcpy(&h, tree->hdr, sizeof(h), cudaMemcpyDeviceToHost));
+    for (int l = 0; l < FREP_MAX_LEVELS; l++) ops[l] = h.fp32_ops[l];
     return FREP_OK;
 }
 

@@ -28,6 +28,7 @@ struct TreeHeader {
     unsigned long long tape_size_sum[MAX_LEVELS];
     uint32_t tape_size_max[MAX_LEVELS];
     unsigned long long cell_instr[MAX_LEVELS]; // cell-instructions evaluated per level
+    unsigned long long fp32_ops[MAX_LEVELS];   // op-weighted FP32 work per level (see op_weight)
     uint32_t overflow;                         // bit 0 node pool, bit 1 tape pool
     uint32_t status;                           // reserved for bounded-wait failures
 };
@@ -36,6 +37,13 @@ __host__ __device__ inline uint32_t node_words(uint32_t dim, bool last) {
     const uint32_t c3 = dim * dim * dim;       // node.comp:4-15
     return last ? 4 + (c3 >> 4) : 4 + 17 * (c3 >> 4);
 }
+
+// Algorithmic FP32 operations per cell for one tape instruction: the weights
+// of the reference's interval formulas (interval.comp:36-111) and of the point
+// interpreter (point.comp:41-81). Used only for work accounting.
+//                                  CONST SIN COS ADD SUB MUL DIV MIN MAX EXP NEG SQRT COPY
+__device__ __constant__ const uint8_t kIntervalOps[16] = {0, 18, 18, 2, 2, 10, 16, 4, 4, 2, 0, 4, 0, 0, 0, 0};
+__device__ __constant__ const uint8_t kPointOps[16]    = {0, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 0, 0, 0, 0};
 
 __device__ __forceinline__ uint32_t w_op(uint64_t w) { return (uint32_t)w & 0xFFu; }
 __device__ __forceinline__ uint32_t w_out(uint64_t w) { return ((uint32_t)w >> 16) & 0xFFFFu; }

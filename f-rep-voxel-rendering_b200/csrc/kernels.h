@@ -35,16 +35,24 @@ struct LevelPlan {
     int warps_per_block;
     int blocks;                      // persistent grid
     uint32_t smem_per_warp;
+    int point_k;                     // cells per lane in the point pass
     int point_warps_per_block;
     int point_blocks;
     uint32_t point_smem_per_warp;
 };
 
-cudaError_t plan_levels(uint32_t n_slots, uint32_t mm_cap, int rounding, LevelPlan* plan);
+cudaError_t plan_levels(uint32_t n_slots, uint32_t mm_cap, uint32_t last_dim, int rounding,
+                        LevelPlan* plan);
 cudaError_t launch_tree_init(dev::TreeHeader* hdr, uint32_t* nodes, uint32_t root_n_instr,
                              uint32_t root_words, cudaStream_t stream);
 cudaError_t launch_level(const LevelArgs& a, const LevelPlan& plan, int rounding, bool last,
                          cudaStream_t stream);
+
+// Op-weighted work of every node of `level` (interval or point weights),
+// added to the header's fp32_ops[level].
+cudaError_t launch_count_ops(dev::TreeHeader* hdr, const uint32_t* nodes, const uint64_t* tapes,
+                             unsigned long long node_cap, uint32_t level, uint32_t node_size,
+                             uint32_t cells, bool point, cudaStream_t stream);
 
 struct RenderArgs {
     const dev::TreeHeader* hdr;

@@ -4,18 +4,22 @@
 // tape/shorten.comp + tape/point.comp and the host level loop of
 // vulkan/src/engine/voxelizer.cpp:295-329, :429-440.
 //
-// Work decomposition: one WARP owns one work item = (node, 32 cells that form
-// one word of the node's masks, in bit-index order z + dim*y + dim^2*x). All
-// 32 lanes follow the same tape, so the opcode stream is warp-uniform:
-//   * the tape is staged through shared memory 32 instructions at a time
-//     (one coalesced 256-byte load per chunk, then broadcast reads);
-//   * the slot file lives in shared memory as [slot][lane] float2 (interval) or
-//     float (point) — conflict-free 8/4-byte accesses;
-//   * MIN/MAX choices are kept as two 32-bit ballots per MIN/MAX instruction;
+// Work decomposition: one WARP owns one work item = (node, a run of cells that
+// forms whole words of the node's masks, in bit-index order z + dim*y + dim^2*x).
+// All lanes follow the same tape, so the opcode stream is warp-uniform:
+//   * the tape is staged through shared memory 128 instructions at a time, each
+//     instruction decoded once into {op, row offset A, row offset B, row offset
+//     out} (one coalesced load per chunk, the next chunk prefetched into
+//     registers while the current one executes);
+//   * the slot file lives in shared memory as rows of [slot][lane] values
+//     (float2 intervals, or K floats per lane for the point pass);
+//   * MIN/MAX choices are kept as two 32-bit lane masks per MIN/MAX instruction;
+//   * shortening runs the reference's backward liveness on TRANSPOSED bitsets:
+//     live[slot] holds one bit per lane, so the pass is warp-uniform scalar code;
 //   * leaf / interior mask words are written whole from ballots (no atomics);
 //   * children are claimed with one warp-aggregated atomic per item, tapes with
-//     one more; shortened tapes are written cooperatively by the warp, one
-//     coalesced 256-byte store per 32 input instructions.
+//     one more; shortened tapes are written by the whole warp, 32 instructions
+//     per coalesced store.
 // Items are fetched in chunks from a device counter, so a level pass needs no
 // host round trip: the node count of level l is read on the device.
 #include "device_common.cuh"
@@ -23,6 +27,86 @@
 
 namespace frep {
 namespace dev {
+
+constexpr uint32_t STAGE = 128;  // instructions staged per warp
+
+// ---- shared-memory access by 32-bit address ----------------------------------
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ uint4 lds_u4(uint32_t a) {
+    uint4 v;
+    asm volatile("ld.shared.v4.u32 {%0,%1,%2,%3}, [%4];" : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "r"(a));
+    return v;
+}
+__device__ __forceinline__ float2 lds_f2(uint32_t a) {
+    float2 v;
+    asm volatile("ld.shared.v2.f32 {%0,%1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(a));
+    return v;
+}
+__device__ __forceinline__ void sts_f2(uint32_t a, float2 v) {
+    asm volatile("st.shared.v2.f32 [%0], {%1,%2};" ::"r"(a), "f"(v.x), "f"(v.y) : "memory");
+}
+__device__ __forceinline__ float4 lds_f4(uint32_t a) {
+    float4 v;
+    asm volatile("ld.shared.v4.f32 {%0,%1,%2,%3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(a));
+    return v;
+}
+__device__ __forceinline__ void sts_f4(uint32_t a, float4 v) {
+    asm volatile("st.shared.v4.f32 [%0], {%1,%2,%3,%4};" ::"r"(a), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w)
+                 : "memory");
+}
+
+// Decoded instruction as staged for execution (16 bytes):
+//   x: opcode (bits 0-7) | flags (below)
+//   y: byte offset of the A slot row (CONST: the constant's bits)
+//   z: byte offset of the B slot row
+//   w: byte offset of the output slot row
+// A row holds 32 lanes x row_bytes. The flags describe how the interpreter
+// obtains the operands: the A/B value is either forwarded from the previous
+// instruction's result (it reads the slot that instruction wrote) or loaded
+// from the slot file one instruction ahead.
+constexpr uint32_t F_FWD_A = 1u << 4, F_FWD_B = 1u << 5;
+
+__host__ __device__ constexpr bool is_binary(uint32_t op) {
+    return op == OP_ADD || op == OP_SUB || op == OP_MUL || op == OP_DIV || op == OP_MIN || op == OP_MAX;
+}
+
+// x = opcode | F_FWD_A if A is the previous instruction's output | F_FWD_B
+// likewise for B (binary ops). The interpreter switches on x, so every
+// (opcode, forwarding) combination is its own straight-line case.
+__device__ __forceinline__ uint4 decode(uint64_t w, uint32_t prev_out, uint32_t row_bytes) {
+    const uint32_t op = w_op(w);
+    const uint32_t stride = 32u * row_bytes;
+    if (op == OP_CONST) return make_uint4(op, (uint32_t)(w >> 32), 0u, w_out(w) * stride);
+    const bool fa = w_a(w) == prev_out;
+    const bool fb = is_binary(op) && w_b(w) == prev_out;
+    return make_uint4(op | (fa ? F_FWD_A : 0u) | (fb ? F_FWD_B : 0u), w_a(w) * stride, w_b(w) * stride,
+                      w_out(w) * stride);
+}
+
+// Case generators: one case per (opcode, forwarding) combination.
+#define FREP_CASES_BINARY(X, OPC) \
+    X(OPC, false, false)          \
+    X(OPC, true, false)           \
+    X(OPC, false, true)           \
+    X(OPC, true, true)
+#define FREP_CASES_UNARY(X, OPC) \
+    X(OPC, false, false)         \
+    X(OPC, true, false)
+#define FREP_ALL_CASES(X)               \
+    FREP_CASES_BINARY(X, OP_MUL)        \
+    FREP_CASES_BINARY(X, OP_SUB)        \
+    FREP_CASES_BINARY(X, OP_ADD)        \
+    FREP_CASES_BINARY(X, OP_MAX)        \
+    FREP_CASES_BINARY(X, OP_MIN)        \
+    FREP_CASES_BINARY(X, OP_DIV)        \
+    FREP_CASES_UNARY(X, OP_COPY)        \
+    FREP_CASES_UNARY(X, OP_SQRT)        \
+    FREP_CASES_UNARY(X, OP_NEG)         \
+    FREP_CASES_UNARY(X, OP_SIN)         \
+    FREP_CASES_UNARY(X, OP_COS)         \
+    FREP_CASES_UNARY(X, OP_EXP)
 
 // Fetches the next chunk of work items for this warp. Returns the first item
 // of the chunk in *first and its size; 0 when the level is exhausted.
@@ -52,17 +136,67 @@ __device__ __forceinline__ uint32_t level_count(const TreeHeader* H, uint32_t le
     return (uint32_t)min((unsigned long long)H->node_count[level], cap);
 }
 
+// Stages the prefetched chunk `pre` (lane l of group q holds instruction
+// q*32 + l of the chunk), decoded with forwarding flags, into stage[]. The
+// first instruction of a chunk never forwards. Entries past the tape's end
+// decode to a flagless CONST, which is also the sentinel the interpreter reads
+// one past the last instruction.
+__device__ __forceinline__ void stage_chunk(uint4* stage, const uint64_t (&pre)[STAGE / 32], uint32_t row_bytes,
+                                            uint32_t lane) {
+    uint32_t prev_group_last = 0xFFFFFFFFu;
+#pragma unroll
+    for (int q = 0; q < (int)(STAGE / 32); q++) {
+        const uint32_t out = w_out(pre[q]);
+        uint32_t prev = __shfl_up_sync(0xFFFFFFFFu, out, 1);
+        if (lane == 0) prev = prev_group_last;
+        stage[q * 32 + lane] = decode(pre[q], prev, row_bytes);
+        prev_group_last = __shfl_sync(0xFFFFFFFFu, out, 31);
+    }
+}
+__device__ __forceinline__ void prefetch_chunk(uint64_t (&pre)[STAGE / 32], const uint64_t* tape, uint32_t base,
+                                               uint32_t n, uint32_t lane) {
+#pragma unroll
+    for (int q = 0; q < (int)(STAGE / 32); q++) {
+        const uint32_t i = base + q * 32 + lane;
+        pre[q] = i < n ? __ldcg(&tape[i]) : 0ull;
+    }
+}
+
+// One interval instruction with its operand sources fixed at compile time.
+// r: in = the previous instruction's result, out = this one's.
+template <int ROUND, uint32_t OP, bool FA, bool FB>
+__device__ __forceinline__ void iv_exec(const uint4 d, float2& r, uint32_t lane_base, uint32_t lane, uint2* mmb,
+                                        uint32_t& mm, uint32_t mm_cap) {
+    const float2 a = FA ? r : lds_f2(lane_base + d.y);
+    float2 b = make_float2(0.0f, 0.0f);
+    if constexpr (is_binary(OP)) b = FB ? r : lds_f2(lane_base + d.z);
+    r = iv_apply<ROUND>(OP, 0ull, a, b);
+    if constexpr (OP == OP_MIN || OP == OP_MAX) {
+        uint32_t c;
+        if constexpr (OP == OP_MIN) c = a.y < b.x ? MM_FIRST : (b.y < a.x ? MM_SECOND : MM_BOTH);
+        else c = a.y < b.x ? MM_SECOND : (b.y < a.x ? MM_FIRST : MM_BOTH);
+        const uint32_t b0 = __ballot_sync(0xFFFFFFFFu, c & 1u);
+        const uint32_t b1 = __ballot_sync(0xFFFFFFFFu, c & 2u);
+        if (lane == 0 && mm < mm_cap) mmb[mm] = make_uint2(b0, b1);
+        mm++;
+    }
+}
+
+// ---- interval level pass -------------------------------------------------------
+//
+// Per-warp shared memory: slots [n_slots][32] float2 | stage [STAGE] uint4 |
+// choice masks [mm_cap] uint2 | live [n_slots] u32.
 template <int ROUND, int WARPS>
 __global__ void __launch_bounds__(WARPS * 32)
 interval_level_kernel(LevelArgs p) {
     extern __shared__ __align__(16) unsigned char smem[];
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned char* wbase = smem + (size_t)warp * p.smem_per_warp;
-    float2* slots = reinterpret_cast<float2*>(wbase);
-    uint64_t* stage = reinterpret_cast<uint64_t*>(wbase + (size_t)p.n_slots * 256);
-    uint2* mmb = reinterpret_cast<uint2*>(wbase + (size_t)p.n_slots * 256 + 256);
-    uint32_t* live = reinterpret_cast<uint32_t*>(wbase + (size_t)p.n_slots * 256 + 256 + (size_t)p.mm_cap * 8);
-    const uint32_t live_words = (p.n_slots + 31) / 32;
+    const uint32_t lane_base = smem_addr(wbase) + lane * 8;
+    uint4* stage = reinterpret_cast<uint4*>(wbase + (size_t)p.n_slots * 256);
+    uint2* mmb = reinterpret_cast<uint2*>(wbase + (size_t)p.n_slots * 256 + (STAGE + 1) * 16);
+    uint32_t* live = reinterpret_cast<uint32_t*>(wbase + (size_t)p.n_slots * 256 + (STAGE + 1) * 16 + (size_t)p.mm_cap * 8);
+    if (lane == 0) stage[STAGE] = make_uint4(0u, 0u, 0u, 0u);  // sentinel past a full chunk
 
     TreeHeader* H = p.hdr;
     const uint32_t L = p.level;
@@ -75,8 +209,7 @@ interval_level_kernel(LevelArgs p) {
     const unsigned long long child_cap =
         p.node_cap > ofs_next ? (p.node_cap - ofs_next) / p.node_size_next : 0ull;
     const unsigned long long total = (unsigned long long)count * groups;
-    const uint32_t grid_warps = gridDim.x * WARPS;
-    const uint32_t chunk = chunk_for(total, grid_warps);
+    const uint32_t chunk = chunk_for(total, gridDim.x * WARPS);
     uint32_t* keep = p.keep_scratch + (size_t)(blockIdx.x * WARPS + warp) * p.keep_stride;
     const float cs = p.cell_size;
 
@@ -93,7 +226,7 @@ interval_level_kernel(LevelArgs p) {
             const uint32_t tape_idx = rec[0];
             const uint32_t ncx = rec[1], ncy = rec[2], ncz = rec[3];
             const uint64_t* tape = p.tapes + tape_idx + 1;
-            const uint32_t n = (uint32_t)p.tapes[tape_idx];
+            const uint32_t n = (uint32_t)__ldcg(&p.tapes[tape_idx]);
 
             const uint32_t cell = grp * 32 + lane;
             const uint32_t cz = cell % dim, cy = (cell / dim) % dim, cx = cell / (dim * dim);
@@ -102,43 +235,51 @@ interval_level_kernel(LevelArgs p) {
             const float lox = __fadd_rn(p.low[0], __fmul_rn((float)gx, cs));
             const float loy = __fadd_rn(p.low[1], __fmul_rn((float)gy, cs));
             const float loz = __fadd_rn(p.low[2], __fmul_rn((float)gz, cs));
-            slots[0 * 32 + lane] = make_float2(lox, __fadd_rn(lox, cs));
-            slots[1 * 32 + lane] = make_float2(loy, __fadd_rn(loy, cs));
-            slots[2 * 32 + lane] = make_float2(loz, __fadd_rn(loz, cs));
-            slots[3 * 32 + lane] = make_float2(p.tape_time, p.tape_time);
+            sts_f2(lane_base + 0 * 256, make_float2(lox, __fadd_rn(lox, cs)));
+            sts_f2(lane_base + 1 * 256, make_float2(loy, __fadd_rn(loy, cs)));
+            sts_f2(lane_base + 2 * 256, make_float2(loz, __fadd_rn(loz, cs)));
+            sts_f2(lane_base + 3 * 256, make_float2(p.tape_time, p.tape_time));
 
             // ---- forward interval pass (interval.comp:121-160) ----
             uint32_t mm = 0;
-            for (uint32_t base = 0; base < n; base += 32) {
-                const uint32_t m = min(32u, n - base);
+            float2 r = make_float2(0.0f, 0.0f);
+            uint64_t pre[STAGE / 32];
+            prefetch_chunk(pre, tape, 0, n, lane);
+            for (uint32_t base = 0; base < n; base += STAGE) {
+                const uint32_t m = min(STAGE, n - base);
                 __syncwarp();
-                if (lane < m) stage[lane] = tape[base + lane];
+                stage_chunk(stage, pre, 8, lane);
+                prefetch_chunk(pre, tape, base + STAGE, n, lane);
                 __syncwarp();
+                // r holds the previous instruction's result, so a forwarded
+                // operand costs nothing; the decode word of j+1 is read early.
+                const uint32_t sbase = smem_addr(stage);
+                uint4 dn = lds_u4(sbase);
                 for (uint32_t j = 0; j < m; j++) {
-                    const uint64_t w = stage[j];
-                    const uint32_t op = w_op(w);
-                    float2 a = make_float2(0.0f, 0.0f), b = a;
-                    if (op != OP_CONST) {
-                        a = slots[w_a(w) * 32 + lane];
-                        b = slots[w_b(w) * 32 + lane];
+                    const uint4 d = dn;
+                    dn = lds_u4(sbase + (j + 1) * 16);
+                    switch (d.x) {
+                        case OP_CONST: {
+                            const float c = __uint_as_float(d.y);
+                            r = make_float2(c, c);
+                            break;
+                        }
+#define FREP_IV_CASE(OPC, FA, FB)                                                      \
+    case OPC | (FA ? F_FWD_A : 0u) | (FB ? F_FWD_B : 0u):                              \
+        iv_exec<ROUND, OPC, FA, FB>(d, r, lane_base, lane, mmb, mm, p.mm_cap);         \
+        break;
+                        FREP_ALL_CASES(FREP_IV_CASE)
+#undef FREP_IV_CASE
+                        default: break;
                     }
-                    slots[w_out(w) * 32 + lane] = iv_apply<ROUND>(op, w, a, b);
-                    if (is_mm(op)) {
-                        uint32_t c;
-                        if (op == OP_MIN) c = a.y < b.x ? MM_FIRST : (b.y < a.x ? MM_SECOND : MM_BOTH);
-                        else c = a.y < b.x ? MM_SECOND : (b.y < a.x ? MM_FIRST : MM_BOTH);
-                        const uint32_t b0 = __ballot_sync(0xFFFFFFFFu, c & 1u);
-                        const uint32_t b1 = __ballot_sync(0xFFFFFFFFu, c & 2u);
-                        if (lane == 0 && mm < p.mm_cap) mmb[mm] = make_uint2(b0, b1);
-                        mm++;
-                    }
+                    sts_f2(lane_base + d.w, r);
                 }
             }
             __syncwarp();
             stat_work += 32ull * n;
 
             // ---- classification (voxelizer/main.comp:88-108) ----
-            const float2 d = slots[lane];
+            const float2 d = lds_f2(lane_base);
             const bool empty = d.x > 0.0f;
             const bool leaf = !empty && d.y < 0.0f;
             const bool amb = !empty && !leaf;
@@ -160,46 +301,49 @@ interval_level_kernel(LevelArgs p) {
             uint32_t child_tape = tape_idx;
             uint32_t child_len = n;
             if (ok_w && p.shorten) {
-                // ---- backward liveness (shorten.comp:148-186) ----
-                for (uint32_t wd = 0; wd < live_words; wd++) live[wd * 32 + lane] = 0u;
-                if (ok) live[lane] = 1u;  // slot 0 is the output
+                // ---- backward liveness (shorten.comp:148-186) on transposed bitsets:
+                // live[s] bit l = slot s is live for lane l. The kept-mask of an
+                // instruction is live[out]; then live[out] = 0 and the inputs its
+                // choice uses become live for the lanes that kept it.
+                for (uint32_t s = lane; s < p.n_slots; s += 32) live[s] = 0u;
+                __syncwarp();
+                if (lane == 0) live[0] = ok_w;
+                __syncwarp();
                 uint32_t kept = 0;
                 int mmi = (int)mm - 1;
                 for (int hi = (int)n; hi > 0; hi -= 32) {
                     const int lo = max(0, hi - 32);
                     const int m = hi - lo;
-                    __syncwarp();
-                    if ((int)lane < m) stage[lane] = tape[lo + lane];
-                    __syncwarp();
+                    // lane j holds instruction lo + j; walked from the top down
+                    const uint64_t mine = (int)lane < m ? __ldcg(&tape[lo + lane]) : 0ull;
+                    uint32_t my_keep = 0;
                     for (int j = m - 1; j >= 0; j--) {
-                        const uint64_t w = stage[j];
+                        const uint64_t w = __shfl_sync(0xFFFFFFFFu, mine, j);
                         const uint32_t op = w_op(w), o = w_out(w);
-                        uint32_t* lw = &live[(o >> 5) * 32 + lane];
-                        const uint32_t lv = *lw;
-                        const bool k = (lv >> (o & 31)) & 1u;
+                        const uint32_t k = live[o];
                         if (k) {
-                            *lw = lv & ~(1u << (o & 31));
-                            uint32_t c;
-                            if (op == OP_CONST) c = 0;
-                            else if (op == OP_ADD || op == OP_SUB || op == OP_MUL || op == OP_DIV) c = MM_BOTH;
-                            else if (is_mm(op)) {
+                            uint32_t first_m, second_m;
+                            if (op == OP_CONST) { first_m = 0u; second_m = 0u; }
+                            else if (op == OP_ADD || op == OP_SUB || op == OP_MUL || op == OP_DIV) {
+                                first_m = ~0u; second_m = ~0u;
+                            } else if (is_mm(op)) {
                                 const uint2 cb = mmb[mmi];
-                                c = ((cb.x >> lane) & 1u) | (((cb.y >> lane) & 1u) << 1);
-                            } else c = MM_FIRST;
-                            if (c & MM_FIRST) {
-                                const uint32_t s = w_a(w);
-                                live[(s >> 5) * 32 + lane] |= 1u << (s & 31);
+                                first_m = cb.x; second_m = cb.y;
+                            } else { first_m = ~0u; second_m = 0u; }
+                            __syncwarp();
+                            if (lane == 0) {
+                                live[o] = 0u;
+                                const uint32_t fa = k & first_m, sb = k & second_m;
+                                if (fa) live[w_a(w)] |= fa;
+                                if (sb) live[w_b(w)] |= sb;
                             }
-                            if (c & MM_SECOND) {
-                                const uint32_t s = w_b(w);
-                                live[(s >> 5) * 32 + lane] |= 1u << (s & 31);
-                            }
-                            kept++;
+                            __syncwarp();
+                            kept += (k >> lane) & 1u;
                         }
-                        const uint32_t kb = __ballot_sync(0xFFFFFFFFu, k);
-                        if (lane == 0) keep[lo + j] = kb;
+                        if ((int)lane == j) my_keep = k;
                         if (is_mm(op)) mmi--;
                     }
+                    if ((int)lane < m) keep[lo + lane] = my_keep;
                 }
                 __syncwarp();
 
@@ -222,34 +366,43 @@ interval_level_kernel(LevelArgs p) {
                 if (do_short && !tape_ok) atomicOr(&H->overflow, 2u);
                 const uint32_t short_w = __ballot_sync(0xFFFFFFFFu, tape_ok);
 
-                // ---- cooperative copy of each shortened tape (shorten.comp:193-221) ----
-                uint32_t pending = short_w;
-                while (pending) {
-                    const int sel = __ffs(pending) - 1;
-                    pending &= pending - 1;
-                    const unsigned long long dst = __shfl_sync(0xFFFFFFFFu, my_tape, sel);
-                    const uint32_t ksz = __shfl_sync(0xFFFFFFFFu, kept, sel);
-                    if (lane == 0) p.tapes[dst] = (uint64_t)ksz;
-                    uint32_t run = 0, mm_run = 0;
+                // ---- copy of the shortened tapes (shorten.comp:193-221) ----
+                // Chunk-outer: lane j holds instruction base + j, its keep mask
+                // and (for MIN/MAX) its choice masks; each output tape then takes
+                // one ballot + one coalesced store per chunk.
+                if (short_w) {
+                    if (tape_ok) p.tapes[my_tape] = (uint64_t)kept;
+                    uint32_t run = 0;  // lane L: instructions written so far to its own tape
+                    uint32_t mm_run = 0;
                     for (uint32_t b = 0; b < n; b += 32) {
                         const uint32_t idx = b + lane;
                         const bool valid = idx < n;
-                        uint64_t w = valid ? tape[idx] : 0ull;
-                        const bool kb = valid && ((keep[idx] >> sel) & 1u);
+                        const uint64_t w = valid ? __ldcg(&tape[idx]) : 0ull;
+                        const uint32_t kmask = valid ? keep[idx] : 0u;
                         const bool ism = valid && is_mm(w_op(w));
                         const uint32_t mball = __ballot_sync(0xFFFFFFFFu, ism);
-                        if (kb && ism) {
-                            const uint2 cb = mmb[mm_run + __popc(mball & lanemask_lt())];
-                            const uint32_t c = ((cb.x >> sel) & 1u) | (((cb.y >> sel) & 1u) << 1);
-                            if (c == MM_FIRST) {
-                                w = (w & ~0xFFull) | OP_COPY;
-                            } else if (c == MM_SECOND) {  // COPY of B; the B field is kept
-                                w = (w & ~0xFFull & ~(0xFFFFull << 32)) | OP_COPY | ((uint64_t)w_b(w) << 32);
+                        uint2 cb = make_uint2(0u, 0u);
+                        if (ism) cb = mmb[mm_run + __popc(mball & lanemask_lt())];
+                        uint32_t pending = short_w;
+                        while (pending) {
+                            const int sel = __ffs(pending) - 1;
+                            pending &= pending - 1;
+                            const bool kb = (kmask >> sel) & 1u;
+                            uint64_t wo = w;
+                            if (kb && ism) {
+                                const uint32_t c = ((cb.x >> sel) & 1u) | (((cb.y >> sel) & 1u) << 1);
+                                if (c == MM_FIRST) {
+                                    wo = (w & ~0xFFull) | OP_COPY;
+                                } else if (c == MM_SECOND) {  // COPY of B; the B field is kept
+                                    wo = (w & ~0xFFull & ~(0xFFFFull << 32)) | OP_COPY | ((uint64_t)w_b(w) << 32);
+                                }
                             }
+                            const uint32_t kball = __ballot_sync(0xFFFFFFFFu, kb);
+                            const unsigned long long dst = __shfl_sync(0xFFFFFFFFu, my_tape, sel);
+                            const uint32_t r = __shfl_sync(0xFFFFFFFFu, run, sel);
+                            if (kb) p.tapes[dst + 1 + r + __popc(kball & lanemask_lt())] = wo;
+                            if ((int)lane == sel) run += __popc(kball);
                         }
-                        const uint32_t kball = __ballot_sync(0xFFFFFFFFu, kb);
-                        if (kb) p.tapes[dst + 1 + run + __popc(kball & lanemask_lt())] = w;
-                        run += __popc(kball);
                         mm_run += __popc(mball);
                     }
                 }
@@ -291,27 +444,86 @@ interval_level_kernel(LevelArgs p) {
     }
 }
 
-// Last level: the leaf bit is the sign of the point value at the cell's low
-// corner (voxelize_point, main.comp:74-83; tape_eval_point, point.comp:2-63).
-template <int WARPS>
+// ---- point level pass (the last level) ---------------------------------------------
+//
+// The leaf bit is the sign of the point value at the cell's low corner
+// (voxelize_point, main.comp:74-83; tape_eval_point, point.comp:2-63).
+// Each lane evaluates K cells at once (cells grp*32K + k*32 + lane; K = 4, or
+// 2 for nodes too small for 4), so one decoded instruction drives 32*K
+// evaluations and a lane's slot row is one K-float vector. A tape that fits one
+// staged chunk stays staged across consecutive items of the same node.
+template <int K>
+struct alignas(4 * K) FK {
+    float v[K];
+};
+
+template <int K>
+__device__ __forceinline__ FK<K> lds_k(uint32_t a) {
+    FK<K> r;
+    if constexpr (K == 4) {
+        const float4 v = lds_f4(a);
+        r.v[0] = v.x; r.v[1] = v.y; r.v[2] = v.z; r.v[3] = v.w;
+    } else {
+        const float2 v = lds_f2(a);
+        r.v[0] = v.x; r.v[1] = v.y;
+    }
+    return r;
+}
+template <int K>
+__device__ __forceinline__ void sts_k(uint32_t a, const FK<K>& r) {
+    if constexpr (K == 4) sts_f4(a, make_float4(r.v[0], r.v[1], r.v[2], r.v[3]));
+    else sts_f2(a, make_float2(r.v[0], r.v[1]));
+}
+
+// One point instruction with its operand sources fixed at compile time.
+// r: in = the previous instruction's result, out = this one's.
+template <int K, uint32_t OP, bool FA, bool FB>
+__device__ __forceinline__ void pt_exec(const uint4 d, FK<K>& r, uint32_t lane_base) {
+    const FK<K> a = FA ? r : lds_k<K>(lane_base + d.y);
+    FK<K> b;
+    if constexpr (is_binary(OP)) b = FB ? r : lds_k<K>(lane_base + d.z);
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        float v;
+        if constexpr (OP == OP_MUL) v = __fmul_rn(a.v[k], b.v[k]);
+        else if constexpr (OP == OP_SUB) v = __fsub_rn(a.v[k], b.v[k]);
+        else if constexpr (OP == OP_ADD) v = __fadd_rn(a.v[k], b.v[k]);
+        else if constexpr (OP == OP_MAX) v = max_sel(a.v[k], b.v[k]);
+        else if constexpr (OP == OP_MIN) v = min_sel(a.v[k], b.v[k]);
+        else if constexpr (OP == OP_COPY) v = a.v[k];
+        else if constexpr (OP == OP_NEG) v = -a.v[k];
+        else if constexpr (OP == OP_SQRT) v = __fsqrt_rn(a.v[k]);
+        else if constexpr (OP == OP_DIV) v = __fdiv_rn(a.v[k], b.v[k]);
+        else if constexpr (OP == OP_SIN) v = frep_sinf(a.v[k]);
+        else if constexpr (OP == OP_COS) v = frep_cosf(a.v[k]);
+        else v = frep_expf(a.v[k]);  // OP_EXP
+        r.v[k] = v;
+    }
+}
+
+template <int WARPS, int K>
 __global__ void __launch_bounds__(WARPS * 32)
 point_level_kernel(LevelArgs p) {
     extern __shared__ __align__(16) unsigned char smem[];
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned char* wbase = smem + (size_t)warp * p.smem_per_warp;
-    float* slots = reinterpret_cast<float*>(wbase);
-    uint64_t* stage = reinterpret_cast<uint64_t*>(wbase + (size_t)p.n_slots * 128);
+    constexpr uint32_t ROW = 4 * K;  // bytes per lane per slot
+    const uint32_t lane_base = smem_addr(wbase) + lane * ROW;
+    uint4* stage = reinterpret_cast<uint4*>(wbase + (size_t)p.n_slots * 32 * ROW);
+    if (lane == 0) stage[STAGE] = make_uint4(0u, 0u, 0u, 0u);  // sentinel past a full chunk
 
     TreeHeader* H = p.hdr;
     const uint32_t L = p.level;
     const uint32_t dim = p.dim;
-    const uint32_t groups = dim * dim * dim / 32;
+    const uint32_t words = dim * dim * dim / 32;      // mask words per node
+    const uint32_t groups = words / K;                // items per node
     const uint32_t count = level_count(H, L, p.node_cap, p.node_size);
     const unsigned long long ofs_l = H->node_ofs[L];
     const unsigned long long total = (unsigned long long)count * groups;
     const uint32_t chunk = chunk_for(total, gridDim.x * WARPS);
     const float cs = p.cell_size;
     unsigned long long stat_work = 0;
+    uint32_t staged_tape = 0xFFFFFFFFu;  // tape whose whole body is in `stage`
 
     unsigned long long first;
     uint32_t got;
@@ -322,40 +534,73 @@ point_level_kernel(LevelArgs p) {
             uint32_t* rec = p.nodes + ofs_l + (size_t)node * p.node_size;
             const uint32_t tape_idx = rec[0];
             const uint64_t* tape = p.tapes + tape_idx + 1;
-            const uint32_t n = (uint32_t)p.tapes[tape_idx];
-            const uint32_t cell = grp * 32 + lane;
-            const uint32_t cz = cell % dim, cy = (cell / dim) % dim, cx = cell / (dim * dim);
-            const uint32_t gx = rec[1] * dim + cx, gy = rec[2] * dim + cy, gz = rec[3] * dim + cz;
-            slots[0 * 32 + lane] = __fadd_rn(p.low[0], __fmul_rn((float)gx, cs));
-            slots[1 * 32 + lane] = __fadd_rn(p.low[1], __fmul_rn((float)gy, cs));
-            slots[2 * 32 + lane] = __fadd_rn(p.low[2], __fmul_rn((float)gz, cs));
-            slots[3 * 32 + lane] = p.tape_time;
-            for (uint32_t base = 0; base < n; base += 32) {
-                const uint32_t m = min(32u, n - base);
-                __syncwarp();
-                if (lane < m) stage[lane] = tape[base + lane];
-                __syncwarp();
+            const uint32_t n = (uint32_t)__ldcg(&p.tapes[tape_idx]);
+            const uint32_t ncx = rec[1], ncy = rec[2], ncz = rec[3];
+            FK<K> px, py, pz, pt;
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                const uint32_t cell = grp * 32 * K + k * 32 + lane;
+                const uint32_t cz = cell % dim, cy = (cell / dim) % dim, cx = cell / (dim * dim);
+                px.v[k] = __fadd_rn(p.low[0], __fmul_rn((float)(ncx * dim + cx), cs));
+                py.v[k] = __fadd_rn(p.low[1], __fmul_rn((float)(ncy * dim + cy), cs));
+                pz.v[k] = __fadd_rn(p.low[2], __fmul_rn((float)(ncz * dim + cz), cs));
+                pt.v[k] = p.tape_time;
+            }
+            sts_k<K>(lane_base + 0 * 32 * ROW, px);
+            sts_k<K>(lane_base + 1 * 32 * ROW, py);
+            sts_k<K>(lane_base + 2 * 32 * ROW, pz);
+            sts_k<K>(lane_base + 3 * 32 * ROW, pt);
+            const bool resident = n <= STAGE && staged_tape == tape_idx;
+            FK<K> r;
+#pragma unroll
+            for (int k = 0; k < K; k++) r.v[k] = 0.0f;
+            uint64_t pre[STAGE / 32];
+            if (!resident) prefetch_chunk(pre, tape, 0, n, lane);
+            for (uint32_t base = 0; base < n; base += STAGE) {
+                const uint32_t m = min(STAGE, n - base);
+                if (!resident) {
+                    __syncwarp();
+                    stage_chunk(stage, pre, ROW, lane);
+                    prefetch_chunk(pre, tape, base + STAGE, n, lane);
+                    __syncwarp();
+                }
+                // r holds the previous instruction's result, so a forwarded
+                // operand costs nothing; the decode word of j+1 is read early.
+                const uint32_t sbase = smem_addr(stage);
+                uint4 dn = lds_u4(sbase);
                 for (uint32_t j = 0; j < m; j++) {
-                    const uint64_t w = stage[j];
-                    const uint32_t op = w_op(w);
-                    float a = 0.0f, b = 0.0f;
-                    if (op != OP_CONST) {
-                        a = slots[w_a(w) * 32 + lane];
-                        b = slots[w_b(w) * 32 + lane];
+                    const uint4 d = dn;
+                    dn = lds_u4(sbase + (j + 1) * 16);
+                    switch (d.x) {
+                        case OP_CONST:
+#pragma unroll
+                            for (int k = 0; k < K; k++) r.v[k] = __uint_as_float(d.y);
+                            break;
+#define FREP_PT_CASE(OPC, FA, FB)                    \
+    case OPC | (FA ? F_FWD_A : 0u) | (FB ? F_FWD_B : 0u): \
+        pt_exec<K, OPC, FA, FB>(d, r, lane_base);   \
+        break;
+                        FREP_ALL_CASES(FREP_PT_CASE)
+#undef FREP_PT_CASE
+                        default: break;
                     }
-                    slots[w_out(w) * 32 + lane] = pt_apply(op, w, a, b);
+                    sts_k<K>(lane_base + d.w, r);
                 }
             }
+            staged_tape = n <= STAGE ? tape_idx : 0xFFFFFFFFu;
             __syncwarp();
-            stat_work += 32ull * n;
-            const uint32_t leaf_w = __ballot_sync(0xFFFFFFFFu, slots[lane] < 0.0f);
-            if (lane == 0) {
-                rec[4 + grp] = leaf_w;
-                rec[4 + groups + grp] = 0u;  // the unused second mask word range
+            stat_work += 32ull * K * n;
+            const FK<K> d = lds_k<K>(lane_base);
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                const uint32_t leaf_w = __ballot_sync(0xFFFFFFFFu, d.v[k] < 0.0f);
+                if (lane == 0) {
+                    rec[4 + grp * K + k] = leaf_w;
+                    rec[4 + words + grp * K + k] = 0u;  // the unused second mask word range
+                }
             }
         }
     }
-    // stat_work is warp-uniform: lane 0 reports it.
     if (lane == 0 && stat_work) atomicAdd(&H->cell_instr[L], stat_work);
 }
 
@@ -370,6 +615,7 @@ __global__ void tree_init_kernel(TreeHeader* H, uint32_t* nodes, uint32_t root_n
         H->tape_size_sum[l] = l == 0 ? root_n : 0;
         H->tape_size_max[l] = l == 0 ? root_n : 0;
         H->cell_instr[l] = 0;
+        H->fp32_ops[l] = 0;
     }
     if (t == 0) {
         H->tape_top = root_words;
@@ -382,12 +628,35 @@ __global__ void tree_init_kernel(TreeHeader* H, uint32_t* nodes, uint32_t root_n
     }
 }
 
+// Work accounting (run on demand, outside the level passes): for every node of
+// `level`, the op-weighted FP32 work of evaluating its tape on all its cells,
+// with the interval weights (interior levels) or the point weights (last level).
+__global__ void count_ops_kernel(TreeHeader* H, const uint32_t* nodes, const uint64_t* tapes,
+                                 unsigned long long node_cap, uint32_t level, uint32_t node_size,
+                                 uint32_t cells, int point) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t count = level_count(H, level, node_cap, node_size);
+    const unsigned long long ofs = H->node_ofs[level];
+    const uint8_t* wt = point ? kPointOps : kIntervalOps;
+    unsigned long long sum = 0;
+    for (uint32_t node = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); node < count;
+         node += gridDim.x * (blockDim.x / 32)) {
+        const uint32_t tidx = nodes[ofs + (size_t)node * node_size];
+        const uint32_t n = (uint32_t)tapes[tidx];
+        uint32_t s = 0;
+        for (uint32_t i = lane; i < n; i += 32) s += wt[w_op(tapes[tidx + 1 + i]) & 15];
+        sum += (unsigned long long)s * cells;
+    }
+    for (int off = 16; off > 0; off >>= 1) sum += __shfl_down_sync(0xFFFFFFFFu, sum, off);
+    if (lane == 0 && sum) atomicAdd(&H->fp32_ops[level], sum);
+}
+
 }  // namespace dev
 
 namespace {
 
-template <typename K>
-cudaError_t occupancy(K kernel, int threads, size_t smem, int* blocks) {
+template <typename Kern>
+cudaError_t occupancy(Kern kernel, int threads, size_t smem, int* blocks) {
     cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
@@ -403,12 +672,26 @@ cudaError_t occupancy(K kernel, int threads, size_t smem, int* blocks) {
 
 }  // namespace
 
-cudaError_t plan_levels(uint32_t n_slots, uint32_t mm_cap, int rounding, LevelPlan* plan) {
-    const uint32_t live_words = (n_slots + 31) / 32;
-    const uint32_t iv = (n_slots * 256 + 256 + mm_cap * 8 + live_words * 128 + 15) / 16 * 16;
-    const uint32_t pt = (n_slots * 128 + 256 + 15) / 16 * 16;
-    plan->smem_per_warp = iv;
+// Cells per lane of the point pass: a node of dim^3 cells is dim^3 / (32 K)
+// items, so K must divide the node's dim^3 / 32 mask words. With dim a
+// multiple of 4 that count is even; it is a multiple of 4 when dim is a
+// multiple of 8.
+static int point_k(uint32_t dim) { return (dim * dim * dim / 32) % 4 == 0 ? 4 : 2; }
+
+template <int K>
+static cudaError_t plan_point(uint32_t n_slots, LevelPlan* plan) {
+    const uint32_t pt = (uint32_t)(n_slots * 32 * 4 * K + (dev::STAGE + 1) * 16 + 15) / 16 * 16;
     plan->point_smem_per_warp = pt;
+    plan->point_warps_per_block = 4ull * pt <= 200 * 1024 ? 4 : 1;
+    if (pt > 227 * 1024) return cudaErrorInvalidValue;
+    if (plan->point_warps_per_block == 4)
+        return occupancy(dev::point_level_kernel<4, K>, 128, 4 * pt, &plan->point_blocks);
+    return occupancy(dev::point_level_kernel<1, K>, 32, pt, &plan->point_blocks);
+}
+
+cudaError_t plan_levels(uint32_t n_slots, uint32_t mm_cap, uint32_t last_dim, int rounding, LevelPlan* plan) {
+    const uint32_t iv = (n_slots * 256 + (dev::STAGE + 1) * 16 + mm_cap * 8 + n_slots * 4 + 15) / 16 * 16;
+    plan->smem_per_warp = iv;
     // Four warps per block when they fit in shared memory, else one.
     const bool four = 4ull * iv <= 200 * 1024;
     plan->warps_per_block = four ? 4 : 1;
@@ -422,11 +705,8 @@ cudaError_t plan_levels(uint32_t n_slots, uint32_t mm_cap, int rounding, LevelPl
                      : occupancy(dev::interval_level_kernel<0, 1>, 32, iv, &plan->blocks);
     }
     if (e != cudaSuccess) return e;
-    plan->point_warps_per_block = 4ull * pt <= 200 * 1024 ? 4 : 1;
-    if (pt > 227 * 1024) return cudaErrorInvalidValue;
-    if (plan->point_warps_per_block == 4)
-        return occupancy(dev::point_level_kernel<4>, 128, 4 * pt, &plan->point_blocks);
-    return occupancy(dev::point_level_kernel<1>, 32, pt, &plan->point_blocks);
+    plan->point_k = point_k(last_dim);
+    return plan->point_k == 4 ? plan_point<4>(n_slots, plan) : plan_point<2>(n_slots, plan);
 }
 
 cudaError_t launch_tree_init(dev::TreeHeader* hdr, uint32_t* nodes, uint32_t root_n_instr,
@@ -440,10 +720,15 @@ cudaError_t launch_level(const LevelArgs& a, const LevelPlan& plan, int rounding
     if (last) {
         LevelArgs b = a;
         b.smem_per_warp = plan.point_smem_per_warp;
-        if (plan.point_warps_per_block == 4)
-            dev::point_level_kernel<4><<<plan.point_blocks, 128, 4 * plan.point_smem_per_warp, stream>>>(b);
-        else
-            dev::point_level_kernel<1><<<plan.point_blocks, 32, plan.point_smem_per_warp, stream>>>(b);
+        const int w4 = plan.point_warps_per_block == 4;
+        const size_t smem = (size_t)plan.point_warps_per_block * plan.point_smem_per_warp;
+        if (plan.point_k == 4) {
+            if (w4) dev::point_level_kernel<4, 4><<<plan.point_blocks, 128, smem, stream>>>(b);
+            else dev::point_level_kernel<1, 4><<<plan.point_blocks, 32, smem, stream>>>(b);
+        } else {
+            if (w4) dev::point_level_kernel<4, 2><<<plan.point_blocks, 128, smem, stream>>>(b);
+            else dev::point_level_kernel<1, 2><<<plan.point_blocks, 32, smem, stream>>>(b);
+        }
         return cudaGetLastError();
     }
     LevelArgs b = a;
@@ -457,6 +742,14 @@ cudaError_t launch_level(const LevelArgs& a, const LevelPlan& plan, int rounding
         if (rounding) dev::interval_level_kernel<1, 1><<<plan.blocks, 32, smem, stream>>>(b);
         else dev::interval_level_kernel<0, 1><<<plan.blocks, 32, smem, stream>>>(b);
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_count_ops(dev::TreeHeader* hdr, const uint32_t* nodes, const uint64_t* tapes,
+                             unsigned long long node_cap, uint32_t level, uint32_t node_size,
+                             uint32_t cells, bool point, cudaStream_t stream) {
+    dev::count_ops_kernel<<<1184, 256, 0, stream>>>(hdr, nodes, tapes, node_cap, level, node_size, cells,
+                                                    point ? 1 : 0);
     return cudaGetLastError();
 }
 

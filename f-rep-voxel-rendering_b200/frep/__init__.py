@@ -237,6 +237,11 @@ class VoxelStorage:
         L.check(L.lib().frep_tree_work(self._tree, arr))
         return list(arr[: self.grid_levels])
 
+    def fp32_ops(self) -> list[int]:
+        arr = (C.c_uint64 * L.MAX_LEVELS)()
+        L.check(L.lib().frep_tree_fp32_ops(self._tree, arr))
+        return list(arr[: self.grid_levels])
+
     def set_profiling(self, enable: bool = True) -> None:
         L.check(L.lib().frep_tree_set_profiling(self._tree, 1 if enable else 0))
 

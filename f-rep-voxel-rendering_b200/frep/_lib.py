@@ -93,6 +93,7 @@ _SIGS = {
     "frep_voxelize": (C.c_int, [_P, _P, _P, C.c_float, _P]),
     "frep_tree_sync": (C.c_int, [_P, C.POINTER(TreeInfo)]),
     "frep_tree_work": (C.c_int, [_P, _P]),
+    "frep_tree_fp32_ops": (C.c_int, [_P, _P]),
     "frep_tree_set_profiling": (C.c_int, [_P, C.c_int]),
     "frep_tree_timings": (C.c_int, [_P, _P]),
     "frep_tree_copy_nodes": (C.c_int, [_P, _P, C.c_uint64]),

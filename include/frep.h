@@ -196,6 +196,11 @@ frep_status frep_tree_timings(frep_tree* tree, float ms[FREP_MAX_LEVELS]);
 /* Cell-instructions evaluated per level by the last voxelization: the number
  * of (cell, tape instruction) pairs the interval and point passes executed. */
 frep_status frep_tree_work(frep_tree* tree, uint64_t cell_instr[FREP_MAX_LEVELS]);
+/* Op-weighted FP32 work per level of the last voxelization: for every
+ * (cell, instruction) pair, the number of FP32 operations of the reference's
+ * interval formula for that opcode (interval levels) or 1 per arithmetic
+ * instruction (the last, point level). The roofline numerator. */
+frep_status frep_tree_fp32_ops(frep_tree* tree, uint64_t ops[FREP_MAX_LEVELS]);
 frep_status frep_tree_copy_tapes(frep_tree* tree, uint64_t* dst, uint64_t n_words);
 
 /* ---------------------------------------------------------------------------

@@ -60,6 +60,19 @@ def test_random_csg_perspective_with_shadows(ctx, n, seed, dims):
     np.testing.assert_array_equal(d_rgba, o_rgba)
 
 
+@pytest.mark.parametrize("dims", [(8, 12), (4, 16), (12, 8), (16, 32)])
+def test_last_level_dims(ctx, dims):
+    """Node sizes that select different cells-per-lane and mask layouts."""
+    sc = _small_random(20, 8, list(dims))
+    vs = device_tree(ctx, sc, rounding=1)
+    exp = vs.export()
+    orc = oracle_tree(sc, vs.tape, rounding=1)
+    assert compare_trees(exp, orc) == []
+    d_rgba, d_hits, o_rgba, o_hits = render_both(ctx, vs, orc, sc, frep.Lights())
+    assert compare_hits(d_hits, o_hits, exp, orc) == []
+    np.testing.assert_array_equal(d_rgba, o_rgba)
+
+
 def test_wide_tape_scene(ctx):
     """More than 256 constants: only the wide encoding can hold this tape."""
     sc = _small_random(160, 9, [16, 8])
