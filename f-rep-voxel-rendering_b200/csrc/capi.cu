@@ -8,6 +8,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -576,3 +577,126 @@ frep_status frep_render(frep_ctx* ctx, const frep_tree* tree, const frep_camera*
 }
 
 }  // extern "C"
+
+// ---- voxelization without allocation -------------------------------------------
+//
+// Some callers cannot allocate device memory at the moment they voxelize: a
+// renderer running under a fixed memory budget that was reserved up front, a
+// real-time frame loop that must not hit cudaMalloc's implicit device
+// synchronisation, or a host application that hands every buffer to this
+// library from its own allocator. frep_voxelize allocates the interval pass's
+// per-warp scratch (and a pinned staging buffer) on first use; the entry point
+// below instead takes that scratch from a fixed array in device memory that
+// exists from the moment the library is loaded, and copies the root tape
+// straight from the tape object, so it makes no allocation at all.
+namespace {
+
+// 8 MiB of keep-ballot scratch (one 32-bit lane mask per tape instruction per
+// resident warp). Every GPU that loads the library holds it until exit.
+constexpr uint64_t kStaticScratchWords = 2ull << 20;
+static __device__ __align__(256) uint32_t g_static_scratch[kStaticScratchWords];
+
+std::mutex g_static_mutex;
+uint32_t* g_static_scratch_addr[256] = {};  // device address, per device ordinal
+
+// Looks up the array's device address once per device (the device must be
+// current): in host code the symbol is only a stand-in for the device array.
+frep_status static_scratch_for(int device, uint32_t** out) {
+    std::lock_guard<std::mutex> lock(g_static_mutex);
+    if (device < 0 || device >= 256) return fail(FREP_ERR_INVALID_ARG, "device ordinal %d out of range", device);
+    if (!g_static_scratch_addr[device]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(static scratch)");
+        g_static_scratch_addr[device] = static_cast<uint32_t*>(p);
+    }
+    *out = g_static_scratch_addr[device];
+    return FREP_OK;
+}
+
+}  // namespace
+
+extern "C" frep_status frep_voxelize_static_scratch(frep_ctx* ctx, frep_tree* tree, const frep_tape* tape,
+                                                    float tape_time, void* stream_ptr) {
+    if (!ctx || !tree || !tape) return fail(FREP_ERR_INVALID_ARG, "frep_voxelize_static_scratch: null argument");
+    if (tree->ctx != ctx)
+        return fail(FREP_ERR_INVALID_ARG, "frep_voxelize_static_scratch: tree belongs to another context");
+    cudaStream_t stream = (cudaStream_t)stream_ptr;
+    FREP_CUDA(cudaSetDevice(ctx->device));
+    uint32_t* scratch = nullptr;
+    frep_status st = static_scratch_for(ctx->device, &scratch);
+    if (st != FREP_OK) return st;
+
+    const uint32_t n = (uint32_t)tape->ct.instrs.size();
+    const uint32_t n_slots = std::max<uint32_t>(tape->ct.n_slots, 4);
+    const uint64_t root_words = tape->record.size();
+    if (root_words > tree->tape_cap)
+        return fail(FREP_ERR_CAPACITY, "frep_voxelize_static_scratch: root tape (%llu words) exceeds the tape pool",
+                    (unsigned long long)root_words);
+    if (!tree->plan_valid || tree->plan_slots != n_slots || tree->plan_mm != tape->ct.n_minmax ||
+        tree->plan_round != tree->opts.rounding) {
+        cudaError_t e = frep::plan_levels(n_slots, tape->ct.n_minmax, tree->grid.dims[tree->grid.levels - 1],
+                                          (int)tree->opts.rounding, &tree->plan);
+        if (e == cudaErrorInvalidValue)
+            return fail(FREP_ERR_UNSUPPORTED, "frep_voxelize_static_scratch: %u slots / %u min-max ops exceed shared memory",
+                        n_slots, tape->ct.n_minmax);
+        if (e != cudaSuccess) return cuda_fail(e, "plan_levels");
+        tree->plan_valid = true;
+        tree->plan_slots = n_slots;
+        tree->plan_mm = tape->ct.n_minmax;
+        tree->plan_round = tree->opts.rounding;
+    }
+    // Each resident warp owns keep_stride words of the array; launch only as
+    // many blocks as fit, and refuse tapes too long for even one block.
+    const uint32_t keep_stride = (uint32_t)align_up(std::max<uint32_t>(n, 1), 32);
+    const uint64_t per_block = (uint64_t)tree->plan.warps_per_block * keep_stride;
+    if (per_block > kStaticScratchWords)
+        return fail(FREP_ERR_UNSUPPORTED,
+                    "frep_voxelize_static_scratch: a root tape of %u instructions needs %llu scratch words per block; "
+                    "the static scratch holds %llu (at most %llu instructions)",
+                    n, (unsigned long long)per_block, (unsigned long long)kStaticScratchWords,
+                    (unsigned long long)(kStaticScratchWords / tree->plan.warps_per_block / 32 * 32));
+    frep::LevelPlan plan = tree->plan;
+    plan.blocks = (int)std::min<uint64_t>((uint64_t)plan.blocks, kStaticScratchWords / per_block);
+
+    // The root tape goes straight from the tape object (pageable host memory).
+    FREP_CUDA(cudaMemcpyAsync(tree->tapes, tape->record.data(), root_words * 8, cudaMemcpyHostToDevice, stream));
+    tree->n_slots = n_slots;
+    tree->mm_cap = tape->ct.n_minmax;
+    tree->root_n = n;
+    tree->root_words = (uint32_t)root_words;
+    tree->stream = stream;
+
+    cudaError_t e = frep::launch_tree_init(tree->hdr, tree->nodes, n, (uint32_t)root_words, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "tree_init_kernel");
+    const frep_grid& g = tree->grid;
+    for (uint32_t l = 0; l < g.levels; l++) {
+        const bool last = l == g.levels - 1;
+        frep::LevelArgs a{};
+        a.hdr = tree->hdr;
+        a.nodes = tree->nodes;
+        a.node_cap = tree->node_cap;
+        a.tapes = tree->tapes;
+        a.tape_cap = tree->tape_cap;
+        a.keep_scratch = scratch;
+        a.keep_stride = keep_stride;
+        a.level = l;
+        a.levels = g.levels;
+        a.dim = g.dims[l];
+        a.dim_next = last ? 0 : g.dims[l + 1];
+        a.node_size = tree->node_size[l];
+        a.node_size_next = last ? 1 : tree->node_size[l + 1];
+        a.cell_size = tree->cell_size[l];
+        a.low[0] = g.low_vertex[0];
+        a.low[1] = g.low_vertex[1];
+        a.low[2] = g.low_vertex[2];
+        a.tape_time = tape_time;
+        a.n_slots = n_slots;
+        a.mm_cap = std::max<uint32_t>(tape->ct.n_minmax, 1);
+        a.shorten = tree->opts.shorten;
+        e = frep::launch_level(a, plan, (int)tree->opts.rounding, last, stream);
+        if (e != cudaSuccess) return cuda_fail(e, "level kernel");
+    }
+    tree->voxelized = true;
+    return FREP_OK;
+}

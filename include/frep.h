@@ -163,6 +163,27 @@ void frep_tree_destroy(frep_tree* tree);
 frep_status frep_voxelize(frep_ctx* ctx, frep_tree* tree, const frep_tape* tape, float tape_time,
                           void* stream);
 
+/* Same voxelization as frep_voxelize, for callers that cannot allocate device
+ * memory when they voxelize (a fixed budget reserved up front, a frame loop
+ * that must not hit cudaMalloc's implicit synchronisation, or an application
+ * whose allocator owns every buffer). It makes no allocation: the interval
+ * pass's per-warp scratch is an 8 MiB array in the library's device image
+ * instead of a cudaMalloc'd buffer, and the root tape is copied straight from
+ * `tape` (pageable memory: the call returns once the driver has staged it).
+ * No counterpart in the reference.
+ *   - Limit: a root tape of at most 524288 instructions (8 MiB / 4 bytes / 4
+ *     warps per block; 2097152 when a block holds one warp); longer tapes
+ *     return FREP_ERR_UNSUPPORTED. Tapes of more than 4096 instructions run on
+ *     fewer blocks than frep_voxelize uses, so they take longer.
+ *   - Its first call on a device looks up the array's device address; make that
+ *     first call before any stream capture.
+ *   - Every call on a device shares the one array: calls whose work overlaps
+ *     on the GPU (different streams, no ordering between them) race. Nothing
+ *     in it needs to start at zero; each call overwrites what it reads.
+ * The tree, its pools and the tape must still be created by the caller. */
+frep_status frep_voxelize_static_scratch(frep_ctx* ctx, frep_tree* tree, const frep_tape* tape,
+                                         float tape_time, void* stream);
+
 /* Waits for the tree's stream and reads its header. Replaces the per-level
  * childCount readback (voxelizer.cpp:326-328) and PrintStats (:442-478). */
 typedef struct frep_tree_info {
