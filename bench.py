@@ -230,7 +230,7 @@ def run_ours(args, world, rank, local):
     info = vs.sync()
     fp32_ops = vs.fp32_ops()
     cell_instr = vs.work()
-    launches_per_step = 1 + vs.grid_levels + 1  # init + level passes + render
+    launches_per_step = 1 + 2 * vs.grid_levels + 1  # init + (work scan + level pass) per level + render
 
     # ---- device-resident timing (value) -------------------------------------
     torch.cuda.synchronize()

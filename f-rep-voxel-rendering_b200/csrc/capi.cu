@@ -12,14 +12,10 @@
 #include <string>
 #include <vector>
 
-#include "device_common.cuh"
-#include "frep.h"
-#include "kernels.h"
-#include "tape_compiler.h"
+#include "capi_internal.h"
 
-using frep::CompiledTape;
-
-namespace {
+namespace frep {
+namespace detail {
 
 thread_local std::string g_error;
 
@@ -37,60 +33,13 @@ frep_status cuda_fail(cudaError_t e, const char* what) {
     return fail(FREP_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
 }
 
-#define FREP_CUDA(call)                                              \
-    do {                                                             \
-        cudaError_t e_ = (call);                                     \
-        if (e_ != cudaSuccess) return cuda_fail(e_, #call);          \
-    } while (0)
+}  // namespace detail
+}  // namespace frep
 
-uint64_t align_up(uint64_t v, uint64_t a) { return (v + a - 1) / a * a; }
-
-}  // namespace
-
-struct frep_tape {
-    CompiledTape ct;
-    std::vector<uint64_t> record;  // [n_instr][instrs...] padded to 16 words
-    void build_record() {
-        record.assign(align_up(1 + ct.instrs.size(), frep::dev::TAPE_ALIGN_WORDS), 0);
-        record[0] = ct.instrs.size();
-        std::memcpy(&record[1], ct.instrs.data(), ct.instrs.size() * 8);
-    }
-};
-
-struct frep_ctx {
-    int device = 0;
-    uint64_t budget = 0;
-    uint64_t used = 0;
-    int sm_count = 0;
-};
-
-struct frep_tree {
-    frep_ctx* ctx = nullptr;
-    frep_grid grid{};
-    frep_voxelize_opts opts{};
-    float cell_size[FREP_MAX_LEVELS] = {};
-    uint32_t node_size[FREP_MAX_LEVELS] = {};
-    frep::dev::TreeHeader* hdr = nullptr;
-    uint32_t* nodes = nullptr;
-    uint64_t* tapes = nullptr;
-    uint64_t node_cap = 0, tape_cap = 0;
-    uint32_t* keep = nullptr;
-    uint64_t keep_words = 0;
-    uint64_t bytes = 0;
-    // staging for the root tape upload
-    uint64_t* staging = nullptr;
-    uint64_t staging_words = 0;
-    cudaEvent_t upload_done = nullptr;
-    // the root tape of the last voxelization
-    uint32_t n_slots = 4, mm_cap = 0, root_n = 0, root_words = 0;
-    bool plan_valid = false;
-    uint32_t plan_slots = 0, plan_mm = 0, plan_round = 0;
-    frep::LevelPlan plan{};
-    cudaStream_t stream = nullptr;
-    bool voxelized = false;
-    bool profile = false;
-    cudaEvent_t ev[FREP_MAX_LEVELS + 1] = {};
-};
+using frep::detail::align_up;
+using frep::detail::cuda_fail;
+using frep::detail::fail;
+using frep::detail::g_error;
 
 extern "C" {
 
@@ -251,18 +200,47 @@ frep_status frep_tree_create(frep_ctx* ctx, const frep_grid* grid, const frep_vo
                     (unsigned long long)bytes, (unsigned long long)avail);
     }
     cudaError_t e = cudaMalloc(&t->hdr, sizeof(frep::dev::TreeHeader));
+    if (e == cudaSuccess) e = cudaMalloc(&t->d_small, 64);
     if (e == cudaSuccess) e = cudaMalloc(&t->nodes, t->node_cap * 4);
     if (e == cudaSuccess) e = cudaMalloc(&t->tapes, t->tape_cap * 8);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&t->upload_done, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         cudaGetLastError();
         cudaFree(t->hdr);
+        cudaFree(t->d_small);
         cudaFree(t->nodes);
         cudaFree(t->tapes);
         delete t;
         return fail(FREP_ERR_OOM, "frep_tree_create: cudaMalloc failed (%s)", cudaGetErrorString(e));
     }
-    cudaMemset(t->hdr, 0, sizeof(frep::dev::TreeHeader));
+    // The header's static part: where the pools are and the grid.
+    frep::dev::TreeHeader h{};
+    h.nodes = t->nodes;
+    h.tapes = t->tapes;
+    h.node_cap = t->node_cap;
+    h.tape_cap = t->tape_cap;
+    h.levels = grid->levels;
+    h.shorten = t->opts.shorten;
+    for (uint32_t l = 0; l < grid->levels; l++) {
+        h.dims[l] = grid->dims[l];
+        h.node_size[l] = t->node_size[l];
+        h.cell_size[l] = t->cell_size[l];
+    }
+    for (int k = 0; k < 3; k++) h.low[k] = grid->low_vertex[k];
+    t->d_self = reinterpret_cast<frep::dev::TreeHeader**>(t->d_small);
+    t->d_prefix = t->d_small + 1;
+    t->d_cursor = t->d_small + 3;
+    cudaError_t ce = cudaMemcpy(t->hdr, &h, sizeof(h), cudaMemcpyHostToDevice);
+    if (ce == cudaSuccess) ce = cudaMemcpy(t->d_self, &t->hdr, sizeof(void*), cudaMemcpyHostToDevice);
+    if (ce != cudaSuccess) {
+        cudaFree(t->hdr);
+        cudaFree(t->d_small);
+        cudaFree(t->nodes);
+        cudaFree(t->tapes);
+        cudaEventDestroy(t->upload_done);
+        delete t;
+        return cuda_fail(ce, "frep_tree_create: header upload");
+    }
     t->bytes = bytes;
     ctx->used += bytes;
     *out = t;
@@ -275,6 +253,7 @@ void frep_tree_destroy(frep_tree* t) {
     if (t->stream) cudaStreamSynchronize(t->stream);
     else cudaDeviceSynchronize();
     cudaFree(t->hdr);
+    cudaFree(t->d_small);
     cudaFree(t->nodes);
     cudaFree(t->tapes);
     cudaFree(t->keep);
@@ -285,6 +264,63 @@ void frep_tree_destroy(frep_tree* t) {
     t->ctx->used -= std::min(t->ctx->used, t->bytes);
     delete t;
 }
+
+}  // extern "C"
+
+namespace {
+
+// Plans the level passes of `tree` for `tape` (cached on the tree).
+frep_status ensure_plan(frep_tree* tree, const frep_tape* tape, const char* who) {
+    const uint32_t n_slots = std::max<uint32_t>(tape->ct.n_slots, 4);
+    if (tree->plan_valid && tree->plan_slots == n_slots && tree->plan_mm == tape->ct.n_minmax &&
+        tree->plan_round == tree->opts.rounding)
+        return FREP_OK;
+    const int k = frep::point_k_for(tree->grid.dims[tree->grid.levels - 1]);
+    cudaError_t e = frep::plan_levels(n_slots, tape->ct.n_minmax, k, (int)tree->opts.rounding, &tree->plan);
+    if (e == cudaErrorInvalidValue)
+        return fail(FREP_ERR_UNSUPPORTED, "%s: %u slots / %u min-max ops exceed shared memory", who, n_slots,
+                    tape->ct.n_minmax);
+    if (e != cudaSuccess) return cuda_fail(e, "plan_levels");
+    tree->plan_valid = true;
+    tree->plan_slots = n_slots;
+    tree->plan_mm = tape->ct.n_minmax;
+    tree->plan_round = tree->opts.rounding;
+    return FREP_OK;
+}
+
+// Enqueues init + every level pass of one tree whose root tape is already at
+// word 0 of its pool. `plan` may narrow the grid (the static-scratch path).
+frep_status enqueue_tree_levels(frep_tree* tree, const frep_tape* tape, float tape_time, uint32_t* keep,
+                                uint32_t keep_stride, const frep::LevelPlan& plan, cudaStream_t stream) {
+    cudaError_t e = frep::launch_tree_init(tree->d_self, 1, nullptr, tape_time, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "tree_init_kernel");
+    const frep_grid& g = tree->grid;
+    if (tree->profile) FREP_CUDA(cudaEventRecord(tree->ev[0], stream));
+    frep::LevelLaunch a{};
+    a.trees = tree->d_self;
+    a.prefix = tree->d_prefix;
+    a.cursor = tree->d_cursor;
+    a.n_trees = 1;
+    a.keep_scratch = keep;
+    a.keep_stride = keep_stride;
+    a.n_slots = std::max<uint32_t>(tape->ct.n_slots, 4);
+    a.mm_cap = std::max<uint32_t>(tape->ct.n_minmax, 1);
+    for (uint32_t l = 0; l < g.levels; l++) {
+        const bool point = l == g.levels - 1;
+        a.level = l;
+        e = frep::launch_level_scan(a, point, plan.point_k, stream);
+        if (e != cudaSuccess) return cuda_fail(e, "level_scan_kernel");
+        e = frep::launch_level(a, plan, (int)tree->opts.rounding, point, stream);
+        if (e != cudaSuccess) return cuda_fail(e, "level kernel");
+        if (tree->profile) FREP_CUDA(cudaEventRecord(tree->ev[l + 1], stream));
+    }
+    tree->voxelized = true;
+    return FREP_OK;
+}
+
+}  // namespace
+
+extern "C" {
 
 frep_status frep_voxelize(frep_ctx* ctx, frep_tree* tree, const frep_tape* tape, float tape_time,
                           void* stream_ptr) {
@@ -298,19 +334,8 @@ frep_status frep_voxelize(frep_ctx* ctx, frep_tree* tree, const frep_tape* tape,
     if (root_words > tree->tape_cap)
         return fail(FREP_ERR_CAPACITY, "frep_voxelize: root tape (%llu words) exceeds the tape pool", (unsigned long long)root_words);
 
-    // Launch plan for this slot / MIN-MAX count.
-    if (!tree->plan_valid || tree->plan_slots != n_slots || tree->plan_mm != tape->ct.n_minmax ||
-        tree->plan_round != tree->opts.rounding) {
-        cudaError_t e = frep::plan_levels(n_slots, tape->ct.n_minmax, tree->grid.dims[tree->grid.levels - 1],
-                                          (int)tree->opts.rounding, &tree->plan);
-        if (e == cudaErrorInvalidValue)
-            return fail(FREP_ERR_UNSUPPORTED, "frep_voxelize: %u slots / %u min-max ops exceed shared memory", n_slots, tape->ct.n_minmax);
-        if (e != cudaSuccess) return cuda_fail(e, "plan_levels");
-        tree->plan_valid = true;
-        tree->plan_slots = n_slots;
-        tree->plan_mm = tape->ct.n_minmax;
-        tree->plan_round = tree->opts.rounding;
-    }
+    frep_status pst = ensure_plan(tree, tape, "frep_voxelize");
+    if (pst != FREP_OK) return pst;
     // Per-warp keep-ballot scratch: one word per instruction of the longest tape.
     const uint32_t keep_stride = (uint32_t)align_up(std::max<uint32_t>(n, 1), 32);
     const uint64_t keep_words = (uint64_t)tree->plan.blocks * tree->plan.warps_per_block * keep_stride;
@@ -351,40 +376,7 @@ frep_status frep_voxelize(frep_ctx* ctx, frep_tree* tree, const frep_tape* tape,
     tree->root_words = (uint32_t)root_words;
     tree->stream = stream;
 
-    cudaError_t e = frep::launch_tree_init(tree->hdr, tree->nodes, n, (uint32_t)root_words, stream);
-    if (e != cudaSuccess) return cuda_fail(e, "tree_init_kernel");
-    const frep_grid& g = tree->grid;
-    if (tree->profile) FREP_CUDA(cudaEventRecord(tree->ev[0], stream));
-    for (uint32_t l = 0; l < g.levels; l++) {
-        const bool last = l == g.levels - 1;
-        frep::LevelArgs a{};
-        a.hdr = tree->hdr;
-        a.nodes = tree->nodes;
-        a.node_cap = tree->node_cap;
-        a.tapes = tree->tapes;
-        a.tape_cap = tree->tape_cap;
-        a.keep_scratch = tree->keep;
-        a.keep_stride = keep_stride;
-        a.level = l;
-        a.levels = g.levels;
-        a.dim = g.dims[l];
-        a.dim_next = last ? 0 : g.dims[l + 1];
-        a.node_size = tree->node_size[l];
-        a.node_size_next = last ? 1 : tree->node_size[l + 1];
-        a.cell_size = tree->cell_size[l];
-        a.low[0] = g.low_vertex[0];
-        a.low[1] = g.low_vertex[1];
-        a.low[2] = g.low_vertex[2];
-        a.tape_time = tape_time;
-        a.n_slots = n_slots;
-        a.mm_cap = std::max<uint32_t>(tape->ct.n_minmax, 1);
-        a.shorten = tree->opts.shorten;
-        e = frep::launch_level(a, tree->plan, (int)tree->opts.rounding, last, stream);
-        if (e != cudaSuccess) return cuda_fail(e, "level kernel");
-        if (tree->profile) FREP_CUDA(cudaEventRecord(tree->ev[l + 1], stream));
-    }
-    tree->voxelized = true;
-    return FREP_OK;
+    return enqueue_tree_levels(tree, tape, tape_time, tree->keep, keep_stride, tree->plan, stream);
 }
 
 frep_status frep_tree_sync(frep_tree* tree, frep_tree_info* info) {
@@ -513,18 +505,22 @@ H3 normalize3(H3 v) {
 }
 }  // namespace
 
-frep_status frep_render(frep_ctx* ctx, const frep_tree* tree, const frep_camera* cam,
-                        const frep_lights* lights, float tape_time, const frep_image* out,
-                        void* stream_ptr) {
-    if (!ctx || !tree || !cam || !lights || !out) return fail(FREP_ERR_INVALID_ARG, "frep_render: null argument");
+}  // extern "C"
+
+namespace frep {
+namespace detail {
+
+frep_status fill_render_args(const frep_tree* tree, const frep_camera* cam, const frep_lights* lights,
+                             float tape_time, const frep_image* out, RenderArgs* args) {
+    if (!tree || !cam || !lights || !out) return fail(FREP_ERR_INVALID_ARG, "frep_render: null argument");
     if (!tree->voxelized) return fail(FREP_ERR_INVALID_ARG, "frep_render: the tree has not been voxelized");
     if (cam->width == 0 || cam->height == 0 || cam->projection > 1)
         return fail(FREP_ERR_INVALID_ARG, "frep_render: bad camera");
     if (lights->count > FREP_MAX_LIGHTS) return fail(FREP_ERR_INVALID_ARG, "frep_render: too many lights");
     if (((uintptr_t)out->rgba8 & 3) || ((uintptr_t)out->hits & 3))
         return fail(FREP_ERR_INVALID_ARG, "frep_render: output buffers must be 4-byte aligned");
-    FREP_CUDA(cudaSetDevice(ctx->device));
-    frep::RenderArgs a{};
+    RenderArgs& a = *args;
+    a = RenderArgs{};
     a.hdr = tree->hdr;
     a.nodes = tree->nodes;
     a.tapes = tree->tapes;
@@ -570,6 +566,22 @@ frep_status frep_render(frep_ctx* ctx, const frep_tree* tree, const frep_camera*
     a.n_slots = tree->n_slots;
     a.rgba8 = out->rgba8;
     a.hits = out->hits;
+    return FREP_OK;
+}
+
+}  // namespace detail
+}  // namespace frep
+
+extern "C" {
+
+frep_status frep_render(frep_ctx* ctx, const frep_tree* tree, const frep_camera* cam,
+                        const frep_lights* lights, float tape_time, const frep_image* out,
+                        void* stream_ptr) {
+    if (!ctx || !tree) return fail(FREP_ERR_INVALID_ARG, "frep_render: null argument");
+    FREP_CUDA(cudaSetDevice(ctx->device));
+    frep::RenderArgs a{};
+    frep_status st = frep::detail::fill_render_args(tree, cam, lights, tape_time, out, &a);
+    if (st != FREP_OK) return st;
     cudaError_t e = frep::launch_render(a, (cudaStream_t)stream_ptr);
     if (e == cudaErrorInvalidValue) return fail(FREP_ERR_UNSUPPORTED, "frep_render: more than 1024 slots");
     if (e != cudaSuccess) return cuda_fail(e, "render_kernel");
@@ -633,19 +645,8 @@ extern "C" frep_status frep_voxelize_static_scratch(frep_ctx* ctx, frep_tree* tr
     if (root_words > tree->tape_cap)
         return fail(FREP_ERR_CAPACITY, "frep_voxelize_static_scratch: root tape (%llu words) exceeds the tape pool",
                     (unsigned long long)root_words);
-    if (!tree->plan_valid || tree->plan_slots != n_slots || tree->plan_mm != tape->ct.n_minmax ||
-        tree->plan_round != tree->opts.rounding) {
-        cudaError_t e = frep::plan_levels(n_slots, tape->ct.n_minmax, tree->grid.dims[tree->grid.levels - 1],
-                                          (int)tree->opts.rounding, &tree->plan);
-        if (e == cudaErrorInvalidValue)
-            return fail(FREP_ERR_UNSUPPORTED, "frep_voxelize_static_scratch: %u slots / %u min-max ops exceed shared memory",
-                        n_slots, tape->ct.n_minmax);
-        if (e != cudaSuccess) return cuda_fail(e, "plan_levels");
-        tree->plan_valid = true;
-        tree->plan_slots = n_slots;
-        tree->plan_mm = tape->ct.n_minmax;
-        tree->plan_round = tree->opts.rounding;
-    }
+    frep_status pst = ensure_plan(tree, tape, "frep_voxelize_static_scratch");
+    if (pst != FREP_OK) return pst;
     // Each resident warp owns keep_stride words of the array; launch only as
     // many blocks as fit, and refuse tapes too long for even one block.
     const uint32_t keep_stride = (uint32_t)align_up(std::max<uint32_t>(n, 1), 32);
@@ -667,36 +668,5 @@ extern "C" frep_status frep_voxelize_static_scratch(frep_ctx* ctx, frep_tree* tr
     tree->root_words = (uint32_t)root_words;
     tree->stream = stream;
 
-    cudaError_t e = frep::launch_tree_init(tree->hdr, tree->nodes, n, (uint32_t)root_words, stream);
-    if (e != cudaSuccess) return cuda_fail(e, "tree_init_kernel");
-    const frep_grid& g = tree->grid;
-    for (uint32_t l = 0; l < g.levels; l++) {
-        const bool last = l == g.levels - 1;
-        frep::LevelArgs a{};
-        a.hdr = tree->hdr;
-        a.nodes = tree->nodes;
-        a.node_cap = tree->node_cap;
-        a.tapes = tree->tapes;
-        a.tape_cap = tree->tape_cap;
-        a.keep_scratch = scratch;
-        a.keep_stride = keep_stride;
-        a.level = l;
-        a.levels = g.levels;
-        a.dim = g.dims[l];
-        a.dim_next = last ? 0 : g.dims[l + 1];
-        a.node_size = tree->node_size[l];
-        a.node_size_next = last ? 1 : tree->node_size[l + 1];
-        a.cell_size = tree->cell_size[l];
-        a.low[0] = g.low_vertex[0];
-        a.low[1] = g.low_vertex[1];
-        a.low[2] = g.low_vertex[2];
-        a.tape_time = tape_time;
-        a.n_slots = n_slots;
-        a.mm_cap = std::max<uint32_t>(tape->ct.n_minmax, 1);
-        a.shorten = tree->opts.shorten;
-        e = frep::launch_level(a, plan, (int)tree->opts.rounding, last, stream);
-        if (e != cudaSuccess) return cuda_fail(e, "level kernel");
-    }
-    tree->voxelized = true;
-    return FREP_OK;
+    return enqueue_tree_levels(tree, tape, tape_time, scratch, keep_stride, plan, stream);
 }

@@ -18,17 +18,31 @@ constexpr uint32_t MAX_LEVELS = 8;
 constexpr uint32_t MAX_DDA_STEPS = 1u << 16;      // bound on every DDA loop
 constexpr uint32_t TAPE_ALIGN_WORDS = 16;         // tape records start on 128-byte lines
 
-// Device-resident state of one tree (one per frep_tree). Counters are reset by
-// the init kernel at the start of every voxelization.
+// Device-resident state of one tree (one per frep_tree). The first block is
+// written once when the tree is created; the rest is reset by the init kernel
+// at the start of every voxelization. Level passes read a tree entirely from
+// here, so one launch can serve many trees.
 struct TreeHeader {
+    // ---- static: set at creation ----
+    uint32_t* nodes;                           // node pool
+    uint64_t* tapes;                           // tape pool
+    unsigned long long node_cap;               // u32 words
+    unsigned long long tape_cap;               // u64 words
+    uint32_t levels;
+    uint32_t shorten;
+    uint32_t dims[MAX_LEVELS];
+    uint32_t node_size[MAX_LEVELS];            // u32 words
+    float cell_size[MAX_LEVELS];
+    float low[3];
+    // ---- per voxelization ----
+    float tape_time;
     uint32_t node_count[MAX_LEVELS];           // interiorNodeCount
-    unsigned long long work_cursor[MAX_LEVELS]; // dynamic work fetch per level
     unsigned long long node_ofs[MAX_LEVELS];   // u32 words
     unsigned long long tape_top;               // u64 words
     unsigned long long tape_size_sum[MAX_LEVELS];
     uint32_t tape_size_max[MAX_LEVELS];
     unsigned long long cell_instr[MAX_LEVELS]; // cell-instructions evaluated per level
-    unsigned long long fp32_ops[MAX_LEVELS];   // op-weighted FP32 work per level (see op_weight)
+    unsigned long long fp32_ops[MAX_LEVELS];   // op-weighted FP32 work per level (count_ops_kernel)
     uint32_t overflow;                         // bit 0 node pool, bit 1 tape pool
     uint32_t status;                           // reserved for bounded-wait failures
 };

@@ -8,45 +8,53 @@ namespace dev {
 struct TreeHeader;
 }
 
-// Arguments of one level pass (voxelizer/main.comp's ParamsBuffer, made
-// per-launch and device-resident where the reference read it back on the host).
-struct LevelArgs {
-    dev::TreeHeader* hdr;
-    uint32_t* nodes;
-    unsigned long long node_cap;     // u32 words
-    uint64_t* tapes;
-    unsigned long long tape_cap;     // u64 words
-    uint32_t* keep_scratch;          // per-warp keep ballots (global scratch)
-    uint32_t keep_stride;            // u32 words per warp (>= longest tape)
-    uint32_t level, levels;
-    uint32_t dim, dim_next;
-    uint32_t node_size, node_size_next;
-    float cell_size;
-    float low[3];
-    float tape_time;
-    uint32_t n_slots;                // slot-file entries per lane
-    uint32_t mm_cap;                 // MIN/MAX choice entries per warp
-    uint32_t shorten;
-    uint32_t smem_per_warp;          // bytes
+// One level launch over a batch of trees (a single tree is a batch of one).
+// The scan kernel fills `prefix` (work items before each tree, for the trees
+// this launch serves) and resets `cursor`; the level kernel then hands out
+// items of every tree from that one cursor.
+struct LevelLaunch {
+    dev::TreeHeader* const* trees;     // device array of n_trees header pointers
+    unsigned long long* prefix;        // device, n_trees + 1 entries
+    unsigned long long* cursor;        // device work cursor
+    uint32_t n_trees;
+    uint32_t level;
+    uint32_t* keep_scratch;            // per-warp keep masks (global scratch)
+    uint32_t keep_stride;              // u32 words per warp (>= longest tape)
+    uint32_t n_slots;                  // slot-file rows per lane (max over the batch)
+    uint32_t mm_cap;                   // MIN/MAX choice entries per warp (max over the batch)
+    uint32_t smem_per_warp;            // bytes (set by launch_level from the plan)
 };
 
 // Launch geometry of the level passes for one (slot count, MIN/MAX count).
 struct LevelPlan {
     int warps_per_block;
-    int blocks;                      // persistent grid
+    int blocks;                        // persistent grid
     uint32_t smem_per_warp;
-    int point_k;                     // cells per lane in the point pass
+    int point_k;                       // cells per lane in the point pass
     int point_warps_per_block;
     int point_blocks;
     uint32_t point_smem_per_warp;
 };
 
-cudaError_t plan_levels(uint32_t n_slots, uint32_t mm_cap, uint32_t last_dim, int rounding,
-                        LevelPlan* plan);
-cudaError_t launch_tree_init(dev::TreeHeader* hdr, uint32_t* nodes, uint32_t root_n_instr,
-                             uint32_t root_words, cudaStream_t stream);
-cudaError_t launch_level(const LevelArgs& a, const LevelPlan& plan, int rounding, bool last,
-                         cudaStream_t stream);
+// Cells per lane the point pass uses for a last level of this dim.
+int point_k_for(uint32_t dim);
+cudaError_t plan_levels(uint32_t n_slots, uint32_t mm_cap, int point_k, int rounding, LevelPlan* plan);
+
+// Resets the headers of n trees (tape time from `tape_times`, or `tape_time`
+// when it is null) and writes their root nodes. Each tree's root tape must
+// already be at word 0 of its tape pool.
+cudaError_t launch_tree_init(dev::TreeHeader* const* trees, uint32_t n, const float* tape_times, float tape_time,
+                             cudaStream_t stream);
+// Same for a batch whose root tapes are staged in one device buffer: tree i's
+// record is words [offsets[i], offsets[i+1]) of `staged`; it is copied to
+// word 0 of the tree's pool first. tape_times has n entries.
+cudaError_t launch_tree_init_staged(dev::TreeHeader* const* trees, uint32_t n, const uint64_t* staged,
+                                    const unsigned long long* offsets, const float* tape_times,
+                                    cudaStream_t stream);
+// Work prefix of `level` over the batch, for interval (point = false) or
+// point passes with `point_k` cells per lane.
+cudaError_t launch_level_scan(const LevelLaunch& a, bool point, int point_k, cudaStream_t stream);
+cudaError_t launch_level(const LevelLaunch& a, const LevelPlan& plan, int rounding, bool point, cudaStream_t stream);
 
 // Op-weighted work of every node of `level` (interval or point weights),
 // added to the header's fp32_ops[level].
@@ -81,5 +89,9 @@ struct RenderArgs {
 };
 
 cudaError_t launch_render(const RenderArgs& a, cudaStream_t stream);
+// Renders n frames in one launch: args is a device array of n RenderArgs,
+// max_w / max_h bound every frame's size.
+cudaError_t launch_render_batch(const RenderArgs* args, uint32_t n, uint32_t max_w, uint32_t max_h,
+                                uint32_t max_slots, cudaStream_t stream);
 
 }  // namespace frep

@@ -205,10 +205,7 @@ struct HitRecord {  // == frep_hit
 };
 
 template <int NS>
-__global__ void __launch_bounds__(64) render_kernel(const RenderArgs A) {
-    const uint32_t x = blockIdx.x * 8 + (threadIdx.x & 7);
-    const uint32_t y = blockIdx.y * 8 + (threadIdx.x >> 3);
-    if (x >= A.width || y >= A.height) return;
+__device__ __forceinline__ void render_pixel(const RenderArgs& A, uint32_t x, uint32_t y) {
     Tree T;
     T.nodes = A.nodes;
     T.a = &A;
@@ -290,6 +287,24 @@ __global__ void __launch_bounds__(64) render_kernel(const RenderArgs A) {
     }
 }
 
+template <int NS>
+__global__ void __launch_bounds__(64) render_kernel(const RenderArgs A) {
+    const uint32_t x = blockIdx.x * 8 + (threadIdx.x & 7);
+    const uint32_t y = blockIdx.y * 8 + (threadIdx.x >> 3);
+    if (x >= A.width || y >= A.height) return;
+    render_pixel<NS>(A, x, y);
+}
+
+// Many frames in one launch: blockIdx.z selects the frame.
+template <int NS>
+__global__ void __launch_bounds__(64) render_batch_kernel(const RenderArgs* args) {
+    const RenderArgs& A = args[blockIdx.z];
+    const uint32_t x = blockIdx.x * 8 + (threadIdx.x & 7);
+    const uint32_t y = blockIdx.y * 8 + (threadIdx.x >> 3);
+    if (x >= A.width || y >= A.height) return;
+    render_pixel<NS>(A, x, y);
+}
+
 }  // namespace dev
 
 cudaError_t launch_render(const RenderArgs& a, cudaStream_t stream) {
@@ -301,6 +316,21 @@ cudaError_t launch_render(const RenderArgs& a, cudaStream_t stream) {
     else if (ns <= 256) dev::render_kernel<256><<<grid, 64, 0, stream>>>(a);
     else if (ns <= 512) dev::render_kernel<512><<<grid, 64, 0, stream>>>(a);
     else if (ns <= 1024) dev::render_kernel<1024><<<grid, 64, 0, stream>>>(a);
+    else return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_render_batch(const RenderArgs* args, uint32_t n, uint32_t max_w, uint32_t max_h,
+                                uint32_t max_slots, cudaStream_t stream) {
+    if (n == 0) return cudaSuccess;
+    if (n > 65535) return cudaErrorInvalidValue;
+    const dim3 grid((max_w + 7) / 8, (max_h + 7) / 8, n);
+    if (max_slots <= 32) dev::render_batch_kernel<32><<<grid, 64, 0, stream>>>(args);
+    else if (max_slots <= 64) dev::render_batch_kernel<64><<<grid, 64, 0, stream>>>(args);
+    else if (max_slots <= 128) dev::render_batch_kernel<128><<<grid, 64, 0, stream>>>(args);
+    else if (max_slots <= 256) dev::render_batch_kernel<256><<<grid, 64, 0, stream>>>(args);
+    else if (max_slots <= 512) dev::render_batch_kernel<512><<<grid, 64, 0, stream>>>(args);
+    else if (max_slots <= 1024) dev::render_batch_kernel<1024><<<grid, 64, 0, stream>>>(args);
     else return cudaErrorInvalidValue;
     return cudaGetLastError();
 }

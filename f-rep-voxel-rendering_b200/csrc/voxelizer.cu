@@ -21,7 +21,10 @@
 //     one more; shortened tapes are written by the whole warp, 32 instructions
 //     per coalesced store.
 // Items are fetched in chunks from a device counter, so a level pass needs no
-// host round trip: the node count of level l is read on the device.
+// host round trip: the node count of level l is read on the device. One launch
+// serves a whole batch of trees: a scan kernel lays the trees' items end to end
+// and a warp resolves each item to its tree (binary search, cached per warp),
+// so idle warps steal work from any scene of the batch.
 #include "device_common.cuh"
 #include "kernels.h"
 
@@ -136,6 +139,58 @@ __device__ __forceinline__ uint32_t level_count(const TreeHeader* H, uint32_t le
     return (uint32_t)min((unsigned long long)H->node_count[level], cap);
 }
 
+// Largest tree index i with prefix[i] <= item (prefix[0] = 0 <= item < prefix[n]).
+__device__ __forceinline__ uint32_t find_tree(const unsigned long long* prefix, uint32_t n, unsigned long long item) {
+    uint32_t lo = 0, hi = n;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldcg(&prefix[mid]) <= item) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__host__ __device__ inline int point_k_of(uint32_t dim) { return (dim * dim * dim / 32) % 4 == 0 ? 4 : 2; }
+
+// What a level pass needs of one tree, read from its header when a warp
+// moves on to that tree.
+struct LevelTree {
+    TreeHeader* H;
+    uint32_t* nodes;
+    uint64_t* tapes;
+    unsigned long long tape_cap, ofs_l, ofs_next, child_cap;
+    uint32_t dim, node_size, node_size_next, shorten;
+    float cs, lx, ly, lz, tt;
+};
+
+__device__ __forceinline__ LevelTree load_tree(TreeHeader* H, uint32_t L, bool point) {
+    LevelTree t;
+    t.H = H;
+    t.nodes = H->nodes;
+    t.tapes = H->tapes;
+    t.tape_cap = H->tape_cap;
+    t.dim = H->dims[L];
+    t.node_size = H->node_size[L];
+    t.ofs_l = H->node_ofs[L];
+    t.shorten = H->shorten;
+    t.cs = H->cell_size[L];
+    t.lx = H->low[0];
+    t.ly = H->low[1];
+    t.lz = H->low[2];
+    t.tt = H->tape_time;
+    if (!point) {
+        t.node_size_next = H->node_size[L + 1];
+        t.ofs_next = H->node_ofs[L + 1];  // written by the scan kernel
+        const unsigned long long cap = H->node_cap;
+        t.child_cap = cap > t.ofs_next ? (cap - t.ofs_next) / t.node_size_next : 0ull;
+    } else {
+        t.node_size_next = 1;
+        t.ofs_next = 0;
+        t.child_cap = 0;
+    }
+    return t;
+}
+
 // Stages the prefetched chunk `pre` (lane l of group q holds instruction
 // q*32 + l of the chunk), decoded with forwarding flags, into stage[]. The
 // first instruction of a chunk never forwards. Entries past the tape's end
@@ -188,7 +243,7 @@ __device__ __forceinline__ void iv_exec(const uint4 d, float2& r, uint32_t lane_
 // choice masks [mm_cap] uint2 | live [n_slots] u32.
 template <int ROUND, int WARPS>
 __global__ void __launch_bounds__(WARPS * 32)
-interval_level_kernel(LevelArgs p) {
+interval_level_kernel(LevelLaunch p) {
     extern __shared__ __align__(16) unsigned char smem[];
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned char* wbase = smem + (size_t)warp * p.smem_per_warp;
@@ -198,47 +253,70 @@ interval_level_kernel(LevelArgs p) {
     uint32_t* live = reinterpret_cast<uint32_t*>(wbase + (size_t)p.n_slots * 256 + (STAGE + 1) * 16 + (size_t)p.mm_cap * 8);
     if (lane == 0) stage[STAGE] = make_uint4(0u, 0u, 0u, 0u);  // sentinel past a full chunk
 
-    TreeHeader* H = p.hdr;
     const uint32_t L = p.level;
-    const uint32_t dim = p.dim;
-    const uint32_t groups = dim * dim * dim / 32;
-    const uint32_t count = level_count(H, L, p.node_cap, p.node_size);
-    const unsigned long long ofs_l = H->node_ofs[L];
-    const unsigned long long ofs_next = ofs_l + (unsigned long long)count * p.node_size;
-    if (blockIdx.x == 0 && threadIdx.x == 0) H->node_ofs[L + 1] = ofs_next;
-    const unsigned long long child_cap =
-        p.node_cap > ofs_next ? (p.node_cap - ofs_next) / p.node_size_next : 0ull;
-    const unsigned long long total = (unsigned long long)count * groups;
+    const unsigned long long total = __ldcg(&p.prefix[p.n_trees]);
     const uint32_t chunk = chunk_for(total, gridDim.x * WARPS);
     uint32_t* keep = p.keep_scratch + (size_t)(blockIdx.x * WARPS + warp) * p.keep_stride;
-    const float cs = p.cell_size;
 
+    // The tree of the current item, and its statistics so far (flushed to its
+    // header when the warp moves to another tree: stats_buf, main.comp:146-147).
+    LevelTree T{};
+    unsigned long long t_lo = 0, t_hi = 0;
+    bool have_tree = false;
     unsigned long long stat_sum = 0, stat_work = 0;
     uint32_t stat_max = 0;
+    auto flush = [&]() {
+        unsigned long long ssum = stat_sum;
+        uint32_t smax = stat_max;
+        for (int off = 16; off > 0; off >>= 1) {
+            ssum += __shfl_down_sync(0xFFFFFFFFu, ssum, off);
+            smax = max(smax, __shfl_down_sync(0xFFFFFFFFu, smax, off));
+        }
+        if (lane == 0) {
+            if (ssum) atomicAdd(&T.H->tape_size_sum[L + 1], ssum);
+            if (smax) atomicMax(&T.H->tape_size_max[L + 1], smax);
+            if (stat_work) atomicAdd(&T.H->cell_instr[L], stat_work);
+        }
+        stat_sum = 0;
+        stat_max = 0;
+        stat_work = 0;
+    };
 
     unsigned long long first;
     uint32_t got;
-    while ((got = fetch_items(&H->work_cursor[L], total, chunk, &first)) != 0) {
+    while ((got = fetch_items(p.cursor, total, chunk, &first)) != 0) {
         for (uint32_t it = 0; it < got; it++) {
             const unsigned long long item = first + it;
-            const uint32_t node = (uint32_t)(item / groups), grp = (uint32_t)(item % groups);
-            uint32_t* rec = p.nodes + ofs_l + (size_t)node * p.node_size;
+            if (!have_tree || item >= t_hi) {
+                if (have_tree) flush();
+                const uint32_t ti = find_tree(p.prefix, p.n_trees, item);
+                t_lo = __ldcg(&p.prefix[ti]);
+                t_hi = __ldcg(&p.prefix[ti + 1]);
+                T = load_tree(p.trees[ti], L, false);
+                have_tree = true;
+            }
+            const uint32_t dim = T.dim;
+            const uint32_t groups = dim * dim * dim / 32;
+            const unsigned long long local = item - t_lo;
+            const uint32_t node = (uint32_t)(local / groups), grp = (uint32_t)(local % groups);
+            uint32_t* rec = T.nodes + T.ofs_l + (size_t)node * T.node_size;
             const uint32_t tape_idx = rec[0];
             const uint32_t ncx = rec[1], ncy = rec[2], ncz = rec[3];
-            const uint64_t* tape = p.tapes + tape_idx + 1;
-            const uint32_t n = (uint32_t)__ldcg(&p.tapes[tape_idx]);
+            const uint64_t* tape = T.tapes + tape_idx + 1;
+            const uint32_t n = (uint32_t)__ldcg(&T.tapes[tape_idx]);
+            const float cs = T.cs;
 
             const uint32_t cell = grp * 32 + lane;
             const uint32_t cz = cell % dim, cy = (cell / dim) % dim, cx = cell / (dim * dim);
             const uint32_t gx = ncx * dim + cx, gy = ncy * dim + cy, gz = ncz * dim + cz;
             // voxelizer/main.comp:113-116, :124-126
-            const float lox = __fadd_rn(p.low[0], __fmul_rn((float)gx, cs));
-            const float loy = __fadd_rn(p.low[1], __fmul_rn((float)gy, cs));
-            const float loz = __fadd_rn(p.low[2], __fmul_rn((float)gz, cs));
+            const float lox = __fadd_rn(T.lx, __fmul_rn((float)gx, cs));
+            const float loy = __fadd_rn(T.ly, __fmul_rn((float)gy, cs));
+            const float loz = __fadd_rn(T.lz, __fmul_rn((float)gz, cs));
             sts_f2(lane_base + 0 * 256, make_float2(lox, __fadd_rn(lox, cs)));
             sts_f2(lane_base + 1 * 256, make_float2(loy, __fadd_rn(loy, cs)));
             sts_f2(lane_base + 2 * 256, make_float2(loz, __fadd_rn(loz, cs)));
-            sts_f2(lane_base + 3 * 256, make_float2(p.tape_time, p.tape_time));
+            sts_f2(lane_base + 3 * 256, make_float2(T.tt, T.tt));
 
             // ---- forward interval pass (interval.comp:121-160) ----
             uint32_t mm = 0;
@@ -290,17 +368,17 @@ interval_level_kernel(LevelArgs p) {
             const uint32_t n_amb = __popc(amb_w);
             unsigned long long child_base = 0;
             if (n_amb) {
-                if (lane == 0) child_base = atomicAdd(&H->node_count[L + 1], n_amb);
+                if (lane == 0) child_base = atomicAdd(&T.H->node_count[L + 1], n_amb);
                 child_base = __shfl_sync(0xFFFFFFFFu, child_base, 0);
             }
             const unsigned long long my_child = child_base + __popc(amb_w & lanemask_lt());
-            const bool ok = amb && my_child < child_cap;
+            const bool ok = amb && my_child < T.child_cap;
             const uint32_t ok_w = __ballot_sync(0xFFFFFFFFu, ok);
-            if (ok_w != amb_w && lane == 0) atomicOr(&H->overflow, 1u);
+            if (ok_w != amb_w && lane == 0) atomicOr(&T.H->overflow, 1u);
 
             uint32_t child_tape = tape_idx;
             uint32_t child_len = n;
-            if (ok_w && p.shorten) {
+            if (ok_w && T.shorten) {
                 // ---- backward liveness (shorten.comp:148-186) on transposed bitsets:
                 // live[s] bit l = slot s is live for lane l. The kept-mask of an
                 // instruction is live[out]; then live[out] = 0 and the inputs its
@@ -358,12 +436,12 @@ interval_level_kernel(LevelArgs p) {
                 const uint32_t total_words = __shfl_sync(0xFFFFFFFFu, incl, 31);
                 unsigned long long tbase = 0;
                 if (total_words) {
-                    if (lane == 0) tbase = atomicAdd(&H->tape_top, (unsigned long long)total_words);
+                    if (lane == 0) tbase = atomicAdd(&T.H->tape_top, (unsigned long long)total_words);
                     tbase = __shfl_sync(0xFFFFFFFFu, tbase, 0);
                 }
                 const unsigned long long my_tape = tbase + (incl - words);
-                const bool tape_ok = do_short && my_tape + words <= p.tape_cap;
-                if (do_short && !tape_ok) atomicOr(&H->overflow, 2u);
+                const bool tape_ok = do_short && my_tape + words <= T.tape_cap;
+                if (do_short && !tape_ok) atomicOr(&T.H->overflow, 2u);
                 const uint32_t short_w = __ballot_sync(0xFFFFFFFFu, tape_ok);
 
                 // ---- copy of the shortened tapes (shorten.comp:193-221) ----
@@ -371,7 +449,7 @@ interval_level_kernel(LevelArgs p) {
                 // and (for MIN/MAX) its choice masks; each output tape then takes
                 // one ballot + one coalesced store per chunk.
                 if (short_w) {
-                    if (tape_ok) p.tapes[my_tape] = (uint64_t)kept;
+                    if (tape_ok) T.tapes[my_tape] = (uint64_t)kept;
                     uint32_t run = 0;  // lane L: instructions written so far to its own tape
                     uint32_t mm_run = 0;
                     for (uint32_t b = 0; b < n; b += 32) {
@@ -400,7 +478,7 @@ interval_level_kernel(LevelArgs p) {
                             const uint32_t kball = __ballot_sync(0xFFFFFFFFu, kb);
                             const unsigned long long dst = __shfl_sync(0xFFFFFFFFu, my_tape, sel);
                             const uint32_t r = __shfl_sync(0xFFFFFFFFu, run, sel);
-                            if (kb) p.tapes[dst + 1 + r + __popc(kball & lanemask_lt())] = wo;
+                            if (kb) T.tapes[dst + 1 + r + __popc(kball & lanemask_lt())] = wo;
                             if ((int)lane == sel) run += __popc(kball);
                         }
                         mm_run += __popc(mball);
@@ -414,7 +492,7 @@ interval_level_kernel(LevelArgs p) {
 
             // ---- node records: masks, child list, children ----
             if (ok) {
-                uint32_t* crec = p.nodes + ofs_next + (size_t)my_child * p.node_size_next;
+                uint32_t* crec = T.nodes + T.ofs_next + (size_t)my_child * T.node_size_next;
                 crec[0] = child_tape;
                 crec[1] = gx;
                 crec[2] = gy;
@@ -432,16 +510,7 @@ interval_level_kernel(LevelArgs p) {
         }
     }
 
-    // Per-warp statistics, flushed once (stats_buf of main.comp:146-147).
-    for (int off = 16; off > 0; off >>= 1) {
-        stat_sum += __shfl_down_sync(0xFFFFFFFFu, stat_sum, off);
-        stat_max = max(stat_max, __shfl_down_sync(0xFFFFFFFFu, stat_max, off));
-    }
-    if (lane == 0) {
-        if (stat_sum) atomicAdd(&H->tape_size_sum[L + 1], stat_sum);
-        if (stat_max) atomicMax(&H->tape_size_max[L + 1], stat_max);
-        if (stat_work) atomicAdd(&H->cell_instr[L], stat_work);
-    }
+    if (have_tree) flush();
 }
 
 // ---- point level pass (the last level) ---------------------------------------------
@@ -503,7 +572,7 @@ __device__ __forceinline__ void pt_exec(const uint4 d, FK<K>& r, uint32_t lane_b
 
 template <int WARPS, int K>
 __global__ void __launch_bounds__(WARPS * 32)
-point_level_kernel(LevelArgs p) {
+point_level_kernel(LevelLaunch p) {
     extern __shared__ __align__(16) unsigned char smem[];
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned char* wbase = smem + (size_t)warp * p.smem_per_warp;
@@ -512,45 +581,56 @@ point_level_kernel(LevelArgs p) {
     uint4* stage = reinterpret_cast<uint4*>(wbase + (size_t)p.n_slots * 32 * ROW);
     if (lane == 0) stage[STAGE] = make_uint4(0u, 0u, 0u, 0u);  // sentinel past a full chunk
 
-    TreeHeader* H = p.hdr;
     const uint32_t L = p.level;
-    const uint32_t dim = p.dim;
-    const uint32_t words = dim * dim * dim / 32;      // mask words per node
-    const uint32_t groups = words / K;                // items per node
-    const uint32_t count = level_count(H, L, p.node_cap, p.node_size);
-    const unsigned long long ofs_l = H->node_ofs[L];
-    const unsigned long long total = (unsigned long long)count * groups;
+    const unsigned long long total = __ldcg(&p.prefix[p.n_trees]);
     const uint32_t chunk = chunk_for(total, gridDim.x * WARPS);
-    const float cs = p.cell_size;
     unsigned long long stat_work = 0;
     uint32_t staged_tape = 0xFFFFFFFFu;  // tape whose whole body is in `stage`
+    const uint64_t* staged_pool = nullptr;
+    LevelTree T{};
+    unsigned long long t_lo = 0, t_hi = 0;
+    bool have_tree = false;
 
     unsigned long long first;
     uint32_t got;
-    while ((got = fetch_items(&H->work_cursor[L], total, chunk, &first)) != 0) {
+    while ((got = fetch_items(p.cursor, total, chunk, &first)) != 0) {
         for (uint32_t it = 0; it < got; it++) {
             const unsigned long long item = first + it;
-            const uint32_t node = (uint32_t)(item / groups), grp = (uint32_t)(item % groups);
-            uint32_t* rec = p.nodes + ofs_l + (size_t)node * p.node_size;
+            if (!have_tree || item >= t_hi) {
+                if (have_tree && lane == 0 && stat_work) atomicAdd(&T.H->cell_instr[L], stat_work);
+                stat_work = 0;
+                const uint32_t ti = find_tree(p.prefix, p.n_trees, item);
+                t_lo = __ldcg(&p.prefix[ti]);
+                t_hi = __ldcg(&p.prefix[ti + 1]);
+                T = load_tree(p.trees[ti], L, true);
+                have_tree = true;
+            }
+            const uint32_t dim = T.dim;
+            const uint32_t words = dim * dim * dim / 32;      // mask words per node
+            const uint32_t groups = words / K;                // items per node
+            const float cs = T.cs;
+            const unsigned long long local = item - t_lo;
+            const uint32_t node = (uint32_t)(local / groups), grp = (uint32_t)(local % groups);
+            uint32_t* rec = T.nodes + T.ofs_l + (size_t)node * T.node_size;
             const uint32_t tape_idx = rec[0];
-            const uint64_t* tape = p.tapes + tape_idx + 1;
-            const uint32_t n = (uint32_t)__ldcg(&p.tapes[tape_idx]);
+            const uint64_t* tape = T.tapes + tape_idx + 1;
+            const uint32_t n = (uint32_t)__ldcg(&T.tapes[tape_idx]);
             const uint32_t ncx = rec[1], ncy = rec[2], ncz = rec[3];
             FK<K> px, py, pz, pt;
 #pragma unroll
             for (int k = 0; k < K; k++) {
                 const uint32_t cell = grp * 32 * K + k * 32 + lane;
                 const uint32_t cz = cell % dim, cy = (cell / dim) % dim, cx = cell / (dim * dim);
-                px.v[k] = __fadd_rn(p.low[0], __fmul_rn((float)(ncx * dim + cx), cs));
-                py.v[k] = __fadd_rn(p.low[1], __fmul_rn((float)(ncy * dim + cy), cs));
-                pz.v[k] = __fadd_rn(p.low[2], __fmul_rn((float)(ncz * dim + cz), cs));
-                pt.v[k] = p.tape_time;
+                px.v[k] = __fadd_rn(T.lx, __fmul_rn((float)(ncx * dim + cx), cs));
+                py.v[k] = __fadd_rn(T.ly, __fmul_rn((float)(ncy * dim + cy), cs));
+                pz.v[k] = __fadd_rn(T.lz, __fmul_rn((float)(ncz * dim + cz), cs));
+                pt.v[k] = T.tt;
             }
             sts_k<K>(lane_base + 0 * 32 * ROW, px);
             sts_k<K>(lane_base + 1 * 32 * ROW, py);
             sts_k<K>(lane_base + 2 * 32 * ROW, pz);
             sts_k<K>(lane_base + 3 * 32 * ROW, pt);
-            const bool resident = n <= STAGE && staged_tape == tape_idx;
+            const bool resident = n <= STAGE && staged_tape == tape_idx && staged_pool == T.tapes;
             FK<K> r;
 #pragma unroll
             for (int k = 0; k < K; k++) r.v[k] = 0.0f;
@@ -588,6 +668,7 @@ point_level_kernel(LevelArgs p) {
                 }
             }
             staged_tape = n <= STAGE ? tape_idx : 0xFFFFFFFFu;
+            staged_pool = T.tapes;
             __syncwarp();
             stat_work += 32ull * K * n;
             const FK<K> d = lds_k<K>(lane_base);
@@ -601,30 +682,116 @@ point_level_kernel(LevelArgs p) {
             }
         }
     }
-    if (lane == 0 && stat_work) atomicAdd(&H->cell_instr[L], stat_work);
+    if (have_tree && lane == 0 && stat_work) atomicAdd(&T.H->cell_instr[L], stat_work);
 }
 
-// Resets the header and writes the root node (Voxelizer::Voxelize sets
-// interiorNodeCount[0] = 1 and relies on a zeroed root, voxelizer.cpp:432-435).
-__global__ void tree_init_kernel(TreeHeader* H, uint32_t* nodes, uint32_t root_n, uint32_t root_words) {
-    const uint32_t t = threadIdx.x;
-    for (uint32_t l = t; l < MAX_LEVELS; l += blockDim.x) {
-        H->node_count[l] = l == 0 ? 1u : 0u;
-        H->work_cursor[l] = 0;
-        H->node_ofs[l] = 0;
-        H->tape_size_sum[l] = l == 0 ? root_n : 0;
-        H->tape_size_max[l] = l == 0 ? root_n : 0;
-        H->cell_instr[l] = 0;
-        H->fp32_ops[l] = 0;
+// Lays the batch's items for `level` end to end: prefix[i] = items of trees
+// before i that this launch serves (interval passes: trees for which `level`
+// is not the last; point passes: trees for which it is, with a last-level node
+// size that takes `point_k` cells per lane). Interval passes also fix where
+// each tree's next level starts (node_ofs[level + 1]). One block.
+__device__ __forceinline__ unsigned long long level_items(TreeHeader* H, uint32_t L, int point, int point_k,
+                                                          bool write_ofs) {
+    if (L >= H->levels) return 0;
+    const bool last = L == H->levels - 1;
+    if ((point != 0) != last) return 0;
+    const uint32_t dim = H->dims[L];
+    const uint32_t words = dim * dim * dim / 32;
+    if (point && point_k_of(dim) != point_k) return 0;
+    const uint32_t count = level_count(H, L, H->node_cap, H->node_size[L]);
+    if (!point && write_ofs) H->node_ofs[L + 1] = H->node_ofs[L] + (unsigned long long)count * H->node_size[L];
+    return (unsigned long long)count * (point ? words / (uint32_t)point_k : words);
+}
+
+__global__ void __launch_bounds__(1024)
+level_scan_kernel(TreeHeader* const* trees, uint32_t n, uint32_t L, int point, int point_k,
+                  unsigned long long* prefix, unsigned long long* cursor) {
+    __shared__ unsigned long long part[1024];
+    const uint32_t t = threadIdx.x, T = blockDim.x;
+    const uint32_t per = (n + T - 1) / T;
+    const uint32_t b = min(n, t * per), e = min(n, b + per);
+    unsigned long long sum = 0;
+    for (uint32_t i = b; i < e; i++) sum += level_items(trees[i], L, point, point_k, true);
+    part[t] = sum;
+    __syncthreads();
+    for (uint32_t off = 1; off < T; off <<= 1) {  // inclusive scan
+        const unsigned long long v = t >= off ? part[t - off] : 0ull;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
     }
-    if (t == 0) {
-        H->tape_top = root_words;
-        H->overflow = 0;
-        H->status = 0;
-        nodes[0] = 0;  // root tape at word 0 of the tape pool
-        nodes[1] = 0;
-        nodes[2] = 0;
-        nodes[3] = 0;
+    unsigned long long run = part[t] - sum;
+    for (uint32_t i = b; i < e; i++) {
+        prefix[i] = run;
+        run += level_items(trees[i], L, point, point_k, false);
+    }
+    if (t == T - 1) prefix[n] = part[t];
+    if (t == 0) *cursor = 0ull;
+}
+
+// Resets the headers and writes the root nodes (Voxelizer::Voxelize sets
+// interiorNodeCount[0] = 1 and relies on a zeroed root, voxelizer.cpp:432-435).
+// One block per tree; each tree's root tape is already at word 0 of its pool.
+__global__ void tree_init_kernel(TreeHeader* const* trees, uint32_t n, const float* tape_times, float tape_time) {
+    for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
+        TreeHeader* H = trees[i];
+        const uint32_t t = threadIdx.x;
+        const uint32_t root_n = (uint32_t)H->tapes[0];
+        if (t < MAX_LEVELS) {
+            H->node_count[t] = t == 0 ? 1u : 0u;
+            H->node_ofs[t] = 0;
+            H->tape_size_sum[t] = t == 0 ? root_n : 0;
+            H->tape_size_max[t] = t == 0 ? root_n : 0;
+            H->cell_instr[t] = 0;
+            H->fp32_ops[t] = 0;
+        }
+        if (t == 0) {
+            H->tape_top = (1 + (unsigned long long)root_n + TAPE_ALIGN_WORDS - 1) / TAPE_ALIGN_WORDS * TAPE_ALIGN_WORDS;
+            H->overflow = 0;
+            H->status = 0;
+            H->tape_time = tape_times ? tape_times[i] : tape_time;
+            uint32_t* root = H->nodes;
+            root[0] = 0;  // root tape at word 0 of the tape pool
+            root[1] = 0;
+            root[2] = 0;
+            root[3] = 0;
+        }
+    }
+}
+
+// Batch variant of tree_init_kernel: block i first copies tree i's root tape
+// record from the staged upload (words offsets[i] .. offsets[i+1] of `staged`)
+// to word 0 of its tape pool, then resets its header like tree_init_kernel.
+__global__ void tree_init_staged_kernel(TreeHeader* const* trees, uint32_t n, const uint64_t* staged,
+                                        const unsigned long long* offsets, const float* tape_times) {
+    for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
+        TreeHeader* H = trees[i];
+        uint64_t* pool = H->tapes;
+        const unsigned long long b = offsets[i], e = offsets[i + 1];
+        for (unsigned long long w = b + threadIdx.x; w < e; w += blockDim.x) pool[w - b] = staged[w];
+        __syncthreads();
+        const uint32_t t = threadIdx.x;
+        const uint32_t root_n = (uint32_t)pool[0];
+        if (t < MAX_LEVELS) {
+            H->node_count[t] = t == 0 ? 1u : 0u;
+            H->node_ofs[t] = 0;
+            H->tape_size_sum[t] = t == 0 ? root_n : 0;
+            H->tape_size_max[t] = t == 0 ? root_n : 0;
+            H->cell_instr[t] = 0;
+            H->fp32_ops[t] = 0;
+        }
+        if (t == 0) {
+            H->tape_top = e - b;
+            H->overflow = 0;
+            H->status = 0;
+            H->tape_time = tape_times[i];
+            uint32_t* root = H->nodes;
+            root[0] = 0;
+            root[1] = 0;
+            root[2] = 0;
+            root[3] = 0;
+        }
+        __syncthreads();
     }
 }
 
@@ -676,7 +843,7 @@ cudaError_t occupancy(Kern kernel, int threads, size_t smem, int* blocks) {
 // items, so K must divide the node's dim^3 / 32 mask words. With dim a
 // multiple of 4 that count is even; it is a multiple of 4 when dim is a
 // multiple of 8.
-static int point_k(uint32_t dim) { return (dim * dim * dim / 32) % 4 == 0 ? 4 : 2; }
+int point_k_for(uint32_t dim) { return dev::point_k_of(dim); }
 
 template <int K>
 static cudaError_t plan_point(uint32_t n_slots, LevelPlan* plan) {
@@ -689,7 +856,7 @@ static cudaError_t plan_point(uint32_t n_slots, LevelPlan* plan) {
     return occupancy(dev::point_level_kernel<1, K>, 32, pt, &plan->point_blocks);
 }
 
-cudaError_t plan_levels(uint32_t n_slots, uint32_t mm_cap, uint32_t last_dim, int rounding, LevelPlan* plan) {
+cudaError_t plan_levels(uint32_t n_slots, uint32_t mm_cap, int point_k, int rounding, LevelPlan* plan) {
     const uint32_t iv = (n_slots * 256 + (dev::STAGE + 1) * 16 + mm_cap * 8 + n_slots * 4 + 15) / 16 * 16;
     plan->smem_per_warp = iv;
     // Four warps per block when they fit in shared memory, else one.
@@ -705,20 +872,35 @@ cudaError_t plan_levels(uint32_t n_slots, uint32_t mm_cap, uint32_t last_dim, in
                      : occupancy(dev::interval_level_kernel<0, 1>, 32, iv, &plan->blocks);
     }
     if (e != cudaSuccess) return e;
-    plan->point_k = point_k(last_dim);
-    return plan->point_k == 4 ? plan_point<4>(n_slots, plan) : plan_point<2>(n_slots, plan);
+    plan->point_k = point_k;
+    return point_k == 4 ? plan_point<4>(n_slots, plan) : plan_point<2>(n_slots, plan);
 }
 
-cudaError_t launch_tree_init(dev::TreeHeader* hdr, uint32_t* nodes, uint32_t root_n_instr,
-                             uint32_t root_words, cudaStream_t stream) {
-    dev::tree_init_kernel<<<1, 32, 0, stream>>>(hdr, nodes, root_n_instr, root_words);
+cudaError_t launch_tree_init(dev::TreeHeader* const* trees, uint32_t n, const float* tape_times, float tape_time,
+                             cudaStream_t stream) {
+    const uint32_t blocks = n < 4096 ? n : 4096;
+    dev::tree_init_kernel<<<blocks, 32, 0, stream>>>(trees, n, tape_times, tape_time);
     return cudaGetLastError();
 }
 
-cudaError_t launch_level(const LevelArgs& a, const LevelPlan& plan, int rounding, bool last,
+cudaError_t launch_tree_init_staged(dev::TreeHeader* const* trees, uint32_t n, const uint64_t* staged,
+                                    const unsigned long long* offsets, const float* tape_times,
+                                    cudaStream_t stream) {
+    const uint32_t blocks = n < 4096 ? n : 4096;
+    dev::tree_init_staged_kernel<<<blocks, 256, 0, stream>>>(trees, n, staged, offsets, tape_times);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_level_scan(const LevelLaunch& a, bool point, int point_k, cudaStream_t stream) {
+    dev::level_scan_kernel<<<1, 1024, 0, stream>>>(a.trees, a.n_trees, a.level, point ? 1 : 0, point_k, a.prefix,
+                                                   a.cursor);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_level(const LevelLaunch& a, const LevelPlan& plan, int rounding, bool point,
                          cudaStream_t stream) {
-    if (last) {
-        LevelArgs b = a;
+    if (point) {
+        LevelLaunch b = a;
         b.smem_per_warp = plan.point_smem_per_warp;
         const int w4 = plan.point_warps_per_block == 4;
         const size_t smem = (size_t)plan.point_warps_per_block * plan.point_smem_per_warp;
@@ -731,7 +913,7 @@ cudaError_t launch_level(const LevelArgs& a, const LevelPlan& plan, int rounding
         }
         return cudaGetLastError();
     }
-    LevelArgs b = a;
+    LevelLaunch b = a;
     b.smem_per_warp = plan.smem_per_warp;
     const int w = plan.warps_per_block;
     const size_t smem = (size_t)w * plan.smem_per_warp;

@@ -381,3 +381,59 @@ class Raytracer:
         L.check(L.lib().frep_render(self.ctx._h, self.voxels.tree, C.byref(cam), C.byref(lights),
                                     float(tape_time), C.byref(img), _stream_ptr(stream)))
         return rgba, hit_buf
+
+
+class Batch:
+    """Many scenes voxelized and rendered together (frep_batch): one launch per
+    level pass over all trees, one launch for all frames, optionally replayed
+    as a CUDA graph. Scenes keep their own VoxelStorage (tree and tape)."""
+
+    def __init__(self, ctx: Context, storages: list):
+        self.ctx = ctx
+        self.storages = list(storages)
+        arr = (C.c_void_p * len(self.storages))(*[s.tree.value for s in self.storages])
+        self._h = C.c_void_p()
+        L.check(L.lib().frep_batch_create(ctx._h, arr, len(self.storages), C.byref(self._h)))
+        self._tapes = (C.c_void_p * len(self.storages))(*[s.tape.handle.value for s in self.storages])
+
+    def close(self):
+        if self._h is not None and self._h.value and L._lib is not None:
+            L.lib().frep_batch_destroy(self._h)
+        self._h = C.c_void_p()
+
+    def __del__(self):
+        self.close()
+
+    def set_tapes(self):
+        self._tapes = (C.c_void_p * len(self.storages))(*[s.tape.handle.value for s in self.storages])
+
+    def _times(self, tape_times):
+        if tape_times is None:
+            return None
+        return (C.c_float * len(self.storages))(*[float(t) for t in tape_times])
+
+    def voxelize(self, tape_times=None, stream=None):
+        L.check(L.lib().frep_batch_voxelize(self._h, self._tapes, self._times(tape_times), _stream_ptr(stream)))
+
+    @staticmethod
+    def _frames(cameras, sizes, rgba, hits):
+        n = len(cameras)
+        cams = (L.CameraStruct * n)(*[c.struct(w, h) for c, (w, h) in zip(cameras, sizes)])
+        imgs = (L.Image * n)()
+        for i in range(n):
+            imgs[i].rgba8 = rgba[i].data_ptr()
+            imgs[i].hits = hits[i].data_ptr() if hits is not None else None
+        return cams, imgs
+
+    def render(self, cameras, sizes, rgba, hits=None, lights=None, tape_times=None, stream=None):
+        """rgba[i] / hits[i]: device tensors (H, W, 4) uint8 / (H, W, 8) int32."""
+        cams, imgs = self._frames(cameras, sizes, rgba, hits)
+        lt = (lights or Lights()).struct()
+        L.check(L.lib().frep_batch_render(self._h, cams, C.byref(lt), self._times(tape_times), imgs,
+                                          _stream_ptr(stream)))
+
+    def run(self, cameras, sizes, rgba, hits=None, lights=None, tape_times=None, graph=True, stream=None):
+        cams, imgs = self._frames(cameras, sizes, rgba, hits)
+        lt = (lights or Lights()).struct()
+        L.check(L.lib().frep_batch_run(self._h, self._tapes, self._times(tape_times), cams, C.byref(lt), imgs,
+                                       1 if graph else 0, _stream_ptr(stream)))

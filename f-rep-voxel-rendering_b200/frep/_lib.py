@@ -100,6 +100,11 @@ _SIGS = {
     "frep_tree_copy_nodes": (C.c_int, [_P, _P, C.c_uint64]),
     "frep_tree_copy_tapes": (C.c_int, [_P, _P, C.c_uint64]),
     "frep_lights_default": (C.c_int, [C.POINTER(LightsStruct)]),
+    "frep_batch_create": (C.c_int, [_P, _P, C.c_uint32, C.POINTER(_P)]),
+    "frep_batch_destroy": (None, [_P]),
+    "frep_batch_voxelize": (C.c_int, [_P, _P, _P, _P]),
+    "frep_batch_render": (C.c_int, [_P, _P, C.POINTER(LightsStruct), _P, _P, _P]),
+    "frep_batch_run": (C.c_int, [_P, _P, _P, _P, C.POINTER(LightsStruct), _P, C.c_int, _P]),
     "frep_render": (C.c_int, [_P, _P, C.POINTER(CameraStruct), C.POINTER(LightsStruct), C.c_float,
                               C.POINTER(Image), _P]),
 }

@@ -287,6 +287,37 @@ frep_status frep_render(frep_ctx* ctx, const frep_tree* tree, const frep_camera*
                         const frep_lights* lights, float tape_time, const frep_image* out,
                         void* stream);
 
+/* ---------------------------------------------------------------------------
+ * Batching: many scenes per launch
+ * ------------------------------------------------------------------------- */
+
+/* A fixed set of trees that are voxelized and rendered together. Every level
+ * pass is ONE launch over all the trees (warps take work items from any tree
+ * through one device cursor), and all frames are one launch. No counterpart in
+ * the reference, which voxelizes one scene at a time with a host fence per
+ * level (voxelizer.cpp:295-329). All trees must use the same rounding. */
+typedef struct frep_batch frep_batch;
+
+frep_status frep_batch_create(frep_ctx* ctx, frep_tree* const* trees, uint32_t n, frep_batch** out);
+void frep_batch_destroy(frep_batch* batch);
+
+/* Voxelizes tree i from tapes[i] at tape_times[i] (tape_times may be NULL:
+ * all 0). Enqueued on `stream`; frep_tree_sync works per tree afterwards. */
+frep_status frep_batch_voxelize(frep_batch* batch, const frep_tape* const* tapes, const float* tape_times,
+                                void* stream);
+
+/* Renders tree i with cameras[i] into images[i] (one launch for all frames). */
+frep_status frep_batch_render(frep_batch* batch, const frep_camera* cameras, const frep_lights* lights,
+                              const float* tape_times, const frep_image* images, void* stream);
+
+/* Voxelize + render. With use_graph != 0 the whole sequence (one upload, the
+ * level passes, the frames) is captured into a CUDA graph on first use and
+ * replayed while the batch keeps its shape (same tape lengths, frame sizes and
+ * buffers); a new shape is captured again. */
+frep_status frep_batch_run(frep_batch* batch, const frep_tape* const* tapes, const float* tape_times,
+                           const frep_camera* cameras, const frep_lights* lights, const frep_image* images,
+                           int use_graph, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
