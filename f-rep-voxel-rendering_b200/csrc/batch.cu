@@ -44,6 +44,14 @@ struct frep_batch {
     frep::LevelPlan plan4{}, plan2{};
     uint32_t plan_slots = 0, plan_mm = 0;
     bool plan_valid = false;
+    // profiling (plain launches only): ev[0] before the root copy, ev[1] after
+    // it, ev[2 + 3 l + kind] after level l's pass of that kind (0 interval,
+    // 1 point with 4 cells per lane, 2 point with 2); rev around the frames
+    bool profile = false;
+    bool profiled = false, render_profiled = false;
+    uint32_t profiled_levels = 0;
+    cudaEvent_t ev[2 + 3 * FREP_MAX_LEVELS] = {};
+    cudaEvent_t rev[2] = {};
     // graph replay
     cudaStream_t capture_stream = nullptr;
     cudaGraphExec_t graph = nullptr;
@@ -158,12 +166,14 @@ frep_status ensure_plans(frep_batch* b, const TapeStats& st) {
 // Enqueues the voxelization of every tree: root copy + header reset, then for
 // each level index one interval pass and up to two point passes, each a single
 // launch over the whole batch.
-frep_status enqueue_voxelize(frep_batch* b, const TapeStats& st, const Layout& L, cudaStream_t s) {
+frep_status enqueue_voxelize(frep_batch* b, const TapeStats& st, const Layout& L, cudaStream_t s, bool prof) {
+    if (prof) FREP_CUDA(cudaEventRecord(b->ev[0], s));
     const uint64_t* staged_roots = reinterpret_cast<const uint64_t*>(b->d_stage + L.roots);
     const unsigned long long* offsets = reinterpret_cast<const unsigned long long*>(b->d_stage + L.offsets);
     const float* times = reinterpret_cast<const float*>(b->d_stage + L.times);
     cudaError_t e = frep::launch_tree_init_staged(b->d_trees, b->n, staged_roots, offsets, times, s);
     if (e != cudaSuccess) return cuda_fail(e, "tree_init_staged_kernel");
+    if (prof) FREP_CUDA(cudaEventRecord(b->ev[1], s));
     frep::LevelLaunch a{};
     a.trees = b->d_trees;
     a.prefix = b->d_prefix;
@@ -179,16 +189,23 @@ frep_status enqueue_voxelize(frep_batch* b, const TapeStats& st, const Layout& L
         e = frep::launch_level_scan(a, false, 4, s);
         if (e == cudaSuccess) e = frep::launch_level(a, b->plan4, b->rounding, false, s);
         if (e != cudaSuccess) return cuda_fail(e, "batched interval pass");
+        if (prof) FREP_CUDA(cudaEventRecord(b->ev[2 + 3 * l], s));
         if (st.any_k4) {
             e = frep::launch_level_scan(a, true, 4, s);
             if (e == cudaSuccess) e = frep::launch_level(a, b->plan4, b->rounding, true, s);
             if (e != cudaSuccess) return cuda_fail(e, "batched point pass");
         }
+        if (prof) FREP_CUDA(cudaEventRecord(b->ev[3 + 3 * l], s));
         if (st.any_k2) {
             e = frep::launch_level_scan(a, true, 2, s);
             if (e == cudaSuccess) e = frep::launch_level(a, b->plan2, b->rounding, true, s);
             if (e != cudaSuccess) return cuda_fail(e, "batched point pass");
         }
+        if (prof) FREP_CUDA(cudaEventRecord(b->ev[4 + 3 * l], s));
+    }
+    if (prof) {
+        b->profiled = true;
+        b->profiled_levels = st.max_levels;
     }
     return FREP_OK;
 }
@@ -289,6 +306,10 @@ void frep_batch_destroy(frep_batch* b) {
     if (b->h_stage) cudaFreeHost(b->h_stage);
     if (b->upload_done) cudaEventDestroy(b->upload_done);
     if (b->capture_stream) cudaStreamDestroy(b->capture_stream);
+    for (cudaEvent_t e : b->ev)
+        if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : b->rev)
+        if (e) cudaEventDestroy(e);
     b->ctx->used -= std::min<uint64_t>(b->ctx->used, b->bytes);
     delete b;
 }
@@ -312,7 +333,7 @@ frep_status frep_batch_voxelize(frep_batch* b, const frep_tape* const* tapes, co
     FREP_CUDA(cudaMemcpyAsync(b->d_stage + L.roots, b->h_stage + L.roots, L.total - L.roots,
                               cudaMemcpyHostToDevice, s));
     FREP_CUDA(cudaEventRecord(b->upload_done, s));
-    r = enqueue_voxelize(b, st, L, s);
+    r = enqueue_voxelize(b, st, L, s, b->profile);
     if (r != FREP_OK) return r;
     mark_voxelized(b, tapes, s);
     return FREP_OK;
@@ -337,10 +358,15 @@ frep_status frep_batch_render(frep_batch* b, const frep_camera* cameras, const f
     FREP_CUDA(cudaMemcpyAsync(b->d_stage + L.frames, b->h_stage + L.frames, L.roots - L.frames,
                               cudaMemcpyHostToDevice, s));
     FREP_CUDA(cudaEventRecord(b->upload_done, s));
+    if (b->profile) FREP_CUDA(cudaEventRecord(b->rev[0], s));
     cudaError_t e = frep::launch_render_batch(reinterpret_cast<const frep::RenderArgs*>(b->d_stage + L.frames), b->n,
                                               mw, mh, ms, s);
     if (e == cudaErrorInvalidValue) return fail(FREP_ERR_UNSUPPORTED, "frep_batch_render: too many frames or slots");
     if (e != cudaSuccess) return cuda_fail(e, "render_batch_kernel");
+    if (b->profile) {
+        FREP_CUDA(cudaEventRecord(b->rev[1], s));
+        b->render_profiled = true;
+    }
     return FREP_OK;
 }
 
@@ -382,7 +408,7 @@ frep_status frep_batch_run(frep_batch* b, const frep_tape* const* tapes, const f
         cudaStream_t cs = b->capture_stream;
         FREP_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
         cudaError_t ce = cudaMemcpyAsync(b->d_stage, b->h_stage, L.total, cudaMemcpyHostToDevice, cs);
-        frep_status vr = ce == cudaSuccess ? enqueue_voxelize(b, st, L, cs) : cuda_fail(ce, "upload");
+        frep_status vr = ce == cudaSuccess ? enqueue_voxelize(b, st, L, cs, false) : cuda_fail(ce, "upload");
         if (vr == FREP_OK) {
             ce = frep::launch_render_batch(reinterpret_cast<const frep::RenderArgs*>(b->d_stage + L.frames), b->n,
                                            mw, mh, ms, cs);
@@ -402,6 +428,36 @@ frep_status frep_batch_run(frep_batch* b, const frep_tape* const* tapes, const f
     }
     FREP_CUDA(cudaGraphLaunch(b->graph, s));
     FREP_CUDA(cudaEventRecord(b->upload_done, s));
+    return FREP_OK;
+}
+
+frep_status frep_batch_set_profiling(frep_batch* b, int enable) {
+    if (!b) return fail(FREP_ERR_INVALID_ARG, "frep_batch_set_profiling: null batch");
+    FREP_CUDA(cudaSetDevice(b->ctx->device));
+    if (enable && !b->ev[0]) {
+        for (cudaEvent_t& e : b->ev) FREP_CUDA(cudaEventCreate(&e));
+        for (cudaEvent_t& e : b->rev) FREP_CUDA(cudaEventCreate(&e));
+    }
+    b->profile = enable != 0;
+    b->profiled = b->render_profiled = false;
+    return FREP_OK;
+}
+
+frep_status frep_batch_timings(frep_batch* b, float ms[3 * FREP_MAX_LEVELS + 2]) {
+    if (!b || !ms) return fail(FREP_ERR_INVALID_ARG, "frep_batch_timings: null argument");
+    if (!b->profile || !b->profiled)
+        return fail(FREP_ERR_INVALID_ARG, "frep_batch_timings: no profiled frep_batch_voxelize since profiling was enabled");
+    FREP_CUDA(cudaSetDevice(b->ctx->device));
+    for (int i = 0; i < 3 * FREP_MAX_LEVELS + 2; i++) ms[i] = 0.0f;
+    const uint32_t last = 1 + 3 * b->profiled_levels;
+    FREP_CUDA(cudaEventSynchronize(b->ev[last]));
+    FREP_CUDA(cudaEventElapsedTime(&ms[3 * FREP_MAX_LEVELS], b->ev[0], b->ev[1]));
+    for (uint32_t g = 0; g < 3 * b->profiled_levels; g++)
+        FREP_CUDA(cudaEventElapsedTime(&ms[g], b->ev[1 + g], b->ev[2 + g]));
+    if (b->render_profiled) {
+        FREP_CUDA(cudaEventSynchronize(b->rev[1]));
+        FREP_CUDA(cudaEventElapsedTime(&ms[3 * FREP_MAX_LEVELS + 1], b->rev[0], b->rev[1]));
+    }
     return FREP_OK;
 }
 

@@ -412,6 +412,17 @@ class Batch:
             return None
         return (C.c_float * len(self.storages))(*[float(t) for t in tape_times])
 
+    def set_profiling(self, enable: bool = True) -> None:
+        L.check(L.lib().frep_batch_set_profiling(self._h, 1 if enable else 0))
+
+    def timings(self) -> dict:
+        """Device ms of the last profiled plain calls: {"level": [[interval,
+        point K=4, point K=2] per level], "init": ms, "render": ms}."""
+        arr = (C.c_float * (3 * L.MAX_LEVELS + 2))()
+        L.check(L.lib().frep_batch_timings(self._h, arr))
+        lv = [[arr[3 * l + k] for k in range(3)] for l in range(L.MAX_LEVELS)]
+        return {"level": lv, "init": arr[3 * L.MAX_LEVELS], "render": arr[3 * L.MAX_LEVELS + 1]}
+
     def voxelize(self, tape_times=None, stream=None):
         L.check(L.lib().frep_batch_voxelize(self._h, self._tapes, self._times(tape_times), _stream_ptr(stream)))
 

@@ -105,6 +105,8 @@ _SIGS = {
     "frep_batch_voxelize": (C.c_int, [_P, _P, _P, _P]),
     "frep_batch_render": (C.c_int, [_P, _P, C.POINTER(LightsStruct), _P, _P, _P]),
     "frep_batch_run": (C.c_int, [_P, _P, _P, _P, C.POINTER(LightsStruct), _P, C.c_int, _P]),
+    "frep_batch_set_profiling": (C.c_int, [_P, C.c_int]),
+    "frep_batch_timings": (C.c_int, [_P, _P]),
     "frep_render": (C.c_int, [_P, _P, C.POINTER(CameraStruct), C.POINTER(LightsStruct), C.c_float,
                               C.POINTER(Image), _P]),
 }

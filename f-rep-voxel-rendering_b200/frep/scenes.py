@@ -223,3 +223,63 @@ DEMO_SHAPES = {
     "TwistedTower": TwistedTower,
     "OrganicBalls": lambda level: OrganicBalls(),
 }
+
+
+# ---- batching / serving workload --------------------------------------------------
+
+BATCH_RESOLUTIONS = (64, 128, 256, 512, 1024)
+
+# Branching per effective resolution when no tuned choice is given: 16 at the
+# root, then the largest factors that leave a last level of at least 4.
+DEFAULT_BRANCHING = {64: (16, 4), 128: (16, 8), 256: (16, 16), 512: (16, 8, 4), 1024: (16, 16, 4)}
+
+
+def orbit_camera(rng, distance: float = 4.1, fov_deg: float = 60.0):
+    """A perspective camera on a sphere around the origin, looking at it, at a
+    random azimuth and an elevation in [-0.35, 1.0] rad."""
+    from . import Camera
+    az = float(rng.uniform(0.0, 2.0 * np.pi))
+    el = float(rng.uniform(-0.35, 1.0))
+    pos = (distance * np.cos(el) * np.cos(az), distance * np.sin(el), distance * np.cos(el) * np.sin(az))
+    return Camera(position=pos, forward=tuple(-v for v in pos), initial_up=(0.0, 1.0, 0.0), fov_deg=fov_deg)
+
+
+def _batch_scene(job):
+    """One scene of batch_workload, its shape flattened to DAG arrays so that
+    it crosses a process boundary."""
+    i, seed, count, res, dims, width, height, shadows = job
+    sc = random_csg(count, seed=seed, grid_dims=dims, width=width, height=height, shadows=shadows)
+    sc.name = "batch"
+    sc.meta.update(index=i, res=res)
+    sc.shape = sc.shape.flatten()
+    return sc
+
+
+def batch_workload(n_scenes: int = 512, seed: int = 3, width: int = 512, height: int = 512,
+                   shadows: bool = True, branching: dict | None = None, min_prims: int = 4,
+                   max_prims: int = 1024, processes: int = 0) -> list:
+    """Independent scenes as in random_csg with primitive counts log-uniform in
+    [min_prims, max_prims] and effective resolutions drawn uniformly from
+    BATCH_RESOLUTIONS. `branching` maps an effective resolution to grid dims
+    (default DEFAULT_BRANCHING). Scene i's meta holds its index, primitive
+    count and resolution; its shape is a compiled frep.Tape. `processes` > 1
+    builds the expressions in that many spawned worker processes (expression
+    building is Python-bound: about 0.25 ms per primitive)."""
+    from . import Tape
+    rng = np.random.default_rng(seed)
+    counts = np.exp(rng.uniform(np.log(min_prims), np.log(max_prims), n_scenes))
+    counts = np.clip(np.round(counts), min_prims, max_prims).astype(int)
+    res = rng.choice(np.array(BATCH_RESOLUTIONS), n_scenes)
+    br = dict(DEFAULT_BRANCHING)
+    br.update(branching or {})
+    jobs = [(i, seed * 1_000_003 + i, int(counts[i]), int(res[i]), tuple(br[int(res[i])]), width, height, shadows)
+            for i in range(n_scenes)]
+    if processes > 1 and n_scenes > 1:
+        import multiprocessing as mp
+        with mp.get_context("spawn").Pool(processes) as pool:
+            out = pool.map(_batch_scene, jobs, chunksize=max(1, n_scenes // (4 * processes)))
+    else:
+        out = [_batch_scene(j) for j in jobs]
+    for sc in out:
+        sc.shape = Tape.from_dag(*sc.shape)
+    return out

@@ -318,6 +318,16 @@ frep_status frep_batch_run(frep_batch* batch, const frep_tape* const* tapes, con
                            const frep_camera* cameras, const frep_lights* lights, const frep_image* images,
                            int use_graph, void* stream);
 
+/* Profiling of plain (non-graph) batch calls: with profiling on,
+ * frep_batch_voxelize and frep_batch_render record events between their
+ * launches. frep_batch_timings waits for them and returns device milliseconds:
+ * ms[3 l + k] = level l's pass of kind k (0 interval, 1 point with 4 cells per
+ * lane, 2 point with 2 cells per lane; each with its work-scan launch),
+ * ms[3 FREP_MAX_LEVELS] = root copy + header reset, ms[3 FREP_MAX_LEVELS + 1]
+ * = the frames (0 if none were rendered since profiling was enabled). */
+frep_status frep_batch_set_profiling(frep_batch* batch, int enable);
+frep_status frep_batch_timings(frep_batch* batch, float ms[3 * FREP_MAX_LEVELS + 2]);
+
 #ifdef __cplusplus
 }
 #endif
