@@ -1,12 +1,21 @@
-"""Benchmark: scenes/s of voxelize + render on the large single-scene workload.
+"""Benchmark: scenes/s of voxelize + render, batched vs plain, on one B200.
 
-Workload (BASELINE's large scene): 256 primitives (sphere / box / capsule,
-sizes U[0.02, 0.2]) combined by a random binary tree of min / max / max(a,-b)
-/ polynomial smooth-min; 3-level tree {16, 16, 8} = 2048^3 effective; 1920x1080
-perspective render at 60 degrees with one shadow ray per hit. Seeded synthetic
-scene (the reference ships no dataset).
+Default workload (`--workload batch`): 512 independent scenes, each a random
+CSG of sphere / box / capsule primitives (sizes U[0.02, 0.2]) combined by a
+random binary tree of min / max / max(a,-b) / polynomial smooth-min, with
+primitive counts log-uniform in [4, 1024] and effective resolutions drawn from
+{64, 128, 256, 512, 1024}^3; every scene rendered at 512x512 from its own
+orbit camera (60 degrees) with one shadow ray per hit. Branching, last-level
+tile and tapes per block are chosen by the autotuner before timing. One step =
+the whole batch voxelized and rendered (one frep_batch_run, CUDA graph
+replay). The same trees are also run as 512 sequential plain launches
+(frep_voxelize + frep_render per scene) for the batched/plain ratio.
 
-One step = one full voxelization (every level pass) + one rendered frame.
+`--workload large`: one scene of 256 primitives on a {16, 16, 8} = 2048^3
+tree, 1920x1080 perspective + shadow rays; one step = one voxelization + one
+frame.
+
+Seeded synthetic scenes (the reference ships no dataset).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -43,17 +52,28 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=("batch", "large"), default="batch")
+    ap.add_argument("--scenes", type=int, default=512, help="batch: number of scenes")
+    ap.add_argument("--plain-steps", type=int, default=2, help="batch: timed passes of the plain launch loop")
+    ap.add_argument("--no-tune", action="store_true", help="batch: default branching, no autotuning")
+    ap.add_argument("--tune-cache", default=None, help="batch: autotuner cache file (JSON)")
+    ap.add_argument("--budget-gb", type=int, default=150, help="HBM budget of the context, GB")
     ap.add_argument("--grid", default="16,16,8",
-                    help="tree branching per level (profiling uses a smaller grid of the same scene)")
-    ap.add_argument("--res", default="1920x1080", help="render resolution WxH")
-    ap.add_argument("--pool-mb", type=int, default=3072, help="node + tape pool size of the tree, MB")
+                    help="large: tree branching per level (profiling uses a smaller grid of the same scene)")
+    ap.add_argument("--res", default=None, help="render resolution WxH (batch 512x512, large 1920x1080)")
+    ap.add_argument("--pool-mb", type=int, default=3072, help="large: node + tape pool size of the tree, MB")
     args = ap.parse_args()
     args.grid_dims = tuple(int(v) for v in args.grid.split(","))
+    if args.res is None:
+        args.res = "512x512" if args.workload == "batch" else "1920x1080"
     args.width, args.height = (int(v) for v in args.res.lower().split("x"))
     fine = 1
     for d in args.grid_dims:
         fine *= d
-    args.workload = f"random_csg_256prim_{fine}cube_{args.width}x{args.height}_shadow"
+    if args.workload == "batch":
+        args.workload_name = (f"batch_{args.scenes}scenes_4-1024prim_64-1024cube_{args.width}x{args.height}_shadow")
+    else:
+        args.workload_name = f"random_csg_256prim_{fine}cube_{args.width}x{args.height}_shadow"
     return args
 
 
@@ -190,7 +210,7 @@ def run_reference(args, world, rank):
         "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "impl": "reference",
-        "config": {"workload": args.workload, "grid": list(args.grid_dims), "resolution": [args.width, args.height],
+        "config": {"workload": args.workload_name, "grid": list(args.grid_dims), "resolution": [args.width, args.height],
                    "shadow_rays": 1, "rounding": "outward"},
         "cpu_baseline": {"value": value, "unit": "scenes/s", "cores": threads, "kind": "port",
                          "sample": f"{args.steps} full scenes (voxelize + 1080p render), oracle C++ port, "
@@ -304,7 +324,7 @@ def run_ours(args, world, rank, local):
         "metric": METRIC, "value": value, "unit": "scenes/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": args.workload, "grid": scene.grid_dims, "resolution": [W, H], "shadow_rays": 1,
+        "config": {"workload": args.workload_name, "grid": scene.grid_dims, "resolution": [W, H], "shadow_rays": 1,
                    "tape_instructions": vs.tape.n_instr, "rounding": "outward",
                    "nodes_per_level": list(info.node_count[:vs.grid_levels]),
                    "l2": "flushed between timed steps (256 MB write, outside the step events)",
@@ -326,15 +346,282 @@ def run_ours(args, world, rank, local):
     vs.cleanup()
     ctx.close()
 
+# ---- many-scene batch ----------------------------------------------------------------
+
+def make_batch_scenes(args, world: int = 1):
+    """The batch workload with one orbit camera per scene (seeded)."""
+    import numpy as np
+    from frep import scenes
+    procs = max(1, min(32, (os.cpu_count() or 1) // max(1, world)))
+    scs = scenes.batch_workload(args.scenes, seed=3, width=args.width, height=args.height, processes=procs)
+    rng = np.random.default_rng(11)
+    for sc in scs:
+        sc.camera = scenes.orbit_camera(rng)
+    return scs
+
+
+def oracle_scene_seconds(scene, dims, threads: int) -> float:
+    """Oracle (C++ restatement of the reference's shaders): one voxelization +
+    one frame of `scene` on `threads` host threads, in seconds."""
+    sys.path.insert(0, str(REPO / "oracle"))
+    import oracle
+    import frep
+    tape = scene.shape
+    t0 = time.perf_counter()
+    tree = oracle.OracleTree(tape.wide(), tape.n_slots, list(dims), scene.low_vertex, scene.world_size,
+                             rounding=1, threads=threads)
+    tree.render(oracle.camera_vector(scene.camera, scene.width, scene.height),
+                frep.Lights(shadow_mask=scene.shadow_mask), threads=threads)
+    return time.perf_counter() - t0
+
+
+def cpu_sample_order(n: int):
+    import numpy as np
+    return [int(i) for i in np.random.default_rng(17).permutation(n)]
+
+
+def run_reference_batch(args, world, rank):
+    """--impl reference on the batch workload: each step is the next scene of
+    a seeded permutation of the batch, voxelized + rendered by the oracle on
+    all host threads; value = scenes / total seconds."""
+    if rank != 0:
+        return
+    from frep import scenes as S
+    scs = make_batch_scenes(args)
+    threads = os.cpu_count() or 1
+    order = cpu_sample_order(len(scs))
+    pick = lambda i: scs[order[i % len(order)]]
+    for i in range(args.warmup):
+        sc = pick(i)
+        oracle_scene_seconds(sc, S.DEFAULT_BRANCHING[sc.meta["res"]], threads)
+    times = []
+    for i in range(args.steps):
+        sc = pick(args.warmup + i)
+        times.append(oracle_scene_seconds(sc, S.DEFAULT_BRANCHING[sc.meta["res"]], threads))
+    total = sum(times)
+    value = args.steps / total
+    sample = (f"{args.steps} scenes of the batch (seeded permutation, after {args.warmup} warm-up scenes), "
+              f"each voxelized at its default branching + rendered {args.width}x{args.height}; "
+              f"oracle C++ port, {threads} threads")
+    line = {
+        "metric": METRIC, "value": value, "unit": "scenes/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+        "config": {"workload": args.workload_name, "scenes": args.scenes, "resolution": [args.width, args.height],
+                   "shadow_rays": 1, "rounding": "outward"},
+        "cpu_baseline": {"value": value, "unit": "scenes/s", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "scenes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours_batch(args, world, rank, local):
+    import numpy as np
+    import torch
+    import frep
+    from frep.autotune import Autotuner, fit_pools
+
+    scs = make_batch_scenes(args, world)  # spawned workers, before any CUDA work
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    ctx = frep.Context(local, hbm_budget_bytes=args.budget_gb << 30)
+    stream = torch.cuda.current_stream()
+
+    # ---- untimed setup: autotune, size the pools, build resident trees -------
+    t0 = time.perf_counter()
+    tuner = Autotuner(ctx, cache_path=args.tune_cache)
+    if not args.no_tune:
+        tuner.tune(scs)
+    t_tune = time.perf_counter() - t0
+    chosen = [tuner.apply(sc) for sc in scs]
+    pools = fit_pools(ctx, [sc.shape for sc in scs], [d for d, _ in chosen], scs[0].low_vertex, scs[0].world_size)
+    storages = []
+    for sc, (dims, k), p in zip(scs, chosen, pools):
+        vs = frep.VoxelStorage(dims, sc.low_vertex, sc.world_size, rounding=frep.ROUND_OUTWARD,
+                               node_words=p.node_words, tape_words=p.tape_words, point_cells_per_lane=k)
+        storages.append(vs.init(ctx, sc.shape))
+    batch = frep.Batch(ctx, storages)
+    batch.set_tuning(*tuner.warps)
+    W, H = args.width, args.height
+    n = len(scs)
+    rgba = torch.empty((n, H, W, 4), dtype=torch.uint8, device=dev)
+    frames = [rgba[i] for i in range(n)]
+    host_img = torch.empty((n, H, W, 4), dtype=torch.uint8, pin_memory=True)
+    cams = [sc.camera for sc in scs]
+    sizes = [(W, H)] * n
+    lights = frep.Lights(shadow_mask=scs[0].shadow_mask)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
+
+    def step():
+        batch.run(cams, sizes, frames, lights=lights, graph=True, stream=stream)
+
+    for _ in range(max(1, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    binfo = batch.info()
+
+    # ---- batched, device-resident (value) ------------------------------------
+    barrier(world)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(local) as clocks:
+        for s, e in evs:
+            flush.fill_(1)
+            s.record(stream)
+            step()
+            e.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    t_ms = max_over_ranks(world, sum(s.elapsed_time(e) for s, e in evs))
+    value = world * n * args.steps / (t_ms / 1e3)
+
+    # ---- plain: one frep_voxelize + frep_render per scene, in sequence --------
+    voxs = [frep.Voxelizer(ctx, vs) for vs in storages]
+    rts = []
+    for vs in storages:
+        rt = frep.Raytracer(ctx, vs)
+        rt.lights = lights
+        rts.append(rt)
+
+    def plain_pass():
+        for i in range(n):
+            voxs[i].voxelize(0.0, stream)
+            rts[i].trace(cams[i], 0.0, W, H, out=(frames[i], None), stream=stream)
+
+    plain_pass()
+    torch.cuda.synchronize()
+    barrier(world)
+    pevs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+            for _ in range(args.plain_steps)]
+    for s, e in pevs:
+        flush.fill_(1)
+        s.record(stream)
+        plain_pass()
+        e.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    p_ms = max_over_ranks(world, sum(s.elapsed_time(e) for s, e in pevs))
+    plain_value = world * n * args.plain_steps / (p_ms / 1e3)
+
+    # ---- per-launch timing of the batched passes (plain batch calls + events) -
+    batch.set_profiling(True)
+    reps = 3
+    acc = None
+    for _ in range(reps):
+        flush.fill_(1)
+        batch.voxelize(stream=stream)
+        batch.render(cams, sizes, frames, lights=lights, stream=stream)
+        tm = batch.timings()
+        grid_ms = np.array(tm["level"]) / reps
+        acc = grid_ms if acc is None else acc + grid_ms
+        render_ms = tm["render"]
+    batch.set_profiling(False)
+    # op-weighted FP32 work of each (level, kind) launch, summed over the trees
+    ops = np.zeros_like(acc)
+    cinstr = np.zeros_like(acc)
+    for vs, (dims, k) in zip(storages, chosen):
+        f = vs.fp32_ops()
+        c = vs.work()
+        kk = vs.point_cells_per_lane or (4 if (dims[-1] ** 3 // 32) % 4 == 0 else 2)
+        for l in range(len(dims)):
+            kind = 0 if l < len(dims) - 1 else (1 if kk == 4 else 2)
+            ops[l, kind] += f[l]
+            cinstr[l, kind] += c[l]
+    max_levels = max(len(d) for d, _ in chosen)
+    dom = np.unravel_index(int(np.argmax(acc)), acc.shape)
+    dom_ms = float(acc[dom])
+    peaks = measured_peaks()
+    sm_mhz = float(peaks.get("sm_max_mhz", 1965.0))
+    fp32_peak = SM_COUNT * FP32_LANES_PER_SM * sm_mhz * 1e6 / 1e12
+    achieved = float(ops[dom]) / (dom_ms / 1e3) / 1e12
+    kind_name = ["interval_level_kernel", "point_level_kernel (4 cells/lane)", "point_level_kernel (2 cells/lane)"]
+    total_ops = float(ops.sum())
+    roofline = {
+        "bound": "fp32", "kernel": kind_name[dom[1]], "level": int(dom[0]), "achieved": achieved,
+        "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": None,
+        "peak_source": "nominal FP32 issue: 148 SMs x 128 lanes x MEASURED_PEAKS.json sm_max_mhz "
+                       "(the file holds no FP32 figure)",
+        "algorithmic_ops_per_launch": float(ops[dom]), "cell_instr_per_launch": float(cinstr[dom]),
+        "ms_per_launch": dom_ms,
+        "all_level_passes": {"ops": total_ops, "ms": float(acc.sum()),
+                             "frac": total_ops / (float(acc.sum()) / 1e3) / 1e12 / fp32_peak},
+    }
+
+    # ---- end to end: public API with host buffers ----------------------------
+    torch.cuda.synchronize()
+    barrier(world)
+    e2e_evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(args.steps)]
+    for s, e in e2e_evs:
+        flush.fill_(1)
+        s.record(stream)
+        step()                                     # host tapes + frame args -> device inside
+        host_img.copy_(rgba, non_blocking=True)    # all frames -> host
+        e.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    e2e_ms = max_over_ranks(world, sum(s.elapsed_time(e) for s, e in e2e_evs))
+    e2e_value = world * n * args.steps / (e2e_ms / 1e3)
+
+    branching = {}
+    for sc, (dims, k) in zip(scs, chosen):
+        branching.setdefault(str(sc.meta["res"]), set()).add((tuple(dims), k))
+    instr = np.array([sc.shape.n_instr for sc in scs])
+    used = ctx.memory()[0]
+    line = {
+        "metric": METRIC, "value": value, "unit": "scenes/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload_name, "scenes": n, "resolution": [W, H], "shadow_rays": 1,
+                   "rounding": "outward", "tape_instructions": {"min": int(instr.min()),
+                                                                "median": float(np.median(instr)),
+                                                                "max": int(instr.max())},
+                   "branching": {r: sorted([list(d), k] for d, k in v) for r, v in sorted(branching.items())},
+                   "warps_per_block": [binfo.interval_warps_per_block, binfo.point_warps_per_block],
+                   "autotune_seconds": round(t_tune, 1), "resident_bytes": int(used),
+                   "l2": "flushed between timed steps (256 MB write, outside the step events)",
+                   "graph": "one CUDA graph per step (upload, level passes, frames)",
+                   "parallelism": f"replicas x{world}"},
+        "plain": {"value": plain_value, "unit": "scenes/s", "ms_per_pass": p_ms / args.plain_steps,
+                  "passes": args.plain_steps,
+                  "what": "same trees, frep_voxelize + frep_render per scene in sequence on one stream"},
+        "batched_over_plain": value / plain_value,
+        "roofline": roofline,
+        "level_ms": acc[:max_levels].round(3).tolist(),
+        "level_cell_instr": cinstr[:max_levels].tolist(),
+        "level_kinds": ["interval", "point 4 cells/lane", "point 2 cells/lane"],
+        "render_ms": render_ms,
+        "e2e": {"value": e2e_value, "unit": "scenes/s", "h2d_bytes_per_step": int(binfo.upload_bytes),
+                "d2h_bytes_per_step": int(n * W * H * 4)},
+        "clocks": clocks.summary(),
+        "gpu_launches": int((binfo.voxelize_launches + 1) * args.steps),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        order = cpu_sample_order(n)
+        spent, done = 0.0, 0
+        while done < min(n, 64) and spent < 15.0:
+            sc = scs[order[done]]
+            spent += oracle_scene_seconds(sc, chosen[order[done]][0], threads)
+            done += 1
+        line["cpu_baseline"] = {"value": done / spent, "unit": "scenes/s", "cores": threads, "kind": "port",
+                                "sample": f"{done} scenes of the batch (seeded permutation, until 15 s), "
+                                          f"voxelize + {W}x{H} render each, oracle C++ port, {threads} threads"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    batch.close()
+    for vs in storages:
+        vs.cleanup()
+    ctx.close()
+
 
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
     try:
         if args.impl == "reference":
-            run_reference(args, world, rank)
+            (run_reference_batch if args.workload == "batch" else run_reference)(args, world, rank)
         else:
-            run_ours(args, world, rank, local)
+            (run_ours_batch if args.workload == "batch" else run_ours)(args, world, rank, local)
     finally:
         if world > 1:
             import torch.distributed as dist

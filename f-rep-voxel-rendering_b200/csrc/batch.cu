@@ -44,6 +44,7 @@ struct frep_batch {
     frep::LevelPlan plan4{}, plan2{};
     uint32_t plan_slots = 0, plan_mm = 0;
     bool plan_valid = false;
+    int interval_warps = 0, point_warps = 0;  // tuning hints (0 = automatic)
     // profiling (plain launches only): ev[0] before the root copy, ev[1] after
     // it, ev[2 + 3 l + kind] after level l's pass of that kind (0 interval,
     // 1 point with 4 cells per lane, 2 point with 2); rev around the frames
@@ -52,6 +53,9 @@ struct frep_batch {
     uint32_t profiled_levels = 0;
     cudaEvent_t ev[2 + 3 * FREP_MAX_LEVELS] = {};
     cudaEvent_t rev[2] = {};
+    // what the last voxelization enqueued
+    uint64_t last_upload = 0;
+    uint32_t last_launches = 0;
     // graph replay
     cudaStream_t capture_stream = nullptr;
     cudaGraphExec_t graph = nullptr;
@@ -60,17 +64,27 @@ struct frep_batch {
 
 namespace {
 
+// The upload area: [tape times][root offsets][level-pass tree order][frame
+// arguments][root tapes]. Everything before the root tapes depends only on
+// the batch size.
 struct Layout {
-    size_t times = 0, offsets = 0, frames = 0, roots = 0, total = 0;
+    size_t times = 0, offsets = 0, order = 0, frames = 0, roots = 0, total = 0;
     std::vector<unsigned long long> root_ofs;  // n + 1, in words, relative to `roots`
 };
 
-Layout make_layout(const frep_batch* b, const frep_tape* const* tapes) {
+Layout base_layout(uint32_t n) {
     Layout L;
     L.times = 0;
-    L.offsets = align_up(sizeof(float) * b->n, 16);
-    L.frames = L.offsets + align_up(sizeof(unsigned long long) * (b->n + 1), 16);
-    L.roots = L.frames + align_up(sizeof(frep::RenderArgs) * b->n, 16);
+    L.offsets = align_up(sizeof(float) * n, 16);
+    L.order = L.offsets + align_up(sizeof(unsigned long long) * (n + 1), 16);
+    L.frames = L.order + align_up(sizeof(void*) * n, 16);
+    L.roots = L.frames + align_up(sizeof(frep::RenderArgs) * n, 16);
+    L.total = L.roots;
+    return L;
+}
+
+Layout make_layout(const frep_batch* b, const frep_tape* const* tapes) {
+    Layout L = base_layout(b->n);
     L.root_ofs.resize(b->n + 1);
     unsigned long long w = 0;
     for (uint32_t i = 0; i < b->n; i++) {
@@ -144,7 +158,7 @@ frep_status check_tapes(frep_batch* b, const frep_tape* const* tapes, TapeStats*
         st->mm = std::max<uint32_t>(st->mm, t->ct.n_minmax);
         st->longest = std::max<uint32_t>(st->longest, (uint32_t)t->ct.instrs.size());
         st->max_levels = std::max<uint32_t>(st->max_levels, tr->grid.levels);
-        const int k = frep::point_k_for(tr->grid.dims[tr->grid.levels - 1]);
+        const int k = tr->point_k;
         (k == 4 ? st->any_k4 : st->any_k2) = true;
     }
     return FREP_OK;
@@ -152,8 +166,9 @@ frep_status check_tapes(frep_batch* b, const frep_tape* const* tapes, TapeStats*
 
 frep_status ensure_plans(frep_batch* b, const TapeStats& st) {
     if (b->plan_valid && b->plan_slots == st.slots && b->plan_mm == st.mm) return FREP_OK;
-    cudaError_t e = frep::plan_levels(st.slots, st.mm, 4, b->rounding, &b->plan4);
-    if (e == cudaSuccess) e = frep::plan_levels(st.slots, st.mm, 2, b->rounding, &b->plan2);
+    cudaError_t e = frep::plan_levels(st.slots, st.mm, 4, b->rounding, &b->plan4, b->interval_warps, b->point_warps);
+    if (e == cudaSuccess)
+        e = frep::plan_levels(st.slots, st.mm, 2, b->rounding, &b->plan2, b->interval_warps, b->point_warps);
     if (e == cudaErrorInvalidValue)
         return fail(FREP_ERR_UNSUPPORTED, "frep_batch: %u slots / %u min-max ops exceed shared memory", st.slots, st.mm);
     if (e != cudaSuccess) return cuda_fail(e, "plan_levels");
@@ -175,12 +190,16 @@ frep_status enqueue_voxelize(frep_batch* b, const TapeStats& st, const Layout& L
     if (e != cudaSuccess) return cuda_fail(e, "tree_init_staged_kernel");
     if (prof) FREP_CUDA(cudaEventRecord(b->ev[1], s));
     frep::LevelLaunch a{};
-    a.trees = b->d_trees;
+    // The level passes walk the trees longest root tape first (staged order):
+    // warps take the costliest items first and the cheap ones fill the tail.
+    a.trees = reinterpret_cast<frep::dev::TreeHeader* const*>(b->d_stage + L.order);
     a.prefix = b->d_prefix;
     a.cursor = b->d_cursor;
     a.n_trees = b->n;
     a.keep_scratch = b->keep;
-    a.keep_stride = (uint32_t)align_up(st.longest, 32);
+    const frep::WarpScratch ws = frep::warp_scratch(st.longest, st.mm);
+    a.keep_stride = ws.stride;
+    a.mm_ofs = ws.mm_ofs;
     a.n_slots = st.slots;
     a.mm_cap = st.mm;
     for (uint32_t l = 0; l < st.max_levels; l++) {
@@ -207,6 +226,8 @@ frep_status enqueue_voxelize(frep_batch* b, const TapeStats& st, const Layout& L
         b->profiled = true;
         b->profiled_levels = st.max_levels;
     }
+    b->last_launches = 1 + 2 * st.max_levels * (1u + (st.any_k4 ? 1u : 0u) + (st.any_k2 ? 1u : 0u));
+    b->last_upload = L.total;
     return FREP_OK;
 }
 
@@ -222,11 +243,19 @@ void mark_voxelized(frep_batch* b, const frep_tape* const* tapes, cudaStream_t s
     }
 }
 
-// Writes the host part of the upload area: tape times, root offsets, roots.
+// Writes the host part of the upload area: tape times, root offsets, the
+// level-pass order (headers by descending root tape length), roots.
 void stage_inputs(frep_batch* b, const frep_tape* const* tapes, const float* tape_times, const Layout& L) {
     float* times = reinterpret_cast<float*>(b->h_stage + L.times);
     for (uint32_t i = 0; i < b->n; i++) times[i] = tape_times ? tape_times[i] : 0.0f;
     std::memcpy(b->h_stage + L.offsets, L.root_ofs.data(), sizeof(unsigned long long) * (b->n + 1));
+    std::vector<uint32_t> idx(b->n);
+    for (uint32_t i = 0; i < b->n; i++) idx[i] = i;
+    std::stable_sort(idx.begin(), idx.end(), [&](uint32_t x, uint32_t y) {
+        return tapes[x]->ct.instrs.size() > tapes[y]->ct.instrs.size();
+    });
+    auto** order = reinterpret_cast<frep::dev::TreeHeader**>(b->h_stage + L.order);
+    for (uint32_t i = 0; i < b->n; i++) order[i] = b->trees[idx[i]]->hdr;
     uint64_t* roots = reinterpret_cast<uint64_t*>(b->h_stage + L.roots);
     for (uint32_t i = 0; i < b->n; i++)
         std::memcpy(roots + L.root_ofs[i], tapes[i]->record.data(), tapes[i]->record.size() * 8);
@@ -326,10 +355,10 @@ frep_status frep_batch_voxelize(frep_batch* b, const frep_tape* const* tapes, co
     if (r == FREP_OK) r = ensure_stage(b, L.total);
     if (r == FREP_OK) r = ensure_keep(b, (uint64_t)std::max(b->plan4.blocks * b->plan4.warps_per_block,
                                                            b->plan2.blocks * b->plan2.warps_per_block) *
-                                             align_up(st.longest, 32));
+                                             frep::warp_scratch(st.longest, st.mm).stride);
     if (r != FREP_OK) return r;
     stage_inputs(b, tapes, tape_times, L);
-    FREP_CUDA(cudaMemcpyAsync(b->d_stage, b->h_stage, L.frames, cudaMemcpyHostToDevice, s));
+    FREP_CUDA(cudaMemcpyAsync(b->d_stage, b->h_stage, L.frames, cudaMemcpyHostToDevice, s));  // times..order
     FREP_CUDA(cudaMemcpyAsync(b->d_stage + L.roots, b->h_stage + L.roots, L.total - L.roots,
                               cudaMemcpyHostToDevice, s));
     FREP_CUDA(cudaEventRecord(b->upload_done, s));
@@ -346,10 +375,7 @@ frep_status frep_batch_render(frep_batch* b, const frep_camera* cameras, const f
     cudaStream_t s = (cudaStream_t)stream_ptr;
     // Frame arguments go to the upload area's frame block; make sure it is large
     // enough even before the first voxelization.
-    Layout L;
-    L.offsets = align_up(sizeof(float) * b->n, 16);
-    L.frames = L.offsets + align_up(sizeof(unsigned long long) * (b->n + 1), 16);
-    L.roots = L.frames + align_up(sizeof(frep::RenderArgs) * b->n, 16);
+    const Layout L = base_layout(b->n);
     frep_status r = ensure_stage(b, std::max<size_t>(L.roots, b->stage_bytes));
     if (r != FREP_OK) return r;
     uint32_t mw, mh, ms;
@@ -387,7 +413,7 @@ frep_status frep_batch_run(frep_batch* b, const frep_tape* const* tapes, const f
     if (r == FREP_OK) r = ensure_stage(b, L.total);
     if (r == FREP_OK) r = ensure_keep(b, (uint64_t)std::max(b->plan4.blocks * b->plan4.warps_per_block,
                                                            b->plan2.blocks * b->plan2.warps_per_block) *
-                                             align_up(st.longest, 32));
+                                             frep::warp_scratch(st.longest, st.mm).stride);
     if (r != FREP_OK) return r;
     // Fill the whole upload area (the graph's memcpy node reads it when it runs).
     // The frame arguments describe the trees as this run leaves them.
@@ -398,7 +424,9 @@ frep_status frep_batch_run(frep_batch* b, const frep_tape* const* tapes, const f
     if (r != FREP_OK) return r;
     // The graph stays valid while the batch keeps its shape.
     std::vector<uint64_t> key = {L.total, st.slots, st.mm, st.longest, st.max_levels, mw, mh, ms,
-                                 (uint64_t)b->plan4.blocks, (uint64_t)(uintptr_t)b->keep, (uint64_t)(uintptr_t)b->d_stage};
+                                 (uint64_t)b->plan4.blocks, (uint64_t)b->plan4.warps_per_block,
+                                 (uint64_t)b->plan4.point_warps_per_block, (uint64_t)b->plan2.point_warps_per_block,
+                                 (uint64_t)(uintptr_t)b->keep, (uint64_t)(uintptr_t)b->d_stage};
     for (uint32_t i = 0; i < b->n; i++) key.push_back(L.root_ofs[i]);
     if (!b->graph || key != b->graph_key) {
         if (b->graph) {
@@ -428,6 +456,28 @@ frep_status frep_batch_run(frep_batch* b, const frep_tape* const* tapes, const f
     }
     FREP_CUDA(cudaGraphLaunch(b->graph, s));
     FREP_CUDA(cudaEventRecord(b->upload_done, s));
+    return FREP_OK;
+}
+
+frep_status frep_batch_get_info(const frep_batch* b, frep_batch_info* info) {
+    if (!b || !info) return fail(FREP_ERR_INVALID_ARG, "frep_batch_get_info: null argument");
+    info->n_trees = b->n;
+    info->voxelize_launches = b->last_launches;
+    info->upload_bytes = b->last_upload;
+    info->device_bytes = b->bytes;
+    info->interval_warps_per_block = b->plan_valid ? (uint32_t)b->plan4.warps_per_block : 0;
+    info->point_warps_per_block = b->plan_valid ? (uint32_t)b->plan4.point_warps_per_block : 0;
+    return FREP_OK;
+}
+
+frep_status frep_batch_set_tuning(frep_batch* b, uint32_t interval_warps_per_block, uint32_t point_warps_per_block) {
+    if (!b) return fail(FREP_ERR_INVALID_ARG, "frep_batch_set_tuning: null batch");
+    auto ok = [](uint32_t w) { return w == 0 || w == 1 || w == 4; };
+    if (!ok(interval_warps_per_block) || !ok(point_warps_per_block))
+        return fail(FREP_ERR_INVALID_ARG, "frep_batch_set_tuning: warps per block must be 0, 1 or 4");
+    b->interval_warps = (int)interval_warps_per_block;
+    b->point_warps = (int)point_warps_per_block;
+    b->plan_valid = false;
     return FREP_OK;
 }
 

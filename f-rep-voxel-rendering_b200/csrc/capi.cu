@@ -177,6 +177,19 @@ frep_status frep_tree_create(frep_ctx* ctx, const frep_grid* grid, const frep_vo
     if (opts) t->opts = *opts;
     else { t->opts.rounding = FREP_ROUND_OUTWARD; t->opts.shorten = 1; }
     if (t->opts.rounding > 1) { delete t; return fail(FREP_ERR_INVALID_ARG, "opts.rounding must be 0 or 1"); }
+    {
+        const uint32_t dl = grid->dims[grid->levels - 1];
+        const uint32_t k = t->opts.point_cells_per_lane;
+        if (k != 0 && k != 2 && k != 4) {
+            delete t;
+            return fail(FREP_ERR_INVALID_ARG, "opts.point_cells_per_lane must be 0, 2 or 4");
+        }
+        if (k == 4 && (dl * dl * dl / 32) % 4 != 0) {
+            delete t;
+            return fail(FREP_ERR_INVALID_ARG, "opts.point_cells_per_lane = 4 needs a last-level dim of 8 or more");
+        }
+        t->point_k = k ? (int)k : frep::point_k_for(dl);
+    }
     // Cell sizes by successive division (voxelizer.cpp:209-216).
     float cs = grid->world_size;
     uint64_t dense_nodes = 1, dense_words = 0;
@@ -227,6 +240,7 @@ frep_status frep_tree_create(frep_ctx* ctx, const frep_grid* grid, const frep_vo
         h.cell_size[l] = t->cell_size[l];
     }
     for (int k = 0; k < 3; k++) h.low[k] = grid->low_vertex[k];
+    h.point_k = (uint32_t)t->point_k;
     t->d_self = reinterpret_cast<frep::dev::TreeHeader**>(t->d_small);
     t->d_prefix = t->d_small + 1;
     t->d_cursor = t->d_small + 3;
@@ -275,7 +289,7 @@ frep_status ensure_plan(frep_tree* tree, const frep_tape* tape, const char* who)
     if (tree->plan_valid && tree->plan_slots == n_slots && tree->plan_mm == tape->ct.n_minmax &&
         tree->plan_round == tree->opts.rounding)
         return FREP_OK;
-    const int k = frep::point_k_for(tree->grid.dims[tree->grid.levels - 1]);
+    const int k = tree->point_k;
     cudaError_t e = frep::plan_levels(n_slots, tape->ct.n_minmax, k, (int)tree->opts.rounding, &tree->plan);
     if (e == cudaErrorInvalidValue)
         return fail(FREP_ERR_UNSUPPORTED, "%s: %u slots / %u min-max ops exceed shared memory", who, n_slots,
@@ -291,7 +305,7 @@ frep_status ensure_plan(frep_tree* tree, const frep_tape* tape, const char* who)
 // Enqueues init + every level pass of one tree whose root tape is already at
 // word 0 of its pool. `plan` may narrow the grid (the static-scratch path).
 frep_status enqueue_tree_levels(frep_tree* tree, const frep_tape* tape, float tape_time, uint32_t* keep,
-                                uint32_t keep_stride, const frep::LevelPlan& plan, cudaStream_t stream) {
+                                frep::WarpScratch ws, const frep::LevelPlan& plan, cudaStream_t stream) {
     cudaError_t e = frep::launch_tree_init(tree->d_self, 1, nullptr, tape_time, stream);
     if (e != cudaSuccess) return cuda_fail(e, "tree_init_kernel");
     const frep_grid& g = tree->grid;
@@ -302,7 +316,8 @@ frep_status enqueue_tree_levels(frep_tree* tree, const frep_tape* tape, float ta
     a.cursor = tree->d_cursor;
     a.n_trees = 1;
     a.keep_scratch = keep;
-    a.keep_stride = keep_stride;
+    a.keep_stride = ws.stride;
+    a.mm_ofs = ws.mm_ofs;
     a.n_slots = std::max<uint32_t>(tape->ct.n_slots, 4);
     a.mm_cap = std::max<uint32_t>(tape->ct.n_minmax, 1);
     for (uint32_t l = 0; l < g.levels; l++) {
@@ -336,9 +351,9 @@ frep_status frep_voxelize(frep_ctx* ctx, frep_tree* tree, const frep_tape* tape,
 
     frep_status pst = ensure_plan(tree, tape, "frep_voxelize");
     if (pst != FREP_OK) return pst;
-    // Per-warp keep-ballot scratch: one word per instruction of the longest tape.
-    const uint32_t keep_stride = (uint32_t)align_up(std::max<uint32_t>(n, 1), 32);
-    const uint64_t keep_words = (uint64_t)tree->plan.blocks * tree->plan.warps_per_block * keep_stride;
+    // Per-warp scratch: a keep mask per instruction, a choice-mask pair per MIN/MAX.
+    const frep::WarpScratch ws = frep::warp_scratch(n, tape->ct.n_minmax);
+    const uint64_t keep_words = (uint64_t)tree->plan.blocks * tree->plan.warps_per_block * ws.stride;
     if (keep_words > tree->keep_words) {
         if (tree->keep) {
             cudaStreamSynchronize(tree->stream);
@@ -376,7 +391,7 @@ frep_status frep_voxelize(frep_ctx* ctx, frep_tree* tree, const frep_tape* tape,
     tree->root_words = (uint32_t)root_words;
     tree->stream = stream;
 
-    return enqueue_tree_levels(tree, tape, tape_time, tree->keep, keep_stride, tree->plan, stream);
+    return enqueue_tree_levels(tree, tape, tape_time, tree->keep, ws, tree->plan, stream);
 }
 
 frep_status frep_tree_sync(frep_tree* tree, frep_tree_info* info) {
@@ -603,8 +618,9 @@ frep_status frep_render(frep_ctx* ctx, const frep_tree* tree, const frep_camera*
 // straight from the tape object, so it makes no allocation at all.
 namespace {
 
-// 8 MiB of keep-ballot scratch (one 32-bit lane mask per tape instruction per
-// resident warp). Every GPU that loads the library holds it until exit.
+// 8 MiB of interval-pass scratch (per resident warp: a 32-bit lane mask per
+// tape instruction and a pair per MIN/MAX). Every GPU that loads the library
+// holds it until exit.
 constexpr uint64_t kStaticScratchWords = 2ull << 20;
 static __device__ __align__(256) uint32_t g_static_scratch[kStaticScratchWords];
 
@@ -647,16 +663,16 @@ extern "C" frep_status frep_voxelize_static_scratch(frep_ctx* ctx, frep_tree* tr
                     (unsigned long long)root_words);
     frep_status pst = ensure_plan(tree, tape, "frep_voxelize_static_scratch");
     if (pst != FREP_OK) return pst;
-    // Each resident warp owns keep_stride words of the array; launch only as
-    // many blocks as fit, and refuse tapes too long for even one block.
-    const uint32_t keep_stride = (uint32_t)align_up(std::max<uint32_t>(n, 1), 32);
-    const uint64_t per_block = (uint64_t)tree->plan.warps_per_block * keep_stride;
+    // Each resident warp owns ws.stride words of the array (a keep mask per
+    // instruction, a choice-mask pair per MIN/MAX); launch only as many blocks
+    // as fit, and refuse tapes too long for even one block.
+    const frep::WarpScratch ws = frep::warp_scratch(n, tape->ct.n_minmax);
+    const uint64_t per_block = (uint64_t)tree->plan.warps_per_block * ws.stride;
     if (per_block > kStaticScratchWords)
         return fail(FREP_ERR_UNSUPPORTED,
-                    "frep_voxelize_static_scratch: a root tape of %u instructions needs %llu scratch words per block; "
-                    "the static scratch holds %llu (at most %llu instructions)",
-                    n, (unsigned long long)per_block, (unsigned long long)kStaticScratchWords,
-                    (unsigned long long)(kStaticScratchWords / tree->plan.warps_per_block / 32 * 32));
+                    "frep_voxelize_static_scratch: a root tape of %u instructions (%u MIN/MAX) needs %llu scratch "
+                    "words per block; the static scratch holds %llu",
+                    n, tape->ct.n_minmax, (unsigned long long)per_block, (unsigned long long)kStaticScratchWords);
     frep::LevelPlan plan = tree->plan;
     plan.blocks = (int)std::min<uint64_t>((uint64_t)plan.blocks, kStaticScratchWords / per_block);
 
@@ -668,5 +684,5 @@ extern "C" frep_status frep_voxelize_static_scratch(frep_ctx* ctx, frep_tree* tr
     tree->root_words = (uint32_t)root_words;
     tree->stream = stream;
 
-    return enqueue_tree_levels(tree, tape, tape_time, scratch, keep_stride, plan, stream);
+    return enqueue_tree_levels(tree, tape, tape_time, scratch, ws, plan, stream);
 }

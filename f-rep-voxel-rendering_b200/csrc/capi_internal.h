@@ -61,6 +61,7 @@ struct frep_tree {
     frep_ctx* ctx = nullptr;
     frep_grid grid{};
     frep_voxelize_opts opts{};
+    int point_k = 4;  // cells per lane of the last-level pass
     float cell_size[FREP_MAX_LEVELS] = {};
     uint32_t node_size[FREP_MAX_LEVELS] = {};
     frep::dev::TreeHeader* hdr = nullptr;

@@ -34,6 +34,7 @@ struct TreeHeader {
     uint32_t node_size[MAX_LEVELS];            // u32 words
     float cell_size[MAX_LEVELS];
     float low[3];
+    uint32_t point_k;                          // last-level pass: cells per lane (2 or 4)
     // ---- per voxelization ----
     float tape_time;
     uint32_t node_count[MAX_LEVELS];           // interiorNodeCount

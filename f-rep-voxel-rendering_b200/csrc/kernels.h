@@ -18,12 +18,25 @@ struct LevelLaunch {
     unsigned long long* cursor;        // device work cursor
     uint32_t n_trees;
     uint32_t level;
-    uint32_t* keep_scratch;            // per-warp keep masks (global scratch)
-    uint32_t keep_stride;              // u32 words per warp (>= longest tape)
+    uint32_t* keep_scratch;            // per-warp global scratch of the interval pass:
+    uint32_t keep_stride;              //   u32 words per warp: keep masks [mm_ofs words,
+    uint32_t mm_ofs;                   //   >= longest tape] then MIN/MAX choice masks
     uint32_t n_slots;                  // slot-file rows per lane (max over the batch)
     uint32_t mm_cap;                   // MIN/MAX choice entries per warp (max over the batch)
     uint32_t smem_per_warp;            // bytes (set by launch_level from the plan)
 };
+
+// Per-warp global scratch of the interval pass, in u32 words: one keep mask per
+// instruction of the longest tape, then a pair of choice masks per MIN/MAX.
+struct WarpScratch {
+    uint32_t stride;  // words per warp
+    uint32_t mm_ofs;  // where the choice masks start
+};
+inline WarpScratch warp_scratch(uint32_t longest, uint32_t mm_cap) {
+    const uint32_t k = ((longest ? longest : 1u) + 31u) / 32u * 32u;
+    const uint32_t m = (2u * (mm_cap ? mm_cap : 1u) + 31u) / 32u * 32u;
+    return WarpScratch{k + m, k};
+}
 
 // Launch geometry of the level passes for one (slot count, MIN/MAX count).
 struct LevelPlan {
@@ -38,7 +51,10 @@ struct LevelPlan {
 
 // Cells per lane the point pass uses for a last level of this dim.
 int point_k_for(uint32_t dim);
-cudaError_t plan_levels(uint32_t n_slots, uint32_t mm_cap, int point_k, int rounding, LevelPlan* plan);
+// interval_warps / point_warps: warps (tapes) per block, 0 = chosen from the
+// shared memory a warp needs, 1 or 4 = that many where shared memory allows.
+cudaError_t plan_levels(uint32_t n_slots, uint32_t mm_cap, int point_k, int rounding, LevelPlan* plan,
+                        int interval_warps = 0, int point_warps = 0);
 
 // Resets the headers of n trees (tape time from `tape_times`, or `tape_time`
 // when it is null) and writes their root nodes. Each tree's root tape must

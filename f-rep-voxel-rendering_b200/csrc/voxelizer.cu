@@ -61,55 +61,35 @@ __device__ __forceinline__ void sts_f4(uint32_t a, float4 v) {
 }
 
 // Decoded instruction as staged for execution (16 bytes):
-//   x: opcode (bits 0-7) | flags (below)
+//   x: opcode (bits 0-3) | F_FWD_A | F_FWD_B (point passes only)
 //   y: byte offset of the A slot row (CONST: the constant's bits)
-//   z: byte offset of the B slot row
+//   z: byte offset of the B slot row (slot 0 for unary opcodes)
 //   w: byte offset of the output slot row
-// A row holds 32 lanes x row_bytes. The flags describe how the interpreter
-// obtains the operands: the A/B value is either forwarded from the previous
-// instruction's result (it reads the slot that instruction wrote) or loaded
-// from the slot file one instruction ahead.
+// A row holds 32 lanes x row_bytes. F_FWD_A / F_FWD_B: the operand is the
+// previous instruction's output, so the point interpreter takes it from the
+// register holding that result instead of loading the slot row.
 constexpr uint32_t F_FWD_A = 1u << 4, F_FWD_B = 1u << 5;
 
 __host__ __device__ constexpr bool is_binary(uint32_t op) {
     return op == OP_ADD || op == OP_SUB || op == OP_MUL || op == OP_DIV || op == OP_MIN || op == OP_MAX;
 }
 
-// x = opcode | F_FWD_A if A is the previous instruction's output | F_FWD_B
-// likewise for B (binary ops). The interpreter switches on x, so every
-// (opcode, forwarding) combination is its own straight-line case.
 __device__ __forceinline__ uint4 decode(uint64_t w, uint32_t prev_out, uint32_t row_bytes) {
     const uint32_t op = w_op(w);
     const uint32_t stride = 32u * row_bytes;
     if (op == OP_CONST) return make_uint4(op, (uint32_t)(w >> 32), 0u, w_out(w) * stride);
-    const bool fa = w_a(w) == prev_out;
-    const bool fb = is_binary(op) && w_b(w) == prev_out;
-    return make_uint4(op | (fa ? F_FWD_A : 0u) | (fb ? F_FWD_B : 0u), w_a(w) * stride, w_b(w) * stride,
-                      w_out(w) * stride);
+    const bool bin = is_binary(op);
+    const uint32_t fa = w_a(w) == prev_out ? F_FWD_A : 0u;
+    const uint32_t fb = bin && w_b(w) == prev_out ? F_FWD_B : 0u;
+    return make_uint4(op | fa | fb, w_a(w) * stride, bin ? w_b(w) * stride : 0u, w_out(w) * stride);
 }
 
-// Case generators: one case per (opcode, forwarding) combination.
-#define FREP_CASES_BINARY(X, OPC) \
-    X(OPC, false, false)          \
-    X(OPC, true, false)           \
-    X(OPC, false, true)           \
-    X(OPC, true, true)
-#define FREP_CASES_UNARY(X, OPC) \
-    X(OPC, false, false)         \
-    X(OPC, true, false)
-#define FREP_ALL_CASES(X)               \
-    FREP_CASES_BINARY(X, OP_MUL)        \
-    FREP_CASES_BINARY(X, OP_SUB)        \
-    FREP_CASES_BINARY(X, OP_ADD)        \
-    FREP_CASES_BINARY(X, OP_MAX)        \
-    FREP_CASES_BINARY(X, OP_MIN)        \
-    FREP_CASES_BINARY(X, OP_DIV)        \
-    FREP_CASES_UNARY(X, OP_COPY)        \
-    FREP_CASES_UNARY(X, OP_SQRT)        \
-    FREP_CASES_UNARY(X, OP_NEG)         \
-    FREP_CASES_UNARY(X, OP_SIN)         \
-    FREP_CASES_UNARY(X, OP_COS)         \
-    FREP_CASES_UNARY(X, OP_EXP)
+// Dispatch of the interval interpreter: opcodes are tested in the order of
+// their frequency in CSG tapes (CONST ~26 %, SUB ~25 %, MUL ~25 %, ADD ~11 %,
+// MIN/MAX ~10 %, the rest ~2 %), so a typical instruction costs two or three
+// uniform compare-and-branch pairs; the rare opcodes share one switch. (This
+// measured ~20 % faster than one switch case per opcode and forwarding
+// combination; the point interpreter keeps that switch, below.)
 
 // Fetches the next chunk of work items for this warp. Returns the first item
 // of the chunk in *first and its size; 0 when the level is exhausted.
@@ -192,20 +172,25 @@ __device__ __forceinline__ LevelTree load_tree(TreeHeader* H, uint32_t L, bool p
 }
 
 // Stages the prefetched chunk `pre` (lane l of group q holds instruction
-// q*32 + l of the chunk), decoded with forwarding flags, into stage[]. The
-// first instruction of a chunk never forwards. Entries past the tape's end
-// decode to a flagless CONST, which is also the sentinel the interpreter reads
-// one past the last instruction.
+// q*32 + l of the chunk), decoded, into stage[]. FWD: mark operands forwarded
+// from the previous instruction (never for the first instruction of a chunk).
+// Entries past the tape's end decode to a CONST that is never executed;
+// stage[STAGE] is the same kind of entry, read (not executed) one past a full
+// chunk.
+template <bool FWD>
 __device__ __forceinline__ void stage_chunk(uint4* stage, const uint64_t (&pre)[STAGE / 32], uint32_t row_bytes,
                                             uint32_t lane) {
     uint32_t prev_group_last = 0xFFFFFFFFu;
 #pragma unroll
     for (int q = 0; q < (int)(STAGE / 32); q++) {
-        const uint32_t out = w_out(pre[q]);
-        uint32_t prev = __shfl_up_sync(0xFFFFFFFFu, out, 1);
-        if (lane == 0) prev = prev_group_last;
+        uint32_t prev = 0xFFFFFFFFu;
+        if constexpr (FWD) {
+            const uint32_t out = w_out(pre[q]);
+            prev = __shfl_up_sync(0xFFFFFFFFu, out, 1);
+            if (lane == 0) prev = prev_group_last;
+            prev_group_last = __shfl_sync(0xFFFFFFFFu, out, 31);
+        }
         stage[q * 32 + lane] = decode(pre[q], prev, row_bytes);
-        prev_group_last = __shfl_sync(0xFFFFFFFFu, out, 31);
     }
 }
 __device__ __forceinline__ void prefetch_chunk(uint64_t (&pre)[STAGE / 32], const uint64_t* tape, uint32_t base,
@@ -217,30 +202,43 @@ __device__ __forceinline__ void prefetch_chunk(uint64_t (&pre)[STAGE / 32], cons
     }
 }
 
-// One interval instruction with its operand sources fixed at compile time.
-// r: in = the previous instruction's result, out = this one's.
-template <int ROUND, uint32_t OP, bool FA, bool FB>
-__device__ __forceinline__ void iv_exec(const uint4 d, float2& r, uint32_t lane_base, uint32_t lane, uint2* mmb,
-                                        uint32_t& mm, uint32_t mm_cap) {
-    const float2 a = FA ? r : lds_f2(lane_base + d.y);
-    float2 b = make_float2(0.0f, 0.0f);
-    if constexpr (is_binary(OP)) b = FB ? r : lds_f2(lane_base + d.z);
-    r = iv_apply<ROUND>(OP, 0ull, a, b);
-    if constexpr (OP == OP_MIN || OP == OP_MAX) {
-        uint32_t c;
-        if constexpr (OP == OP_MIN) c = a.y < b.x ? MM_FIRST : (b.y < a.x ? MM_SECOND : MM_BOTH);
-        else c = a.y < b.x ? MM_SECOND : (b.y < a.x ? MM_FIRST : MM_BOTH);
+// One interval instruction (any opcode but CONST), dispatched by frequency.
+// MIN/MAX also record each lane's choice (interval.comp:140-155) as two
+// ballots: bit 0 = the first operand may be the result, bit 1 = the second.
+template <int ROUND>
+__device__ __forceinline__ float2 iv_exec(const uint4 d, uint32_t lane_base, uint32_t lane, uint2* mmb,
+                                          uint32_t& mm, uint32_t mm_cap) {
+    const uint32_t op = d.x;
+    const float2 a = lds_f2(lane_base + d.y);
+    const float2 b = lds_f2(lane_base + d.z);
+    if (op == OP_SUB)
+        return ROUND ? make_float2(__fsub_rd(a.x, b.y), __fsub_ru(a.y, b.x))
+                     : make_float2(__fsub_rn(a.x, b.y), __fsub_rn(a.y, b.x));
+    if (op == OP_MUL) return iv_mul<ROUND>(a, b);
+    if (op == OP_ADD)
+        return ROUND ? make_float2(__fadd_rd(a.x, b.x), __fadd_ru(a.y, b.y))
+                     : make_float2(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y));
+    if (op == OP_MIN || op == OP_MAX) {
+        const bool mx = op == OP_MAX;
+        const bool first_low = a.y < b.x, second_low = b.y < a.x;
+        uint32_t c = first_low ? (mx ? MM_SECOND : MM_FIRST) : (second_low ? (mx ? MM_FIRST : MM_SECOND) : MM_BOTH);
         const uint32_t b0 = __ballot_sync(0xFFFFFFFFu, c & 1u);
         const uint32_t b1 = __ballot_sync(0xFFFFFFFFu, c & 2u);
         if (lane == 0 && mm < mm_cap) mmb[mm] = make_uint2(b0, b1);
         mm++;
+        return mx ? make_float2(max_sel(a.x, b.x), max_sel(a.y, b.y))
+                  : make_float2(min_sel(a.x, b.x), min_sel(a.y, b.y));
     }
+    return iv_apply<ROUND>(op, 0ull, a, b);
 }
 
 // ---- interval level pass -------------------------------------------------------
 //
 // Per-warp shared memory: slots [n_slots][32] float2 | stage [STAGE] uint4 |
-// choice masks [mm_cap] uint2 | live [n_slots] u32.
+// live [n_slots] u32. Per-warp global scratch: keep masks (one per
+// instruction) | choice masks (a uint2 per MIN/MAX): they grow with the tape,
+// and in shared memory they would cap the resident warps for every tree of a
+// batch at what its longest tape allows.
 template <int ROUND, int WARPS>
 __global__ void __launch_bounds__(WARPS * 32)
 interval_level_kernel(LevelLaunch p) {
@@ -249,14 +247,14 @@ interval_level_kernel(LevelLaunch p) {
     unsigned char* wbase = smem + (size_t)warp * p.smem_per_warp;
     const uint32_t lane_base = smem_addr(wbase) + lane * 8;
     uint4* stage = reinterpret_cast<uint4*>(wbase + (size_t)p.n_slots * 256);
-    uint2* mmb = reinterpret_cast<uint2*>(wbase + (size_t)p.n_slots * 256 + (STAGE + 1) * 16);
-    uint32_t* live = reinterpret_cast<uint32_t*>(wbase + (size_t)p.n_slots * 256 + (STAGE + 1) * 16 + (size_t)p.mm_cap * 8);
+    uint32_t* live = reinterpret_cast<uint32_t*>(wbase + (size_t)p.n_slots * 256 + (STAGE + 1) * 16);
     if (lane == 0) stage[STAGE] = make_uint4(0u, 0u, 0u, 0u);  // sentinel past a full chunk
 
     const uint32_t L = p.level;
     const unsigned long long total = __ldcg(&p.prefix[p.n_trees]);
     const uint32_t chunk = chunk_for(total, gridDim.x * WARPS);
     uint32_t* keep = p.keep_scratch + (size_t)(blockIdx.x * WARPS + warp) * p.keep_stride;
+    uint2* mmb = reinterpret_cast<uint2*>(keep + p.mm_ofs);
 
     // The tree of the current item, and its statistics so far (flushed to its
     // header when the warp moves to another tree: stats_buf, main.comp:146-147).
@@ -326,29 +324,20 @@ interval_level_kernel(LevelLaunch p) {
             for (uint32_t base = 0; base < n; base += STAGE) {
                 const uint32_t m = min(STAGE, n - base);
                 __syncwarp();
-                stage_chunk(stage, pre, 8, lane);
+                stage_chunk<false>(stage, pre, 8, lane);
                 prefetch_chunk(pre, tape, base + STAGE, n, lane);
                 __syncwarp();
-                // r holds the previous instruction's result, so a forwarded
-                // operand costs nothing; the decode word of j+1 is read early.
+                // The decode word of j+1 is read one instruction early.
                 const uint32_t sbase = smem_addr(stage);
                 uint4 dn = lds_u4(sbase);
                 for (uint32_t j = 0; j < m; j++) {
                     const uint4 d = dn;
                     dn = lds_u4(sbase + (j + 1) * 16);
-                    switch (d.x) {
-                        case OP_CONST: {
-                            const float c = __uint_as_float(d.y);
-                            r = make_float2(c, c);
-                            break;
-                        }
-#define FREP_IV_CASE(OPC, FA, FB)                                                      \
-    case OPC | (FA ? F_FWD_A : 0u) | (FB ? F_FWD_B : 0u):                              \
-        iv_exec<ROUND, OPC, FA, FB>(d, r, lane_base, lane, mmb, mm, p.mm_cap);         \
-        break;
-                        FREP_ALL_CASES(FREP_IV_CASE)
-#undef FREP_IV_CASE
-                        default: break;
+                    if (d.x == OP_CONST) {
+                        const float c = __uint_as_float(d.y);
+                        r = make_float2(c, c);
+                    } else {
+                        r = iv_exec<ROUND>(d, lane_base, lane, mmb, mm, p.mm_cap);
                     }
                     sts_f2(lane_base + d.w, r);
                 }
@@ -544,6 +533,32 @@ __device__ __forceinline__ void sts_k(uint32_t a, const FK<K>& r) {
     else sts_f2(a, make_float2(r.v[0], r.v[1]));
 }
 
+// Case generators for the point interpreter's switch: one case per (opcode,
+// forwarding) combination, each straight-line code with its operand sources
+// fixed. (On the point pass, with four cells per lane and vector slot rows,
+// this measured faster than testing the frequent combinations first.)
+#define FREP_CASES_BINARY(X, OPC) \
+    X(OPC, false, false)          \
+    X(OPC, true, false)           \
+    X(OPC, false, true)           \
+    X(OPC, true, true)
+#define FREP_CASES_UNARY(X, OPC) \
+    X(OPC, false, false)         \
+    X(OPC, true, false)
+#define FREP_ALL_CASES(X)               \
+    FREP_CASES_BINARY(X, OP_MUL)        \
+    FREP_CASES_BINARY(X, OP_SUB)        \
+    FREP_CASES_BINARY(X, OP_ADD)        \
+    FREP_CASES_BINARY(X, OP_MAX)        \
+    FREP_CASES_BINARY(X, OP_MIN)        \
+    FREP_CASES_BINARY(X, OP_DIV)        \
+    FREP_CASES_UNARY(X, OP_COPY)        \
+    FREP_CASES_UNARY(X, OP_SQRT)        \
+    FREP_CASES_UNARY(X, OP_NEG)         \
+    FREP_CASES_UNARY(X, OP_SIN)         \
+    FREP_CASES_UNARY(X, OP_COS)         \
+    FREP_CASES_UNARY(X, OP_EXP)
+
 // One point instruction with its operand sources fixed at compile time.
 // r: in = the previous instruction's result, out = this one's.
 template <int K, uint32_t OP, bool FA, bool FB>
@@ -640,12 +655,11 @@ point_level_kernel(LevelLaunch p) {
                 const uint32_t m = min(STAGE, n - base);
                 if (!resident) {
                     __syncwarp();
-                    stage_chunk(stage, pre, ROW, lane);
+                    stage_chunk<true>(stage, pre, ROW, lane);
                     prefetch_chunk(pre, tape, base + STAGE, n, lane);
                     __syncwarp();
                 }
-                // r holds the previous instruction's result, so a forwarded
-                // operand costs nothing; the decode word of j+1 is read early.
+                // The decode word of j+1 is read one instruction early.
                 const uint32_t sbase = smem_addr(stage);
                 uint4 dn = lds_u4(sbase);
                 for (uint32_t j = 0; j < m; j++) {
@@ -656,9 +670,9 @@ point_level_kernel(LevelLaunch p) {
 #pragma unroll
                             for (int k = 0; k < K; k++) r.v[k] = __uint_as_float(d.y);
                             break;
-#define FREP_PT_CASE(OPC, FA, FB)                    \
+#define FREP_PT_CASE(OPC, FA, FB)                         \
     case OPC | (FA ? F_FWD_A : 0u) | (FB ? F_FWD_B : 0u): \
-        pt_exec<K, OPC, FA, FB>(d, r, lane_base);   \
+        pt_exec<K, OPC, FA, FB>(d, r, lane_base);         \
         break;
                         FREP_ALL_CASES(FREP_PT_CASE)
 #undef FREP_PT_CASE
@@ -697,7 +711,7 @@ __device__ __forceinline__ unsigned long long level_items(TreeHeader* H, uint32_
     if ((point != 0) != last) return 0;
     const uint32_t dim = H->dims[L];
     const uint32_t words = dim * dim * dim / 32;
-    if (point && point_k_of(dim) != point_k) return 0;
+    if (point && H->point_k != (uint32_t)point_k) return 0;
     const uint32_t count = level_count(H, L, H->node_cap, H->node_size[L]);
     if (!point && write_ofs) H->node_ofs[L + 1] = H->node_ofs[L] + (unsigned long long)count * H->node_size[L];
     return (unsigned long long)count * (point ? words / (uint32_t)point_k : words);
@@ -822,16 +836,22 @@ __global__ void count_ops_kernel(TreeHeader* H, const uint32_t* nodes, const uin
 
 namespace {
 
+// The kernel's dynamic shared memory limit is raised to the device's opt-in
+// maximum, never to this plan's size: plans are cached per tree and per batch,
+// and a smaller limit set by a later plan would make an earlier plan's
+// launches fail. The limit does not change occupancy; the launch's size does.
 template <typename Kern>
 cudaError_t occupancy(Kern kernel, int threads, size_t smem, int* blocks) {
-    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int dev = 0, sms = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (smem > (size_t)optin) return cudaErrorInvalidValue;
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
     if (e != cudaSuccess) return e;
-    int dev = 0, sms = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     *blocks = per_sm * sms;
     return cudaSuccess;
@@ -846,21 +866,24 @@ cudaError_t occupancy(Kern kernel, int threads, size_t smem, int* blocks) {
 int point_k_for(uint32_t dim) { return dev::point_k_of(dim); }
 
 template <int K>
-static cudaError_t plan_point(uint32_t n_slots, LevelPlan* plan) {
+static cudaError_t plan_point(uint32_t n_slots, LevelPlan* plan, int warps_hint) {
     const uint32_t pt = (uint32_t)(n_slots * 32 * 4 * K + (dev::STAGE + 1) * 16 + 15) / 16 * 16;
     plan->point_smem_per_warp = pt;
-    plan->point_warps_per_block = 4ull * pt <= 200 * 1024 ? 4 : 1;
+    plan->point_warps_per_block = 4ull * pt <= (warps_hint == 4 ? 227u : 200u) * 1024 && warps_hint != 1 ? 4 : 1;
     if (pt > 227 * 1024) return cudaErrorInvalidValue;
     if (plan->point_warps_per_block == 4)
         return occupancy(dev::point_level_kernel<4, K>, 128, 4 * pt, &plan->point_blocks);
     return occupancy(dev::point_level_kernel<1, K>, 32, pt, &plan->point_blocks);
 }
 
-cudaError_t plan_levels(uint32_t n_slots, uint32_t mm_cap, int point_k, int rounding, LevelPlan* plan) {
-    const uint32_t iv = (n_slots * 256 + (dev::STAGE + 1) * 16 + mm_cap * 8 + n_slots * 4 + 15) / 16 * 16;
+cudaError_t plan_levels(uint32_t n_slots, uint32_t mm_cap, int point_k, int rounding, LevelPlan* plan,
+                        int interval_warps, int point_warps) {
+    (void)mm_cap;  // the choice masks live in global scratch
+    const uint32_t iv = (n_slots * 256 + (dev::STAGE + 1) * 16 + n_slots * 4 + 15) / 16 * 16;
     plan->smem_per_warp = iv;
-    // Four warps per block when they fit in shared memory, else one.
-    const bool four = 4ull * iv <= 200 * 1024;
+    // Four warps (four tapes) per block when they fit in shared memory, else
+    // one; a hint of 1 or 4 overrides the choice where shared memory allows.
+    const bool four = 4ull * iv <= (interval_warps == 4 ? 227u : 200u) * 1024 && interval_warps != 1;
     plan->warps_per_block = four ? 4 : 1;
     if (!four && iv > 227 * 1024) return cudaErrorInvalidValue;
     cudaError_t e;
@@ -873,7 +896,7 @@ cudaError_t plan_levels(uint32_t n_slots, uint32_t mm_cap, int point_k, int roun
     }
     if (e != cudaSuccess) return e;
     plan->point_k = point_k;
-    return point_k == 4 ? plan_point<4>(n_slots, plan) : plan_point<2>(n_slots, plan);
+    return point_k == 4 ? plan_point<4>(n_slots, plan, point_warps) : plan_point<2>(n_slots, plan, point_warps);
 }
 
 cudaError_t launch_tree_init(dev::TreeHeader* const* trees, uint32_t n, const float* tape_times, float tape_time,

@@ -172,7 +172,7 @@ class VoxelStorage:
 
     def __init__(self, grid_dims=(16, 4), low_vertex=(-1.5, -1.5, -1.5), world_size=3.0,
                  rounding: int = ROUND_OUTWARD, shorten: bool = True, node_words: int = 0,
-                 tape_words: int = 0):
+                 tape_words: int = 0, point_cells_per_lane: int = 0):
         self.grid_dims = list(grid_dims)
         self.low_vertex = tuple(float(v) for v in low_vertex)
         self.world_size = float(world_size)
@@ -180,6 +180,7 @@ class VoxelStorage:
         self.shorten = shorten
         self.node_words = node_words
         self.tape_words = tape_words
+        self.point_cells_per_lane = point_cells_per_lane
         self.tape: Tape | None = None
         self.ctx: Context | None = None
         self._tree = C.c_void_p()
@@ -206,7 +207,8 @@ class VoxelStorage:
     def init(self, ctx: Context, shape) -> "VoxelStorage":
         self.ctx = ctx
         self.tape = shape if isinstance(shape, Tape) else Tape(shape)
-        opts = L.VoxelizeOpts(self.rounding, 1 if self.shorten else 0, self.node_words, self.tape_words)
+        opts = L.VoxelizeOpts(self.rounding, 1 if self.shorten else 0, self.node_words, self.tape_words,
+                              self.point_cells_per_lane, 0)
         g = self.grid_struct()
         L.check(L.lib().frep_tree_create(ctx._h, C.byref(g), C.byref(opts), C.byref(self._tree)))
         self.interior_node_count = [0] * self.grid_levels
@@ -411,6 +413,14 @@ class Batch:
         if tape_times is None:
             return None
         return (C.c_float * len(self.storages))(*[float(t) for t in tape_times])
+
+    def info(self) -> "L.BatchInfo":
+        out = L.BatchInfo()
+        L.check(L.lib().frep_batch_get_info(self._h, C.byref(out)))
+        return out
+
+    def set_tuning(self, interval_warps_per_block: int = 0, point_warps_per_block: int = 0) -> None:
+        L.check(L.lib().frep_batch_set_tuning(self._h, interval_warps_per_block, point_warps_per_block))
 
     def set_profiling(self, enable: bool = True) -> None:
         L.check(L.lib().frep_batch_set_profiling(self._h, 1 if enable else 0))

@@ -40,9 +40,15 @@ class Grid(C.Structure):
                 ("world_size", C.c_float)]
 
 
+class BatchInfo(C.Structure):
+    _fields_ = [("n_trees", C.c_uint32), ("voxelize_launches", C.c_uint32), ("upload_bytes", C.c_uint64),
+                ("device_bytes", C.c_uint64), ("interval_warps_per_block", C.c_uint32),
+                ("point_warps_per_block", C.c_uint32)]
+
+
 class VoxelizeOpts(C.Structure):
     _fields_ = [("rounding", C.c_uint32), ("shorten", C.c_uint32), ("node_words", C.c_uint64),
-                ("tape_words", C.c_uint64)]
+                ("tape_words", C.c_uint64), ("point_cells_per_lane", C.c_uint32), ("reserved", C.c_uint32)]
 
 
 class TreeInfo(C.Structure):
@@ -106,6 +112,8 @@ _SIGS = {
     "frep_batch_render": (C.c_int, [_P, _P, C.POINTER(LightsStruct), _P, _P, _P]),
     "frep_batch_run": (C.c_int, [_P, _P, _P, _P, C.POINTER(LightsStruct), _P, C.c_int, _P]),
     "frep_batch_set_profiling": (C.c_int, [_P, C.c_int]),
+    "frep_batch_set_tuning": (C.c_int, [_P, C.c_uint32, C.c_uint32]),
+    "frep_batch_get_info": (C.c_int, [_P, C.POINTER(BatchInfo)]),
     "frep_batch_timings": (C.c_int, [_P, _P]),
     "frep_render": (C.c_int, [_P, _P, C.POINTER(CameraStruct), C.POINTER(LightsStruct), C.c_float,
                               C.POINTER(Image), _P]),

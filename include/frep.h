@@ -146,6 +146,9 @@ typedef struct frep_voxelize_opts {
     uint32_t shorten;         /* 1 = prune min/max into shortened child tapes (ref.) */
     uint64_t node_words;      /* node pool capacity in u32 words (0 = automatic)     */
     uint64_t tape_words;      /* tape pool capacity in u64 words (0 = automatic)     */
+    uint32_t point_cells_per_lane; /* last-level pass: cells per lane, 2 or 4 (0 =
+                                    * automatic: 4 when dim^3/32 is a multiple of 4) */
+    uint32_t reserved;        /* 0                                                   */
 } frep_voxelize_opts;
 
 typedef struct frep_tree frep_tree;
@@ -171,10 +174,11 @@ frep_status frep_voxelize(frep_ctx* ctx, frep_tree* tree, const frep_tape* tape,
  * instead of a cudaMalloc'd buffer, and the root tape is copied straight from
  * `tape` (pageable memory: the call returns once the driver has staged it).
  * No counterpart in the reference.
- *   - Limit: a root tape of at most 524288 instructions (8 MiB / 4 bytes / 4
- *     warps per block; 2097152 when a block holds one warp); longer tapes
- *     return FREP_ERR_UNSUPPORTED. Tapes of more than 4096 instructions run on
- *     fewer blocks than frep_voxelize uses, so they take longer.
+ *   - Limit: each warp of a block needs n + 2m 32-bit words (n instructions,
+ *     m of them MIN/MAX, each rounded up to 32), and one block must fit the
+ *     8 MiB: n + 2m <= 524288 with 4 warps per block (2097152 with one);
+ *     longer tapes return FREP_ERR_UNSUPPORTED. Long tapes run on fewer
+ *     blocks than frep_voxelize uses, so they take longer.
  *   - Its first call on a device looks up the array's device address; make that
  *     first call before any stream capture.
  *   - Every call on a device shares the one array: calls whose work overlaps
@@ -317,6 +321,23 @@ frep_status frep_batch_render(frep_batch* batch, const frep_camera* cameras, con
 frep_status frep_batch_run(frep_batch* batch, const frep_tape* const* tapes, const float* tape_times,
                            const frep_camera* cameras, const frep_lights* lights, const frep_image* images,
                            int use_graph, void* stream);
+
+typedef struct frep_batch_info {
+    uint32_t n_trees;
+    uint32_t voxelize_launches;        /* kernels one voxelization of the batch launches */
+    uint64_t upload_bytes;             /* host->device bytes of its last voxelization   */
+    uint64_t device_bytes;             /* the batch's own scratch + upload area          */
+    uint32_t interval_warps_per_block; /* the plan in use (0 before the first run)       */
+    uint32_t point_warps_per_block;
+} frep_batch_info;
+frep_status frep_batch_get_info(const frep_batch* batch, frep_batch_info* info);
+
+/* Tapes per block of the level passes: each warp of a block runs its own
+ * work items (and so its own tape); 0 = chosen from the shared memory a warp
+ * needs (4 when four warps fit in 200 KB, else 1), 1 or 4 = that many where
+ * shared memory allows. Takes effect at the next voxelization. */
+frep_status frep_batch_set_tuning(frep_batch* batch, uint32_t interval_warps_per_block,
+                                  uint32_t point_warps_per_block);
 
 /* Profiling of plain (non-graph) batch calls: with profiling on,
  * frep_batch_voxelize and frep_batch_render record events between their

@@ -288,7 +288,7 @@ public:
     uint32_t fineGridDim = 0;
     std::vector<uint32_t> interiorNodeCount;
     csg::Tape tape;
-    frep_voxelize_opts opts{FREP_ROUND_OUTWARD, 1, 0, 0};
+    frep_voxelize_opts opts{FREP_ROUND_OUTWARD, 1, 0, 0, 0, 0};
 
     void Init(frep_ctx* ctx, const csg::Expr& shape) {
         gridLevels = (uint32_t)gridDims.size();

@@ -91,3 +91,69 @@ def test_batch_voxelize_then_render(ctx):
         assert oracle.canonical_of_export(vs.export())[0] == want[i][0]
         np.testing.assert_array_equal(rgba[i].cpu().numpy(), want[i][1])
     batch.close()
+
+
+@pytest.mark.parametrize("dims", [(16, 8), (8, 8, 8)])
+def test_point_cells_per_lane_override(ctx, dims):
+    """The last-level tile (2 or 4 cells per lane) changes the schedule, not the tree."""
+    import torch
+    sc = scenes.random_csg(40, seed=71, grid_dims=list(dims), width=96, height=80)
+    got = []
+    for k in (2, 4):
+        vs = frep.VoxelStorage(sc.grid_dims, sc.low_vertex, sc.world_size, point_cells_per_lane=k)
+        vs.init(ctx, sc.shape)
+        frep.Voxelizer(ctx, vs).voxelize(0.0)
+        rt = frep.Raytracer(ctx, vs)
+        rgba, _ = rt.trace(sc.camera, 0.0, sc.width, sc.height)
+        torch.cuda.synchronize()
+        canon, prob = oracle.canonical_of_export(vs.export())
+        assert prob == []
+        got.append((canon, rgba.cpu().numpy()))
+        vs.cleanup()
+    assert got[0][0] == got[1][0]
+    np.testing.assert_array_equal(got[0][1], got[1][1])
+
+
+def test_point_cells_per_lane_invalid(ctx):
+    vs = frep.VoxelStorage((16, 4), point_cells_per_lane=4)  # 4^3 / 32 = 2 words: 4 cells per lane cannot tile
+    with pytest.raises(frep.FrepError):
+        vs.init(ctx, scenes.spheres_union(4).shape)
+
+
+@pytest.mark.parametrize("warps", [(1, 1), (4, 4), (1, 4)])
+def test_batch_tuning_same_result(ctx, warps):
+    import torch
+    scs = _scenes()[:4]
+    want = [_alone(ctx, sc, 0.0) for sc in scs]
+    storages = [frep.VoxelStorage(sc.grid_dims, sc.low_vertex, sc.world_size).init(ctx, sc.shape) for sc in scs]
+    batch = frep.Batch(ctx, storages)
+    batch.set_tuning(*warps)
+    dev = torch.device("cuda", 0)
+    rgba = [torch.zeros((sc.height, sc.width, 4), dtype=torch.uint8, device=dev) for sc in scs]
+    batch.run([sc.camera for sc in scs], [(sc.width, sc.height) for sc in scs], rgba,
+              lights=frep.Lights(shadow_mask=1), graph=True)
+    torch.cuda.synchronize()
+    info = batch.info()
+    assert info.n_trees == len(scs) and info.voxelize_launches > 0
+    for i, vs in enumerate(storages):
+        assert oracle.canonical_of_export(vs.export())[0] == want[i][0]
+        np.testing.assert_array_equal(rgba[i].cpu().numpy(), want[i][1])
+    batch.close()
+
+
+def test_cached_plans_of_many_trees(ctx):
+    """Trees keep their level plans; planning a tree with a smaller shared-memory
+    footprint must not break later launches of a tree planned earlier."""
+    big = scenes.random_csg(300, seed=5, grid_dims=[16, 8], width=32, height=32)
+    small = scenes.spheres_union(3)
+    a = frep.VoxelStorage(big.grid_dims, big.low_vertex, big.world_size).init(ctx, big.shape)
+    b = frep.VoxelStorage(small.grid_dims, small.low_vertex, small.world_size).init(ctx, small.shape)
+    assert a.tape.n_slots > b.tape.n_slots
+    frep.Voxelizer(ctx, a).voxelize(0.0)
+    first = oracle.canonical_of_export(a.export())[0]
+    frep.Voxelizer(ctx, b).voxelize(0.0)
+    b.sync()
+    frep.Voxelizer(ctx, a).voxelize(0.0)
+    assert oracle.canonical_of_export(a.export())[0] == first
+    a.cleanup()
+    b.cleanup()
