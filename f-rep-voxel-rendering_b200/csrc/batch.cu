@@ -2,13 +2,19 @@
 // pass and one launch for all frames, optionally replayed as a CUDA graph.
 //
 // The reference voxelizes one scene at a time with a host fence per level
-// (vulkan/src/engine/voxelizer.cpp:295-329). Here a fixed set of trees shares
-// every launch: the scan kernel lays all trees' work items end to end and the
-// level kernels' warps take items from any tree (work stealing through one
-// device cursor), so small and large scenes fill the GPU together. The whole
-// sequence — one staged upload (root tapes, tape times, frame arguments), the
-// root copy + header reset, the level passes and the frames — is captured once
-// into a CUDA graph and replayed while the batch's shape stays the same.
+// (vulkan/src/engine/voxelizer.cpp:295-329). Here a set of trees shares every
+// launch: the scan kernel lays all trees' work items end to end and the level
+// kernels' warps take items from any tree (work stealing through one device
+// cursor), so small and large scenes fill the GPU together.
+//
+// Each call stages its inputs (root tapes, tape times, the tree tables, frame
+// arguments) in one upload area and copies it to the device with one
+// cudaMemcpyAsync. Four upload areas rotate, so the host prepares the next
+// calls while earlier ones still run on the device; it waits only for the
+// call four back (a serving loop makes two calls per step). The tree
+// set can change between calls (frep_batch_set_trees), which is what a serving
+// loop needs; frep_batch_run can capture the whole sequence into a CUDA graph
+// (one per upload area) and replay it while the batch keeps its shape.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -21,22 +27,33 @@ using frep::detail::align_up;
 using frep::detail::cuda_fail;
 using frep::detail::fail;
 
+namespace {
+
+constexpr int kAreas = 4;  // upload areas in rotation
+
+struct UploadArea {
+    uint8_t* h = nullptr;  // pinned
+    uint8_t* d = nullptr;
+    size_t bytes = 0;
+    cudaEvent_t done = nullptr;  // after the last work that reads `d`
+    bool pending = false;        // `done` has been recorded since the last wait
+    cudaGraphExec_t graph = nullptr;
+    std::vector<uint64_t> graph_key;
+};
+
+}  // namespace
+
 struct frep_batch {
     frep_ctx* ctx = nullptr;
     std::vector<frep_tree*> trees;
-    uint32_t n = 0;
     int rounding = 0;
-    // device: [n header pointers][prefix n+1][cursor]
-    void* d_meta = nullptr;
-    frep::dev::TreeHeader** d_trees = nullptr;
+    // device work prefix (capacity + 1 entries) and cursor
     unsigned long long* d_prefix = nullptr;
     unsigned long long* d_cursor = nullptr;
-    // one upload area: [tape times][root offsets][frame arguments][root tapes]
-    size_t stage_bytes = 0;
-    uint8_t* h_stage = nullptr;  // pinned
-    uint8_t* d_stage = nullptr;
-    cudaEvent_t upload_done = nullptr;
-    // keep-mask scratch for the interval passes
+    uint32_t prefix_cap = 0;
+    UploadArea area[kAreas];
+    int next_area = 0;
+    // interval-pass scratch (keep masks + choice masks per warp)
     uint32_t* keep = nullptr;
     uint64_t keep_words = 0;
     uint64_t bytes = 0;
@@ -53,71 +70,93 @@ struct frep_batch {
     uint32_t profiled_levels = 0;
     cudaEvent_t ev[2 + 3 * FREP_MAX_LEVELS] = {};
     cudaEvent_t rev[2] = {};
-    // what the last voxelization enqueued
+    // what the last call enqueued
     uint64_t last_upload = 0;
     uint32_t last_launches = 0;
-    // graph replay
     cudaStream_t capture_stream = nullptr;
-    cudaGraphExec_t graph = nullptr;
-    std::vector<uint64_t> graph_key;
 };
 
 namespace {
 
-// The upload area: [tape times][root offsets][level-pass tree order][frame
-// arguments][root tapes]. Everything before the root tapes depends only on
-// the batch size.
+// One upload area: [tape times][root offsets][tree table][level-pass order]
+// [frame arguments][root tapes].
 struct Layout {
-    size_t times = 0, offsets = 0, order = 0, frames = 0, roots = 0, total = 0;
+    size_t times = 0, offsets = 0, tree_ptrs = 0, order = 0, frames = 0, roots = 0, total = 0;
     std::vector<unsigned long long> root_ofs;  // n + 1, in words, relative to `roots`
 };
 
-Layout base_layout(uint32_t n) {
+Layout make_layout(uint32_t n, uint32_t nf, const frep_tape* const* tapes) {
     Layout L;
     L.times = 0;
     L.offsets = align_up(sizeof(float) * n, 16);
-    L.order = L.offsets + align_up(sizeof(unsigned long long) * (n + 1), 16);
+    L.tree_ptrs = L.offsets + align_up(sizeof(unsigned long long) * (n + 1), 16);
+    L.order = L.tree_ptrs + align_up(sizeof(void*) * n, 16);
     L.frames = L.order + align_up(sizeof(void*) * n, 16);
-    L.roots = L.frames + align_up(sizeof(frep::RenderArgs) * n, 16);
-    L.total = L.roots;
-    return L;
-}
-
-Layout make_layout(const frep_batch* b, const frep_tape* const* tapes) {
-    Layout L = base_layout(b->n);
-    L.root_ofs.resize(b->n + 1);
+    L.roots = L.frames + align_up(sizeof(frep::RenderArgs) * nf, 16);
+    L.root_ofs.assign(n + 1, 0);
     unsigned long long w = 0;
-    for (uint32_t i = 0; i < b->n; i++) {
+    for (uint32_t i = 0; i < n && tapes; i++) {
         L.root_ofs[i] = w;
         w += tapes[i]->record.size();
     }
-    L.root_ofs[b->n] = w;
+    L.root_ofs[n] = w;
     L.total = L.roots + w * 8;
     return L;
 }
 
-frep_status ensure_stage(frep_batch* b, size_t bytes) {
-    if (bytes <= b->stage_bytes) {
-        FREP_CUDA(cudaEventSynchronize(b->upload_done));
-        return FREP_OK;
+// Takes the next upload area, waiting until the call that used it last is
+// done with it on the device, and grows it to `bytes`.
+frep_status acquire_area(frep_batch* b, size_t bytes, int* which) {
+    const int i = b->next_area;
+    UploadArea& A = b->area[i];
+    if (A.pending) {
+        FREP_CUDA(cudaEventSynchronize(A.done));
+        A.pending = false;
     }
-    if (b->h_stage) {
-        cudaEventSynchronize(b->upload_done);
-        cudaFreeHost(b->h_stage);
-        cudaFree(b->d_stage);
-        b->ctx->used -= std::min<uint64_t>(b->ctx->used, b->stage_bytes);
-        b->bytes -= b->stage_bytes;
-        b->h_stage = nullptr;
-        b->d_stage = nullptr;
-        b->stage_bytes = 0;
+    if (bytes > A.bytes) {
+        if (A.graph) {
+            cudaGraphExecDestroy(A.graph);
+            A.graph = nullptr;
+            A.graph_key.clear();
+        }
+        if (A.h) cudaFreeHost(A.h);
+        if (A.d) cudaFree(A.d);
+        b->ctx->used -= std::min<uint64_t>(b->ctx->used, A.bytes);
+        b->bytes -= std::min<uint64_t>(b->bytes, A.bytes);
+        A.h = nullptr;
+        A.d = nullptr;
+        A.bytes = 0;
+        const size_t cap = align_up(bytes + bytes / 4, 4096);
+        if (b->ctx->used + cap > b->ctx->budget) return fail(FREP_ERR_OOM, "frep_batch: upload area exceeds the budget");
+        FREP_CUDA(cudaMallocHost(&A.h, cap));
+        FREP_CUDA(cudaMalloc(&A.d, cap));
+        A.bytes = cap;
+        b->bytes += cap;
+        b->ctx->used += cap;
     }
-    const size_t cap = align_up(bytes + bytes / 4, 4096);
-    if (b->ctx->used + cap > b->ctx->budget) return fail(FREP_ERR_OOM, "frep_batch: upload area exceeds the budget");
-    FREP_CUDA(cudaMallocHost(&b->h_stage, cap));
-    FREP_CUDA(cudaMalloc(&b->d_stage, cap));
-    b->stage_bytes = cap;
-    b->bytes += cap;
-    b->ctx->used += cap;
+    if (!A.done) FREP_CUDA(cudaEventCreateWithFlags(&A.done, cudaEventDisableTiming));
+    b->next_area = (i + 1) % kAreas;
+    *which = i;
+    return FREP_OK;
+}
+
+frep_status release_area(frep_batch* b, int i, cudaStream_t s) {
+    FREP_CUDA(cudaEventRecord(b->area[i].done, s));
+    b->area[i].pending = true;
+    return FREP_OK;
+}
+
+frep_status ensure_prefix(frep_batch* b, uint32_t n) {
+    if (n <= b->prefix_cap && b->d_prefix) return FREP_OK;
+    if (b->d_prefix) {
+        cudaDeviceSynchronize();
+        cudaFree(b->d_prefix);
+        b->d_prefix = nullptr;
+    }
+    const uint32_t cap = std::max<uint32_t>(n, 64);
+    FREP_CUDA(cudaMalloc(&b->d_prefix, sizeof(unsigned long long) * (cap + 2)));
+    b->d_cursor = b->d_prefix + cap + 1;
+    b->prefix_cap = cap;
     return FREP_OK;
 }
 
@@ -145,9 +184,9 @@ struct TapeStats {
     bool any_k4 = false, any_k2 = false;
 };
 
-frep_status check_tapes(frep_batch* b, const frep_tape* const* tapes, TapeStats* st) {
+frep_status check_tapes(const frep_batch* b, const frep_tape* const* tapes, TapeStats* st) {
     if (!tapes) return fail(FREP_ERR_INVALID_ARG, "frep_batch: null tapes");
-    for (uint32_t i = 0; i < b->n; i++) {
+    for (uint32_t i = 0; i < b->trees.size(); i++) {
         const frep_tape* t = tapes[i];
         const frep_tree* tr = b->trees[i];
         if (!t) return fail(FREP_ERR_INVALID_ARG, "frep_batch: tape %u is null", i);
@@ -158,8 +197,7 @@ frep_status check_tapes(frep_batch* b, const frep_tape* const* tapes, TapeStats*
         st->mm = std::max<uint32_t>(st->mm, t->ct.n_minmax);
         st->longest = std::max<uint32_t>(st->longest, (uint32_t)t->ct.instrs.size());
         st->max_levels = std::max<uint32_t>(st->max_levels, tr->grid.levels);
-        const int k = tr->point_k;
-        (k == 4 ? st->any_k4 : st->any_k2) = true;
+        (tr->point_k == 4 ? st->any_k4 : st->any_k2) = true;
     }
     return FREP_OK;
 }
@@ -178,24 +216,38 @@ frep_status ensure_plans(frep_batch* b, const TapeStats& st) {
     return FREP_OK;
 }
 
-// Enqueues the voxelization of every tree: root copy + header reset, then for
-// each level index one interval pass and up to two point passes, each a single
-// launch over the whole batch.
-frep_status enqueue_voxelize(frep_batch* b, const TapeStats& st, const Layout& L, cudaStream_t s, bool prof) {
+// Plans, work prefix and scratch for voxelizing the current tree set.
+frep_status prepare_voxelize(frep_batch* b, const frep_tape* const* tapes, TapeStats* st) {
+    frep_status r = check_tapes(b, tapes, st);
+    if (r == FREP_OK) r = ensure_plans(b, *st);
+    if (r == FREP_OK) r = ensure_prefix(b, (uint32_t)b->trees.size());
+    if (r == FREP_OK)
+        r = ensure_keep(b, (uint64_t)std::max(b->plan4.blocks * b->plan4.warps_per_block,
+                                              b->plan2.blocks * b->plan2.warps_per_block) *
+                               frep::warp_scratch(st->longest, st->mm).stride);
+    return r;
+}
+
+// Enqueues the voxelization of every tree of the set: root copy + header
+// reset, then for each level index one interval pass and up to two point
+// passes, each a single launch over the whole set. The level passes walk the
+// trees longest root tape first (the staged order): warps take the costliest
+// items first and the cheap ones fill the tail.
+frep_status enqueue_voxelize(frep_batch* b, const uint8_t* d_area, const TapeStats& st, const Layout& L,
+                             cudaStream_t s, bool prof) {
+    const uint32_t n = (uint32_t)b->trees.size();
     if (prof) FREP_CUDA(cudaEventRecord(b->ev[0], s));
-    const uint64_t* staged_roots = reinterpret_cast<const uint64_t*>(b->d_stage + L.roots);
-    const unsigned long long* offsets = reinterpret_cast<const unsigned long long*>(b->d_stage + L.offsets);
-    const float* times = reinterpret_cast<const float*>(b->d_stage + L.times);
-    cudaError_t e = frep::launch_tree_init_staged(b->d_trees, b->n, staged_roots, offsets, times, s);
+    auto* const* tree_tab = reinterpret_cast<frep::dev::TreeHeader* const*>(d_area + L.tree_ptrs);
+    cudaError_t e = frep::launch_tree_init_staged(tree_tab, n, reinterpret_cast<const uint64_t*>(d_area + L.roots),
+                                                  reinterpret_cast<const unsigned long long*>(d_area + L.offsets),
+                                                  reinterpret_cast<const float*>(d_area + L.times), s);
     if (e != cudaSuccess) return cuda_fail(e, "tree_init_staged_kernel");
     if (prof) FREP_CUDA(cudaEventRecord(b->ev[1], s));
     frep::LevelLaunch a{};
-    // The level passes walk the trees longest root tape first (staged order):
-    // warps take the costliest items first and the cheap ones fill the tail.
-    a.trees = reinterpret_cast<frep::dev::TreeHeader* const*>(b->d_stage + L.order);
+    a.trees = reinterpret_cast<frep::dev::TreeHeader* const*>(d_area + L.order);
     a.prefix = b->d_prefix;
     a.cursor = b->d_cursor;
-    a.n_trees = b->n;
+    a.n_trees = n;
     a.keep_scratch = b->keep;
     const frep::WarpScratch ws = frep::warp_scratch(st.longest, st.mm);
     a.keep_stride = ws.stride;
@@ -204,7 +256,6 @@ frep_status enqueue_voxelize(frep_batch* b, const TapeStats& st, const Layout& L
     a.mm_cap = st.mm;
     for (uint32_t l = 0; l < st.max_levels; l++) {
         a.level = l;
-        // interval passes of every tree that has a level below l
         e = frep::launch_level_scan(a, false, 4, s);
         if (e == cudaSuccess) e = frep::launch_level(a, b->plan4, b->rounding, false, s);
         if (e != cudaSuccess) return cuda_fail(e, "batched interval pass");
@@ -232,7 +283,7 @@ frep_status enqueue_voxelize(frep_batch* b, const TapeStats& st, const Layout& L
 }
 
 void mark_voxelized(frep_batch* b, const frep_tape* const* tapes, cudaStream_t s) {
-    for (uint32_t i = 0; i < b->n; i++) {
+    for (uint32_t i = 0; i < b->trees.size(); i++) {
         frep_tree* t = b->trees[i];
         t->voxelized = true;
         t->stream = s;
@@ -243,37 +294,70 @@ void mark_voxelized(frep_batch* b, const frep_tape* const* tapes, cudaStream_t s
     }
 }
 
-// Writes the host part of the upload area: tape times, root offsets, the
-// level-pass order (headers by descending root tape length), roots.
-void stage_inputs(frep_batch* b, const frep_tape* const* tapes, const float* tape_times, const Layout& L) {
-    float* times = reinterpret_cast<float*>(b->h_stage + L.times);
-    for (uint32_t i = 0; i < b->n; i++) times[i] = tape_times ? tape_times[i] : 0.0f;
-    std::memcpy(b->h_stage + L.offsets, L.root_ofs.data(), sizeof(unsigned long long) * (b->n + 1));
-    std::vector<uint32_t> idx(b->n);
-    for (uint32_t i = 0; i < b->n; i++) idx[i] = i;
+// Host part of a voxelization's upload: tape times, root offsets, the tree
+// table (set order), the level-pass order (by descending root tape length),
+// the root tapes.
+void stage_inputs(const frep_batch* b, uint8_t* h, const frep_tape* const* tapes, const float* tape_times,
+                  const Layout& L) {
+    const uint32_t n = (uint32_t)b->trees.size();
+    float* times = reinterpret_cast<float*>(h + L.times);
+    for (uint32_t i = 0; i < n; i++) times[i] = tape_times ? tape_times[i] : 0.0f;
+    std::memcpy(h + L.offsets, L.root_ofs.data(), sizeof(unsigned long long) * (n + 1));
+    auto** tab = reinterpret_cast<frep::dev::TreeHeader**>(h + L.tree_ptrs);
+    for (uint32_t i = 0; i < n; i++) tab[i] = b->trees[i]->hdr;
+    std::vector<uint32_t> idx(n);
+    for (uint32_t i = 0; i < n; i++) idx[i] = i;
     std::stable_sort(idx.begin(), idx.end(), [&](uint32_t x, uint32_t y) {
         return tapes[x]->ct.instrs.size() > tapes[y]->ct.instrs.size();
     });
-    auto** order = reinterpret_cast<frep::dev::TreeHeader**>(b->h_stage + L.order);
-    for (uint32_t i = 0; i < b->n; i++) order[i] = b->trees[idx[i]]->hdr;
-    uint64_t* roots = reinterpret_cast<uint64_t*>(b->h_stage + L.roots);
-    for (uint32_t i = 0; i < b->n; i++)
+    auto** order = reinterpret_cast<frep::dev::TreeHeader**>(h + L.order);
+    for (uint32_t i = 0; i < n; i++) order[i] = b->trees[idx[i]]->hdr;
+    uint64_t* roots = reinterpret_cast<uint64_t*>(h + L.roots);
+    for (uint32_t i = 0; i < n; i++)
         std::memcpy(roots + L.root_ofs[i], tapes[i]->record.data(), tapes[i]->record.size() * 8);
 }
 
-frep_status stage_frames(frep_batch* b, const frep_camera* cams, const frep_lights* lights, const float* tape_times,
-                         const frep_image* images, const Layout& L, uint32_t* max_w, uint32_t* max_h,
-                         uint32_t* max_slots) {
-    frep::RenderArgs* frames = reinterpret_cast<frep::RenderArgs*>(b->h_stage + L.frames);
-    *max_w = *max_h = 0;
-    *max_slots = 4;
-    for (uint32_t i = 0; i < b->n; i++) {
-        frep_status st = frep::detail::fill_render_args(b->trees[i], &cams[i], lights,
+struct FrameDims {
+    uint32_t max_w = 0, max_h = 0, max_slots = 4;
+};
+
+frep_status stage_frames(uint8_t* h, const frep_tree* const* frame_trees, uint32_t nf, const frep_camera* cams,
+                         const frep_lights* lights, const float* tape_times, const frep_image* images,
+                         const Layout& L, FrameDims* fd) {
+    frep::RenderArgs* frames = reinterpret_cast<frep::RenderArgs*>(h + L.frames);
+    for (uint32_t i = 0; i < nf; i++) {
+        frep_status st = frep::detail::fill_render_args(frame_trees[i], &cams[i], lights,
                                                         tape_times ? tape_times[i] : 0.0f, &images[i], &frames[i]);
         if (st != FREP_OK) return st;
-        *max_w = std::max(*max_w, cams[i].width);
-        *max_h = std::max(*max_h, cams[i].height);
-        *max_slots = std::max(*max_slots, frames[i].n_slots);
+        fd->max_w = std::max(fd->max_w, cams[i].width);
+        fd->max_h = std::max(fd->max_h, cams[i].height);
+        fd->max_slots = std::max(fd->max_slots, frames[i].n_slots);
+    }
+    return FREP_OK;
+}
+
+frep_status enqueue_frames(frep_batch* b, const uint8_t* d_area, const Layout& L, uint32_t nf, const FrameDims& fd,
+                           cudaStream_t s, bool prof) {
+    if (prof) FREP_CUDA(cudaEventRecord(b->rev[0], s));
+    cudaError_t e = frep::launch_render_batch(reinterpret_cast<const frep::RenderArgs*>(d_area + L.frames), nf,
+                                              fd.max_w, fd.max_h, fd.max_slots, s);
+    if (e == cudaErrorInvalidValue) return fail(FREP_ERR_UNSUPPORTED, "frep_batch: too many frames or slots");
+    if (e != cudaSuccess) return cuda_fail(e, "render_batch_kernel");
+    if (prof) {
+        FREP_CUDA(cudaEventRecord(b->rev[1], s));
+        b->render_profiled = true;
+    }
+    return FREP_OK;
+}
+
+frep_status check_trees(frep_ctx* ctx, frep_tree* const* trees, uint32_t n, int* rounding) {
+    if (!trees || n == 0) return fail(FREP_ERR_INVALID_ARG, "frep_batch: empty tree set");
+    for (uint32_t i = 0; i < n; i++) {
+        if (!trees[i] || trees[i]->ctx != ctx)
+            return fail(FREP_ERR_INVALID_ARG, "frep_batch: tree %u is null or from another context", i);
+        if (i == 0) *rounding = (int)trees[0]->opts.rounding;
+        if ((int)trees[i]->opts.rounding != *rounding)
+            return fail(FREP_ERR_INVALID_ARG, "frep_batch: all trees of a batch use the same rounding");
     }
     return FREP_OK;
 }
@@ -283,42 +367,25 @@ frep_status stage_frames(frep_batch* b, const frep_camera* cams, const frep_ligh
 extern "C" {
 
 frep_status frep_batch_create(frep_ctx* ctx, frep_tree* const* trees, uint32_t n, frep_batch** out) {
-    if (!ctx || !trees || !out || n == 0) return fail(FREP_ERR_INVALID_ARG, "frep_batch_create: bad arguments");
+    if (!ctx || !out) return fail(FREP_ERR_INVALID_ARG, "frep_batch_create: bad arguments");
+    int rounding = 0;
+    frep_status r = check_trees(ctx, trees, n, &rounding);
+    if (r != FREP_OK) return r;
     FREP_CUDA(cudaSetDevice(ctx->device));
     auto* b = new frep_batch();
     b->ctx = ctx;
-    b->n = n;
     b->trees.assign(trees, trees + n);
-    b->rounding = (int)trees[0]->opts.rounding;
-    for (uint32_t i = 0; i < n; i++) {
-        if (!trees[i] || trees[i]->ctx != ctx) {
-            delete b;
-            return fail(FREP_ERR_INVALID_ARG, "frep_batch_create: tree %u is null or from another context", i);
-        }
-        if ((int)trees[i]->opts.rounding != b->rounding) {
-            delete b;
-            return fail(FREP_ERR_INVALID_ARG, "frep_batch_create: all trees of a batch use the same rounding");
-        }
-    }
-    const size_t meta = align_up(sizeof(void*) * n, 16) + sizeof(unsigned long long) * (n + 2);
-    cudaError_t e = cudaMalloc(&b->d_meta, meta);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->upload_done, cudaEventDisableTiming);
-    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->capture_stream, cudaStreamNonBlocking);
+    b->rounding = rounding;
+    cudaError_t e = cudaStreamCreateWithFlags(&b->capture_stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
-        cudaFree(b->d_meta);
         delete b;
         return cuda_fail(e, "frep_batch_create");
     }
-    b->d_trees = static_cast<frep::dev::TreeHeader**>(b->d_meta);
-    b->d_prefix = reinterpret_cast<unsigned long long*>(static_cast<uint8_t*>(b->d_meta) + align_up(sizeof(void*) * n, 16));
-    b->d_cursor = b->d_prefix + n + 1;
-    std::vector<frep::dev::TreeHeader*> h(n);
-    for (uint32_t i = 0; i < n; i++) h[i] = trees[i]->hdr;
-    e = cudaMemcpy(b->d_trees, h.data(), sizeof(void*) * n, cudaMemcpyHostToDevice);
-    if (e != cudaSuccess) {
-        cudaFree(b->d_meta);
+    r = ensure_prefix(b, n);
+    if (r != FREP_OK) {
+        cudaStreamDestroy(b->capture_stream);
         delete b;
-        return cuda_fail(e, "frep_batch_create: tree table upload");
+        return r;
     }
     *out = b;
     return FREP_OK;
@@ -328,12 +395,14 @@ void frep_batch_destroy(frep_batch* b) {
     if (!b) return;
     cudaSetDevice(b->ctx->device);
     cudaDeviceSynchronize();
-    if (b->graph) cudaGraphExecDestroy(b->graph);
-    cudaFree(b->d_meta);
+    for (UploadArea& A : b->area) {
+        if (A.graph) cudaGraphExecDestroy(A.graph);
+        if (A.h) cudaFreeHost(A.h);
+        if (A.d) cudaFree(A.d);
+        if (A.done) cudaEventDestroy(A.done);
+    }
+    cudaFree(b->d_prefix);
     cudaFree(b->keep);
-    cudaFree(b->d_stage);
-    if (b->h_stage) cudaFreeHost(b->h_stage);
-    if (b->upload_done) cudaEventDestroy(b->upload_done);
     if (b->capture_stream) cudaStreamDestroy(b->capture_stream);
     for (cudaEvent_t e : b->ev)
         if (e) cudaEventDestroy(e);
@@ -343,57 +412,71 @@ void frep_batch_destroy(frep_batch* b) {
     delete b;
 }
 
+frep_status frep_batch_set_trees(frep_batch* b, frep_tree* const* trees, uint32_t n) {
+    if (!b) return fail(FREP_ERR_INVALID_ARG, "frep_batch_set_trees: null batch");
+    int rounding = 0;
+    frep_status r = check_trees(b->ctx, trees, n, &rounding);
+    if (r != FREP_OK) return r;
+    if (rounding != b->rounding) {
+        b->rounding = rounding;
+        b->plan_valid = false;
+    }
+    b->trees.assign(trees, trees + n);
+    return FREP_OK;
+}
+
 frep_status frep_batch_voxelize(frep_batch* b, const frep_tape* const* tapes, const float* tape_times,
                                 void* stream_ptr) {
     if (!b) return fail(FREP_ERR_INVALID_ARG, "frep_batch_voxelize: null batch");
     FREP_CUDA(cudaSetDevice(b->ctx->device));
     cudaStream_t s = (cudaStream_t)stream_ptr;
     TapeStats st;
-    frep_status r = check_tapes(b, tapes, &st);
-    if (r == FREP_OK) r = ensure_plans(b, st);
-    const Layout L = make_layout(b, tapes);
-    if (r == FREP_OK) r = ensure_stage(b, L.total);
-    if (r == FREP_OK) r = ensure_keep(b, (uint64_t)std::max(b->plan4.blocks * b->plan4.warps_per_block,
-                                                           b->plan2.blocks * b->plan2.warps_per_block) *
-                                             frep::warp_scratch(st.longest, st.mm).stride);
+    frep_status r = prepare_voxelize(b, tapes, &st);
     if (r != FREP_OK) return r;
-    stage_inputs(b, tapes, tape_times, L);
-    FREP_CUDA(cudaMemcpyAsync(b->d_stage, b->h_stage, L.frames, cudaMemcpyHostToDevice, s));  // times..order
-    FREP_CUDA(cudaMemcpyAsync(b->d_stage + L.roots, b->h_stage + L.roots, L.total - L.roots,
-                              cudaMemcpyHostToDevice, s));
-    FREP_CUDA(cudaEventRecord(b->upload_done, s));
-    r = enqueue_voxelize(b, st, L, s, b->profile);
+    const Layout L = make_layout((uint32_t)b->trees.size(), 0, tapes);
+    int ai = 0;
+    r = acquire_area(b, L.total, &ai);
+    if (r != FREP_OK) return r;
+    UploadArea& A = b->area[ai];
+    stage_inputs(b, A.h, tapes, tape_times, L);
+    FREP_CUDA(cudaMemcpyAsync(A.d, A.h, L.total, cudaMemcpyHostToDevice, s));
+    r = enqueue_voxelize(b, A.d, st, L, s, b->profile);
     if (r != FREP_OK) return r;
     mark_voxelized(b, tapes, s);
-    return FREP_OK;
+    return release_area(b, ai, s);
+}
+
+frep_status frep_batch_render_frames(frep_batch* b, const frep_tree* const* frame_trees, uint32_t n_frames,
+                                     const frep_camera* cameras, const frep_lights* lights, const float* tape_times,
+                                     const frep_image* images, void* stream_ptr) {
+    if (!b || !frame_trees || !cameras || !lights || !images)
+        return fail(FREP_ERR_INVALID_ARG, "frep_batch_render_frames: null argument");
+    if (n_frames == 0) return FREP_OK;
+    for (uint32_t i = 0; i < n_frames; i++)
+        if (!frame_trees[i] || frame_trees[i]->ctx != b->ctx)
+            return fail(FREP_ERR_INVALID_ARG, "frep_batch_render_frames: tree of frame %u is null or foreign", i);
+    FREP_CUDA(cudaSetDevice(b->ctx->device));
+    cudaStream_t s = (cudaStream_t)stream_ptr;
+    const Layout L = make_layout(0, n_frames, nullptr);
+    int ai = 0;
+    frep_status r = acquire_area(b, L.total, &ai);
+    if (r != FREP_OK) return r;
+    UploadArea& A = b->area[ai];
+    FrameDims fd;
+    r = stage_frames(A.h, frame_trees, n_frames, cameras, lights, tape_times, images, L, &fd);
+    if (r != FREP_OK) return r;
+    FREP_CUDA(cudaMemcpyAsync(A.d + L.frames, A.h + L.frames, L.roots - L.frames, cudaMemcpyHostToDevice, s));
+    r = enqueue_frames(b, A.d, L, n_frames, fd, s, b->profile);
+    if (r != FREP_OK) return r;
+    return release_area(b, ai, s);
 }
 
 frep_status frep_batch_render(frep_batch* b, const frep_camera* cameras, const frep_lights* lights,
                               const float* tape_times, const frep_image* images, void* stream_ptr) {
-    if (!b || !cameras || !lights || !images) return fail(FREP_ERR_INVALID_ARG, "frep_batch_render: null argument");
-    FREP_CUDA(cudaSetDevice(b->ctx->device));
-    cudaStream_t s = (cudaStream_t)stream_ptr;
-    // Frame arguments go to the upload area's frame block; make sure it is large
-    // enough even before the first voxelization.
-    const Layout L = base_layout(b->n);
-    frep_status r = ensure_stage(b, std::max<size_t>(L.roots, b->stage_bytes));
-    if (r != FREP_OK) return r;
-    uint32_t mw, mh, ms;
-    r = stage_frames(b, cameras, lights, tape_times, images, L, &mw, &mh, &ms);
-    if (r != FREP_OK) return r;
-    FREP_CUDA(cudaMemcpyAsync(b->d_stage + L.frames, b->h_stage + L.frames, L.roots - L.frames,
-                              cudaMemcpyHostToDevice, s));
-    FREP_CUDA(cudaEventRecord(b->upload_done, s));
-    if (b->profile) FREP_CUDA(cudaEventRecord(b->rev[0], s));
-    cudaError_t e = frep::launch_render_batch(reinterpret_cast<const frep::RenderArgs*>(b->d_stage + L.frames), b->n,
-                                              mw, mh, ms, s);
-    if (e == cudaErrorInvalidValue) return fail(FREP_ERR_UNSUPPORTED, "frep_batch_render: too many frames or slots");
-    if (e != cudaSuccess) return cuda_fail(e, "render_batch_kernel");
-    if (b->profile) {
-        FREP_CUDA(cudaEventRecord(b->rev[1], s));
-        b->render_profiled = true;
-    }
-    return FREP_OK;
+    if (!b) return fail(FREP_ERR_INVALID_ARG, "frep_batch_render: null batch");
+    std::vector<const frep_tree*> ft(b->trees.begin(), b->trees.end());
+    return frep_batch_render_frames(b, ft.data(), (uint32_t)ft.size(), cameras, lights, tape_times, images,
+                                    stream_ptr);
 }
 
 frep_status frep_batch_run(frep_batch* b, const frep_tape* const* tapes, const float* tape_times,
@@ -406,42 +489,40 @@ frep_status frep_batch_run(frep_batch* b, const frep_tape* const* tapes, const f
     }
     FREP_CUDA(cudaSetDevice(b->ctx->device));
     cudaStream_t s = (cudaStream_t)stream_ptr;
+    const uint32_t n = (uint32_t)b->trees.size();
     TapeStats st;
-    frep_status r = check_tapes(b, tapes, &st);
-    if (r == FREP_OK) r = ensure_plans(b, st);
-    const Layout L = make_layout(b, tapes);
-    if (r == FREP_OK) r = ensure_stage(b, L.total);
-    if (r == FREP_OK) r = ensure_keep(b, (uint64_t)std::max(b->plan4.blocks * b->plan4.warps_per_block,
-                                                           b->plan2.blocks * b->plan2.warps_per_block) *
-                                             frep::warp_scratch(st.longest, st.mm).stride);
+    frep_status r = prepare_voxelize(b, tapes, &st);
     if (r != FREP_OK) return r;
-    // Fill the whole upload area (the graph's memcpy node reads it when it runs).
-    // The frame arguments describe the trees as this run leaves them.
+    const Layout L = make_layout(n, n, tapes);
+    int ai = 0;
+    r = acquire_area(b, L.total, &ai);
+    if (r != FREP_OK) return r;
+    UploadArea& A = b->area[ai];
+    // Fill the whole upload area (the graph's copy node reads it when it
+    // runs). The frame arguments describe the trees as this run leaves them.
     mark_voxelized(b, tapes, s);
-    stage_inputs(b, tapes, tape_times, L);
-    uint32_t mw, mh, ms;
-    r = stage_frames(b, cameras, lights, tape_times, images, L, &mw, &mh, &ms);
+    stage_inputs(b, A.h, tapes, tape_times, L);
+    std::vector<const frep_tree*> ft(b->trees.begin(), b->trees.end());
+    FrameDims fd;
+    r = stage_frames(A.h, ft.data(), n, cameras, lights, tape_times, images, L, &fd);
     if (r != FREP_OK) return r;
-    // The graph stays valid while the batch keeps its shape.
-    std::vector<uint64_t> key = {L.total, st.slots, st.mm, st.longest, st.max_levels, mw, mh, ms,
-                                 (uint64_t)b->plan4.blocks, (uint64_t)b->plan4.warps_per_block,
-                                 (uint64_t)b->plan4.point_warps_per_block, (uint64_t)b->plan2.point_warps_per_block,
-                                 (uint64_t)(uintptr_t)b->keep, (uint64_t)(uintptr_t)b->d_stage};
-    for (uint32_t i = 0; i < b->n; i++) key.push_back(L.root_ofs[i]);
-    if (!b->graph || key != b->graph_key) {
-        if (b->graph) {
-            cudaGraphExecDestroy(b->graph);
-            b->graph = nullptr;
+    // The area's graph stays valid while the batch keeps its shape.
+    std::vector<uint64_t> key = {L.total, n, st.slots, st.mm, st.longest, st.max_levels, st.any_k4, st.any_k2,
+                                 fd.max_w, fd.max_h, fd.max_slots, (uint64_t)b->plan4.blocks,
+                                 (uint64_t)b->plan4.warps_per_block, (uint64_t)b->plan4.point_warps_per_block,
+                                 (uint64_t)b->plan2.point_warps_per_block, (uint64_t)(uintptr_t)b->keep,
+                                 (uint64_t)(uintptr_t)b->d_prefix, (uint64_t)(uintptr_t)A.d};
+    for (uint32_t i = 0; i < n; i++) key.push_back(L.root_ofs[i]);
+    if (!A.graph || key != A.graph_key) {
+        if (A.graph) {
+            cudaGraphExecDestroy(A.graph);
+            A.graph = nullptr;
         }
         cudaStream_t cs = b->capture_stream;
         FREP_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-        cudaError_t ce = cudaMemcpyAsync(b->d_stage, b->h_stage, L.total, cudaMemcpyHostToDevice, cs);
-        frep_status vr = ce == cudaSuccess ? enqueue_voxelize(b, st, L, cs, false) : cuda_fail(ce, "upload");
-        if (vr == FREP_OK) {
-            ce = frep::launch_render_batch(reinterpret_cast<const frep::RenderArgs*>(b->d_stage + L.frames), b->n,
-                                           mw, mh, ms, cs);
-            if (ce != cudaSuccess) vr = cuda_fail(ce, "render_batch_kernel");
-        }
+        cudaError_t ce = cudaMemcpyAsync(A.d, A.h, L.total, cudaMemcpyHostToDevice, cs);
+        frep_status vr = ce == cudaSuccess ? enqueue_voxelize(b, A.d, st, L, cs, false) : cuda_fail(ce, "upload");
+        if (vr == FREP_OK) vr = enqueue_frames(b, A.d, L, n, fd, cs, false);
         cudaGraph_t g = nullptr;
         cudaError_t ee = cudaStreamEndCapture(cs, &g);
         if (vr != FREP_OK) {
@@ -449,19 +530,20 @@ frep_status frep_batch_run(frep_batch* b, const frep_tape* const* tapes, const f
             return vr;
         }
         if (ee != cudaSuccess) return cuda_fail(ee, "cudaStreamEndCapture");
-        ce = cudaGraphInstantiate(&b->graph, g, 0);
+        ce = cudaGraphInstantiate(&A.graph, g, 0);
         cudaGraphDestroy(g);
         if (ce != cudaSuccess) return cuda_fail(ce, "cudaGraphInstantiate");
-        b->graph_key = key;
+        A.graph_key = key;
+    } else {
+        b->last_upload = L.total;
     }
-    FREP_CUDA(cudaGraphLaunch(b->graph, s));
-    FREP_CUDA(cudaEventRecord(b->upload_done, s));
-    return FREP_OK;
+    FREP_CUDA(cudaGraphLaunch(A.graph, s));
+    return release_area(b, ai, s);
 }
 
 frep_status frep_batch_get_info(const frep_batch* b, frep_batch_info* info) {
     if (!b || !info) return fail(FREP_ERR_INVALID_ARG, "frep_batch_get_info: null argument");
-    info->n_trees = b->n;
+    info->n_trees = (uint32_t)b->trees.size();
     info->voxelize_launches = b->last_launches;
     info->upload_bytes = b->last_upload;
     info->device_bytes = b->bytes;

@@ -165,13 +165,27 @@ static frep_status validate_grid(const frep_grid* g) {
     return FREP_OK;
 }
 
-frep_status frep_tree_create(frep_ctx* ctx, const frep_grid* grid, const frep_voxelize_opts* opts,
-                             frep_tree** out) {
+}  // extern "C"
+
+namespace frep {
+namespace detail {
+
+uint64_t tree_external_bytes(uint64_t node_words, uint64_t tape_words) {
+    return align_up(sizeof(dev::TreeHeader), 256) + 256 + align_up(node_words * 4, 256) + tape_words * 8;
+}
+
+// Creates a tree; with `ext` its header, work prefix and pools are carved
+// from that caller-owned device memory (the serving loop's arena) instead of
+// cudaMalloc'd, the header upload is ordered on `stream`, and nothing is
+// charged to the context's budget.
+frep_status tree_create_impl(frep_ctx* ctx, const frep_grid* grid, const frep_voxelize_opts* opts, uint8_t* ext,
+                             uint64_t ext_bytes, cudaStream_t stream, frep_tree** out) {
     if (!ctx || !grid || !out) return fail(FREP_ERR_INVALID_ARG, "frep_tree_create: null argument");
     frep_status s = validate_grid(grid);
     if (s != FREP_OK) return s;
     FREP_CUDA(cudaSetDevice(ctx->device));
     auto* t = new frep_tree();
+    t->external = ext != nullptr;
     t->ctx = ctx;
     t->grid = *grid;
     if (opts) t->opts = *opts;
@@ -202,27 +216,42 @@ frep_status frep_tree_create(frep_ctx* ctx, const frep_grid* grid, const frep_vo
         dense_nodes = std::min<uint64_t>(dense_nodes * d3, 1ull << 40);
         dense_words = std::min<uint64_t>(dense_words, 1ull << 44);
     }
-    const uint64_t avail = ctx->budget > ctx->used ? ctx->budget - ctx->used : 0;
+    const uint64_t avail = ext ? ext_bytes : (ctx->budget > ctx->used ? ctx->budget - ctx->used : 0);
+    if (ext && (!t->opts.node_words || !t->opts.tape_words)) {
+        delete t;
+        return fail(FREP_ERR_INVALID_ARG, "tree in caller memory: pool sizes must be given");
+    }
     t->node_cap = t->opts.node_words ? t->opts.node_words : std::min<uint64_t>(dense_words, avail / 4 / 4);
     t->tape_cap = t->opts.tape_words ? t->opts.tape_words : avail / 4 / 8;
     t->tape_cap = std::min<uint64_t>(t->tape_cap, 0xFFFFFFF0ull);  // tape indices are u32
-    const uint64_t bytes = t->node_cap * 4 + t->tape_cap * 8 + sizeof(frep::dev::TreeHeader);
+    const uint64_t bytes = ext ? tree_external_bytes(t->node_cap, t->tape_cap)
+                               : t->node_cap * 4 + t->tape_cap * 8 + sizeof(frep::dev::TreeHeader);
     if (t->node_cap < t->node_size[0] || bytes > avail) {
         delete t;
         return fail(FREP_ERR_OOM, "frep_tree_create: %llu bytes requested, %llu left in the budget",
                     (unsigned long long)bytes, (unsigned long long)avail);
     }
-    cudaError_t e = cudaMalloc(&t->hdr, sizeof(frep::dev::TreeHeader));
-    if (e == cudaSuccess) e = cudaMalloc(&t->d_small, 64);
-    if (e == cudaSuccess) e = cudaMalloc(&t->nodes, t->node_cap * 4);
-    if (e == cudaSuccess) e = cudaMalloc(&t->tapes, t->tape_cap * 8);
+    cudaError_t e = cudaSuccess;
+    if (ext) {
+        t->hdr = reinterpret_cast<frep::dev::TreeHeader*>(ext);
+        t->d_small = reinterpret_cast<unsigned long long*>(ext + align_up(sizeof(frep::dev::TreeHeader), 256));
+        t->nodes = reinterpret_cast<uint32_t*>(reinterpret_cast<uint8_t*>(t->d_small) + 256);
+        t->tapes = reinterpret_cast<uint64_t*>(reinterpret_cast<uint8_t*>(t->nodes) + align_up(t->node_cap * 4, 256));
+    } else {
+        e = cudaMalloc(&t->hdr, sizeof(frep::dev::TreeHeader));
+        if (e == cudaSuccess) e = cudaMalloc(&t->d_small, 64);
+        if (e == cudaSuccess) e = cudaMalloc(&t->nodes, t->node_cap * 4);
+        if (e == cudaSuccess) e = cudaMalloc(&t->tapes, t->tape_cap * 8);
+    }
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&t->upload_done, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         cudaGetLastError();
-        cudaFree(t->hdr);
-        cudaFree(t->d_small);
-        cudaFree(t->nodes);
-        cudaFree(t->tapes);
+        if (!ext) {
+            cudaFree(t->hdr);
+            cudaFree(t->d_small);
+            cudaFree(t->nodes);
+            cudaFree(t->tapes);
+        }
         delete t;
         return fail(FREP_ERR_OOM, "frep_tree_create: cudaMalloc failed (%s)", cudaGetErrorString(e));
     }
@@ -244,32 +273,57 @@ frep_status frep_tree_create(frep_ctx* ctx, const frep_grid* grid, const frep_vo
     t->d_self = reinterpret_cast<frep::dev::TreeHeader**>(t->d_small);
     t->d_prefix = t->d_small + 1;
     t->d_cursor = t->d_small + 3;
-    cudaError_t ce = cudaMemcpy(t->hdr, &h, sizeof(h), cudaMemcpyHostToDevice);
-    if (ce == cudaSuccess) ce = cudaMemcpy(t->d_self, &t->hdr, sizeof(void*), cudaMemcpyHostToDevice);
+    cudaError_t ce;
+    if (ext) {  // pageable sources: the copies are staged before the calls return
+        ce = cudaMemcpyAsync(t->hdr, &h, sizeof(h), cudaMemcpyHostToDevice, stream);
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(t->d_self, &t->hdr, sizeof(void*), cudaMemcpyHostToDevice, stream);
+    } else {
+        ce = cudaMemcpy(t->hdr, &h, sizeof(h), cudaMemcpyHostToDevice);
+        if (ce == cudaSuccess) ce = cudaMemcpy(t->d_self, &t->hdr, sizeof(void*), cudaMemcpyHostToDevice);
+    }
     if (ce != cudaSuccess) {
-        cudaFree(t->hdr);
-        cudaFree(t->d_small);
-        cudaFree(t->nodes);
-        cudaFree(t->tapes);
+        if (!ext) {
+            cudaFree(t->hdr);
+            cudaFree(t->d_small);
+            cudaFree(t->nodes);
+            cudaFree(t->tapes);
+        }
         cudaEventDestroy(t->upload_done);
         delete t;
         return cuda_fail(ce, "frep_tree_create: header upload");
     }
-    t->bytes = bytes;
-    ctx->used += bytes;
+    if (ext) {
+        t->stream = stream;
+    } else {
+        t->bytes = bytes;
+        ctx->used += bytes;
+    }
     *out = t;
     return FREP_OK;
+}
+
+}  // namespace detail
+}  // namespace frep
+
+extern "C" {
+
+frep_status frep_tree_create(frep_ctx* ctx, const frep_grid* grid, const frep_voxelize_opts* opts,
+                             frep_tree** out) {
+    return frep::detail::tree_create_impl(ctx, grid, opts, nullptr, 0, nullptr, out);
 }
 
 void frep_tree_destroy(frep_tree* t) {
     if (!t) return;
     cudaSetDevice(t->ctx->device);
-    if (t->stream) cudaStreamSynchronize(t->stream);
-    else cudaDeviceSynchronize();
-    cudaFree(t->hdr);
-    cudaFree(t->d_small);
-    cudaFree(t->nodes);
-    cudaFree(t->tapes);
+    if (!t->external) {
+        // (a tree in caller memory is released in stream order by its owner)
+        if (t->stream) cudaStreamSynchronize(t->stream);
+        else cudaDeviceSynchronize();
+        cudaFree(t->hdr);
+        cudaFree(t->d_small);
+        cudaFree(t->nodes);
+        cudaFree(t->tapes);
+    }
     cudaFree(t->keep);
     if (t->staging) cudaFreeHost(t->staging);
     if (t->upload_done) cudaEventDestroy(t->upload_done);

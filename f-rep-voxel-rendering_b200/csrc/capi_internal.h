@@ -28,6 +28,10 @@ inline uint64_t align_up(uint64_t v, uint64_t a) { return (v + a - 1) / a * a; }
 struct frep_tree;
 namespace frep {
 namespace detail {
+// Trees whose header and pools are carved from caller-owned device memory.
+uint64_t tree_external_bytes(uint64_t node_words, uint64_t tape_words);
+frep_status tree_create_impl(frep_ctx* ctx, const frep_grid* grid, const frep_voxelize_opts* opts, uint8_t* ext,
+                             uint64_t ext_bytes, cudaStream_t stream, frep_tree** out);
 // Camera basis, lights and tree description for one frame (frep_render).
 frep_status fill_render_args(const frep_tree* tree, const frep_camera* cam, const frep_lights* lights,
                              float tape_time, const frep_image* out, RenderArgs* args);
@@ -62,6 +66,7 @@ struct frep_tree {
     frep_grid grid{};
     frep_voxelize_opts opts{};
     int point_k = 4;  // cells per lane of the last-level pass
+    bool external = false;  // header and pools live in caller-owned memory
     float cell_size[FREP_MAX_LEVELS] = {};
     uint32_t node_size[FREP_MAX_LEVELS] = {};
     frep::dev::TreeHeader* hdr = nullptr;

@@ -69,6 +69,9 @@ cudaError_t launch_tree_init_staged(dev::TreeHeader* const* trees, uint32_t n, c
                                     cudaStream_t stream);
 // Work prefix of `level` over the batch, for interval (point = false) or
 // point passes with `point_k` cells per lane.
+// out[3i..3i+2] = overflow flags, node words used, tape words used of tree i.
+cudaError_t launch_gather_usage(dev::TreeHeader* const* trees, uint32_t n, unsigned long long* out,
+                                cudaStream_t stream);
 cudaError_t launch_level_scan(const LevelLaunch& a, bool point, int point_k, cudaStream_t stream);
 cudaError_t launch_level(const LevelLaunch& a, const LevelPlan& plan, int rounding, bool point, cudaStream_t stream);
 

@@ -809,6 +809,20 @@ __global__ void tree_init_staged_kernel(TreeHeader* const* trees, uint32_t n, co
     }
 }
 
+// Pool use of n trees after a voxelization, for a host that must not read
+// the headers synchronously: out[3i] = overflow flags, out[3i+1] = node words
+// used, out[3i+2] = tape words used.
+__global__ void gather_usage_kernel(TreeHeader* const* trees, uint32_t n, unsigned long long* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const TreeHeader* H = trees[i];
+    const uint32_t last = H->levels - 1;
+    const uint32_t count = level_count(H, last, H->node_cap, H->node_size[last]);
+    out[3 * i] = H->overflow;
+    out[3 * i + 1] = H->node_ofs[last] + (unsigned long long)count * H->node_size[last];
+    out[3 * i + 2] = min(H->tape_top, H->tape_cap);
+}
+
 // Work accounting (run on demand, outside the level passes): for every node of
 // `level`, the op-weighted FP32 work of evaluating its tape on all its cells,
 // with the interval weights (interior levels) or the point weights (last level).
@@ -947,6 +961,13 @@ cudaError_t launch_level(const LevelLaunch& a, const LevelPlan& plan, int roundi
         if (rounding) dev::interval_level_kernel<1, 1><<<plan.blocks, 32, smem, stream>>>(b);
         else dev::interval_level_kernel<0, 1><<<plan.blocks, 32, smem, stream>>>(b);
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gather_usage(dev::TreeHeader* const* trees, uint32_t n, unsigned long long* out,
+                                cudaStream_t stream) {
+    if (n == 0) return cudaSuccess;
+    dev::gather_usage_kernel<<<(n + 127) / 128, 128, 0, stream>>>(trees, n, out);
     return cudaGetLastError();
 }
 

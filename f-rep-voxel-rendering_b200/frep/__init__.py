@@ -409,15 +409,31 @@ class Batch:
     def set_tapes(self):
         self._tapes = (C.c_void_p * len(self.storages))(*[s.tape.handle.value for s in self.storages])
 
-    def _times(self, tape_times):
+    @staticmethod
+    def _times(tape_times):
         if tape_times is None:
             return None
-        return (C.c_float * len(self.storages))(*[float(t) for t in tape_times])
+        return (C.c_float * len(tape_times))(*[float(t) for t in tape_times])
 
     def info(self) -> "L.BatchInfo":
         out = L.BatchInfo()
         L.check(L.lib().frep_batch_get_info(self._h, C.byref(out)))
         return out
+
+    def set_trees(self, storages: list) -> None:
+        """Replaces the tree set (a serving loop's next step)."""
+        self.storages = list(storages)
+        arr = (C.c_void_p * len(self.storages))(*[s.tree.value for s in self.storages])
+        L.check(L.lib().frep_batch_set_trees(self._h, arr, len(self.storages)))
+        self.set_tapes()
+
+    def render_frames(self, storages, cameras, sizes, rgba, hits=None, lights=None, tape_times=None, stream=None):
+        """One launch rendering frame i of storages[i] (repeats allowed)."""
+        trees = (C.c_void_p * len(storages))(*[s.tree.value for s in storages])
+        cams, imgs = self._frames(cameras, sizes, rgba, hits)
+        lt = (lights or Lights()).struct()
+        L.check(L.lib().frep_batch_render_frames(self._h, trees, len(storages), cams, C.byref(lt),
+                                                 self._times(tape_times), imgs, _stream_ptr(stream)))
 
     def set_tuning(self, interval_warps_per_block: int = 0, point_warps_per_block: int = 0) -> None:
         L.check(L.lib().frep_batch_set_tuning(self._h, interval_warps_per_block, point_warps_per_block))
@@ -458,3 +474,72 @@ class Batch:
         lt = (lights or Lights()).struct()
         L.check(L.lib().frep_batch_run(self._h, self._tapes, self._times(tape_times), cams, C.byref(lt), imgs,
                                        1 if graph else 0, _stream_ptr(stream)))
+
+
+REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = range(4)
+
+
+class Server:
+    """Request loop with continuous batching (frep_server): scenes are
+    registered once; each request (scene, camera, tape time, host image) joins
+    the next step the scheduler forms; trees stay resident in a device arena
+    of `hbm_budget_bytes` and are evicted least recently used."""
+
+    def __init__(self, ctx: Context, hbm_budget_bytes: int = 0, max_batch: int = 0, max_inflight: int = 0,
+                 lights: Lights | None = None, warps=(0, 0)):
+        self.ctx = ctx
+        cfg = L.ServerConfig(hbm_budget_bytes, max_batch, max_inflight, warps[0], warps[1])
+        lt = (lights or Lights()).struct()
+        self._h = C.c_void_p()
+        L.check(L.lib().frep_server_create(ctx._h, C.byref(cfg), C.byref(lt), C.byref(self._h)))
+        self._keep = {}  # request id -> host buffer (kept alive until done)
+
+    def close(self):
+        if self._h is not None and self._h.value and L._lib is not None:
+            L.lib().frep_server_destroy(self._h)
+        self._h = C.c_void_p()
+        self._keep.clear()
+
+    def __del__(self):
+        self.close()
+
+    def add_scene(self, tape: Tape, grid_dims, low_vertex, world_size, node_words: int = 0, tape_words: int = 0,
+                  point_cells_per_lane: int = 0, rounding: int = ROUND_OUTWARD) -> int:
+        vs = VoxelStorage(grid_dims, low_vertex, world_size)
+        g = vs.grid_struct()
+        opts = L.VoxelizeOpts(rounding, 1, node_words, tape_words, point_cells_per_lane, 0)
+        sid = C.c_uint64()
+        L.check(L.lib().frep_server_add_scene(self._h, tape.handle, C.byref(g), C.byref(opts), C.byref(sid)))
+        return sid.value
+
+    def submit(self, scene: int, camera: Camera, tape_time: float, width: int, height: int, out) -> int:
+        """out: a host uint8 tensor/array of height*width*4 bytes (pinned for
+        an asynchronous copy); written when the request completes."""
+        ptr = out.data_ptr() if hasattr(out, "data_ptr") else out.ctypes.data
+        req = L.RequestStruct(scene, camera.struct(width, height), float(tape_time), ptr)
+        rid = C.c_uint64()
+        L.check(L.lib().frep_server_submit(self._h, C.byref(req), C.byref(rid)))
+        self._keep[rid.value] = out
+        return rid.value
+
+    def poll(self, rid: int) -> L.RequestStatus:
+        st = L.RequestStatus()
+        L.check(L.lib().frep_server_poll(self._h, rid, C.byref(st)))
+        if st.state in (REQ_DONE, REQ_FAILED):
+            self._keep.pop(rid, None)
+        return st
+
+    def wait(self, rid: int, timeout_ms: int = 60000) -> L.RequestStatus:
+        st = L.RequestStatus()
+        L.check(L.lib().frep_server_wait(self._h, rid, timeout_ms, C.byref(st)))
+        self._keep.pop(rid, None)
+        return st
+
+    def drain(self, timeout_ms: int = 600000) -> None:
+        L.check(L.lib().frep_server_drain(self._h, timeout_ms))
+        self._keep.clear()
+
+    def stats(self, reset: bool = False) -> dict:
+        s = L.ServerStats()
+        L.check(L.lib().frep_server_get_stats(self._h, 1 if reset else 0, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in L.ServerStats._fields_}

@@ -67,6 +67,28 @@ class CameraStruct(C.Structure):
                 ("jitter_seed", C.c_float)]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("hbm_budget", C.c_uint64), ("max_batch", C.c_uint32), ("max_inflight", C.c_uint32),
+                ("interval_warps_per_block", C.c_uint32), ("point_warps_per_block", C.c_uint32)]
+
+
+class RequestStruct(C.Structure):
+    _fields_ = [("scene", C.c_uint64), ("camera", CameraStruct), ("tape_time", C.c_float),
+                ("rgba8", C.c_void_p)]
+
+
+class RequestStatus(C.Structure):
+    _fields_ = [("state", C.c_int32), ("status", C.c_int32), ("voxelized", C.c_uint32), ("retries", C.c_uint32),
+                ("latency_ms", C.c_double)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [(k, C.c_uint64) for k in ("submitted", "completed", "failed", "voxelized", "rerendered",
+                                          "evictions", "steps", "resident_trees", "resident_bytes",
+                                          "arena_bytes")] + \
+               [(k, C.c_double) for k in ("p50_ms", "p99_ms", "mean_ms", "max_ms", "scenes_per_s")]
+
+
 class LightsStruct(C.Structure):
     _fields_ = [("count", C.c_uint32), ("direction", (C.c_float * 3) * MAX_LIGHTS),
                 ("color", (C.c_float * 4) * MAX_LIGHTS), ("ambient", C.c_float * 4),
@@ -112,6 +134,16 @@ _SIGS = {
     "frep_batch_render": (C.c_int, [_P, _P, C.POINTER(LightsStruct), _P, _P, _P]),
     "frep_batch_run": (C.c_int, [_P, _P, _P, _P, C.POINTER(LightsStruct), _P, C.c_int, _P]),
     "frep_batch_set_profiling": (C.c_int, [_P, C.c_int]),
+    "frep_batch_set_trees": (C.c_int, [_P, _P, C.c_uint32]),
+    "frep_server_create": (C.c_int, [_P, C.POINTER(ServerConfig), C.POINTER(LightsStruct), C.POINTER(_P)]),
+    "frep_server_destroy": (None, [_P]),
+    "frep_server_add_scene": (C.c_int, [_P, _P, C.POINTER(Grid), C.POINTER(VoxelizeOpts), C.POINTER(C.c_uint64)]),
+    "frep_server_submit": (C.c_int, [_P, C.POINTER(RequestStruct), C.POINTER(C.c_uint64)]),
+    "frep_server_poll": (C.c_int, [_P, C.c_uint64, C.POINTER(RequestStatus)]),
+    "frep_server_wait": (C.c_int, [_P, C.c_uint64, C.c_uint32, C.POINTER(RequestStatus)]),
+    "frep_server_drain": (C.c_int, [_P, C.c_uint32]),
+    "frep_server_get_stats": (C.c_int, [_P, C.c_int, C.POINTER(ServerStats)]),
+    "frep_batch_render_frames": (C.c_int, [_P, _P, C.c_uint32, _P, C.POINTER(LightsStruct), _P, _P, _P]),
     "frep_batch_set_tuning": (C.c_int, [_P, C.c_uint32, C.c_uint32]),
     "frep_batch_get_info": (C.c_int, [_P, C.POINTER(BatchInfo)]),
     "frep_batch_timings": (C.c_int, [_P, _P]),

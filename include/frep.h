@@ -310,6 +310,16 @@ void frep_batch_destroy(frep_batch* batch);
 frep_status frep_batch_voxelize(frep_batch* batch, const frep_tape* const* tapes, const float* tape_times,
                                 void* stream);
 
+/* Replaces the batch's tree set (any size, same rounding); plans, scratch
+ * and upload areas are kept and grown as needed. */
+frep_status frep_batch_set_trees(frep_batch* batch, frep_tree* const* trees, uint32_t n);
+
+/* Renders frame i of tree frame_trees[i] (any voxelized trees of the batch's
+ * context, repeats allowed) with cameras[i] into images[i]: one launch. */
+frep_status frep_batch_render_frames(frep_batch* batch, const frep_tree* const* frame_trees, uint32_t n_frames,
+                                     const frep_camera* cameras, const frep_lights* lights,
+                                     const float* tape_times, const frep_image* images, void* stream);
+
 /* Renders tree i with cameras[i] into images[i] (one launch for all frames). */
 frep_status frep_batch_render(frep_batch* batch, const frep_camera* cameras, const frep_lights* lights,
                               const float* tape_times, const frep_image* images, void* stream);
@@ -348,6 +358,83 @@ frep_status frep_batch_set_tuning(frep_batch* batch, uint32_t interval_warps_per
  * = the frames (0 if none were rendered since profiling was enabled). */
 frep_status frep_batch_set_profiling(frep_batch* batch, int enable);
 frep_status frep_batch_timings(frep_batch* batch, float ms[3 * FREP_MAX_LEVELS + 2]);
+
+/* ---------------------------------------------------------------------------
+ * Serving (no counterpart in the reference, whose Application voxelizes and
+ * renders one scene per frame, application.cpp:60-93)
+ *
+ * A request loop with continuous batching: requests (a registered scene, a
+ * camera, a tape time, a host image) are queued by frep_server_submit from
+ * any thread; a scheduler thread forms a step from whatever is queued (up to
+ * max_batch requests) whenever fewer than max_inflight steps are on the
+ * device, so requests that arrive while others run join the next step and
+ * the device works through steps back to back. A step voxelizes, in one
+ * batched launch per level pass, the scenes that are not resident at the
+ * requested time and renders every request of the step in one launch; the
+ * images are copied to the requests' host buffers in the same stream.
+ * Trees (nodes + shortened tapes) stay resident in one device arena of
+ * hbm_budget bytes; a request for a resident scene at the same tape time
+ * (any time, for scenes that do not read T) is a re-render only. A scene
+ * that does not fit is admitted after evicting least recently used trees; a
+ * request that cannot be admitted waits. Pools are sized from
+ * frep_voxelize_opts when given, else estimated and then refitted from the
+ * scene's measured use; a voxelization that overflows its pools is retried
+ * with doubled pools (at most 4 times, then FREP_ERR_CAPACITY).
+ * ------------------------------------------------------------------------- */
+
+typedef struct frep_server frep_server;
+
+typedef struct frep_server_config {
+    uint64_t hbm_budget;      /* bytes of the tree arena (0 = 80 % of the context's free budget) */
+    uint32_t max_batch;       /* requests per step (0 = 512)                                     */
+    uint32_t max_inflight;    /* steps enqueued on the device at once (0 = 2)                    */
+    uint32_t interval_warps_per_block, point_warps_per_block;  /* frep_batch_set_tuning         */
+} frep_server_config;
+
+typedef struct frep_request {
+    uint64_t scene;           /* from frep_server_add_scene                                      */
+    frep_camera camera;       /* width x height of the image                                     */
+    float tape_time;
+    uint8_t* rgba8;           /* host buffer of width*height*4 bytes, written by the device copy;
+                                 page-locked memory lets the copy run asynchronously             */
+} frep_request;
+
+enum { FREP_REQ_QUEUED = 0, FREP_REQ_RUNNING = 1, FREP_REQ_DONE = 2, FREP_REQ_FAILED = 3 };
+
+typedef struct frep_request_status {
+    int32_t state;            /* FREP_REQ_*                                                      */
+    int32_t status;           /* frep_status of a failed request                                 */
+    uint32_t voxelized;       /* 1: this request's step voxelized the scene; 0: re-render only   */
+    uint32_t retries;
+    double latency_ms;        /* submit -> image in the host buffer (done requests)              */
+} frep_request_status;
+
+typedef struct frep_server_stats {
+    uint64_t submitted, completed, failed, voxelized, rerendered, evictions, steps;
+    uint64_t resident_trees, resident_bytes, arena_bytes;
+    double p50_ms, p99_ms, mean_ms, max_ms;  /* latency of requests completed since the last reset */
+    double scenes_per_s;      /* completed / (last completion - first submit), since the reset  */
+} frep_server_stats;
+
+/* lights: used for every request (NULL = frep_lights_default). */
+frep_status frep_server_create(frep_ctx* ctx, const frep_server_config* config, const frep_lights* lights,
+                               frep_server** out);
+/* Finishes the work on the device, stops the threads, frees everything. */
+void frep_server_destroy(frep_server* server);
+/* Registers a scene (the tape is copied). opts: rounding, shortening, pool
+ * sizes (0 = estimated), last-level cells per lane. */
+frep_status frep_server_add_scene(frep_server* server, const frep_tape* tape, const frep_grid* grid,
+                                  const frep_voxelize_opts* opts, uint64_t* scene);
+frep_status frep_server_submit(frep_server* server, const frep_request* request, uint64_t* request_id);
+frep_status frep_server_poll(frep_server* server, uint64_t request_id, frep_request_status* status);
+/* Waits until the request is done or failed, at most timeout_ms
+ * (FREP_ERR_TIMEOUT). */
+frep_status frep_server_wait(frep_server* server, uint64_t request_id, uint32_t timeout_ms,
+                             frep_request_status* status);
+/* Waits until every submitted request is done or failed. */
+frep_status frep_server_drain(frep_server* server, uint32_t timeout_ms);
+/* Statistics; reset != 0 clears the latency record and throughput window. */
+frep_status frep_server_get_stats(frep_server* server, int reset, frep_server_stats* stats);
 
 #ifdef __cplusplus
 }

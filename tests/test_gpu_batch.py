@@ -157,3 +157,34 @@ def test_cached_plans_of_many_trees(ctx):
     assert oracle.canonical_of_export(a.export())[0] == first
     a.cleanup()
     b.cleanup()
+
+
+def test_set_trees_and_render_frames(ctx):
+    """A batch object serves changing tree sets (one set per call, upload areas
+    in rotation) and renders frames of any voxelized trees, repeats included."""
+    import torch
+    scs = _scenes()
+    want = [_alone(ctx, sc, 0.05 * i) for i, sc in enumerate(scs)]
+    storages = [frep.VoxelStorage(sc.grid_dims, sc.low_vertex, sc.world_size).init(ctx, sc.shape) for sc in scs]
+    batch = frep.Batch(ctx, storages[:2])
+    batch.voxelize(tape_times=[0.0, 0.05])
+    batch.set_trees(storages[2:5])
+    batch.voxelize(tape_times=[0.1, 0.15, 0.2])
+    batch.set_trees(storages[5:])
+    batch.voxelize(tape_times=[0.05 * i for i in range(5, len(scs))])
+    order = [4, 0, 4, 2, 5, 1, 3, 0]
+    dev = torch.device("cuda", 0)
+    rgba = [torch.zeros((scs[i].height, scs[i].width, 4), dtype=torch.uint8, device=dev) for i in order]
+    hits = [torch.zeros((scs[i].height, scs[i].width, 8), dtype=torch.int32, device=dev) for i in order]
+    batch.render_frames([storages[i] for i in order], [scs[i].camera for i in order],
+                        [(scs[i].width, scs[i].height) for i in order], rgba, hits, lights=frep.Lights(shadow_mask=1),
+                        tape_times=[0.05 * i for i in order])
+    torch.cuda.synchronize()
+    for k, i in enumerate(order):
+        exp = storages[i].export()
+        assert oracle.canonical_of_export(exp)[0] == want[i][0]
+        np.testing.assert_array_equal(rgba[k].cpu().numpy(), want[i][1])
+        cells = oracle.hit_cells(hits[k].cpu().numpy().view(np.uint32), exp.dims, exp.node_offset, exp.node_size,
+                                 exp.nodes)
+        np.testing.assert_array_equal(cells, want[i][2])
+    batch.close()
