@@ -58,6 +58,10 @@ def parse():
     ap.add_argument("--no-tune", action="store_true", help="batch: default branching, no autotuning")
     ap.add_argument("--tune-cache", default=None, help="batch: autotuner cache file (JSON)")
     ap.add_argument("--budget-gb", type=int, default=150, help="HBM budget of the context, GB")
+    ap.add_argument("--serve-seconds", type=float, default=10.0,
+                    help="batch: seconds of the serving run after the batch measurements (0 = none)")
+    ap.add_argument("--serve-rate", type=float, default=1000.0, help="batch: Poisson request rate, requests/s")
+    ap.add_argument("--serve-budget-gb", type=int, default=120, help="batch: tree arena of the server, GB")
     ap.add_argument("--grid", default="16,16,8",
                     help="large: tree branching per level (profiling uses a smaller grid of the same scene)")
     ap.add_argument("--res", default=None, help="render resolution WxH (batch 512x512, large 1920x1080)")
@@ -415,6 +419,92 @@ def run_reference_batch(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def serve_phase(args, ctx, scs, chosen, pools, warps):
+    """Serving: a Poisson request stream at args.serve_rate for
+    args.serve_seconds. Each request is a scene plus an orbit camera pose at
+    the batch resolution: with probability 0.3 a repeat of one of the 64 most
+    recently requested scenes (a re-render when it is still resident), else a
+    new scene of the batching distribution (a batch scene's tape with its
+    constants scaled by U[0.9, 1.1], at that scene's tuned branching). Trees
+    stay resident in an arena of args.serve_budget_gb GB, evicted least
+    recently used. Latency = submit -> image in (pinned) host memory."""
+    import collections
+    import numpy as np
+    import torch
+    import frep
+    from frep import scenes as S
+
+    W, H = args.width, args.height
+    rng = np.random.default_rng(23)
+    n_req = max(1, int(args.serve_rate * args.serve_seconds))
+    arrivals = np.cumsum(rng.exponential(1.0 / args.serve_rate, n_req))
+    srv = frep.Server(ctx, hbm_budget_bytes=args.serve_budget_gb << 30, lights=frep.Lights(shadow_mask=1),
+                      warps=warps)
+    wides = [sc.shape.wide() for sc in scs]
+    recent = collections.deque(maxlen=64)
+    plan = []
+    n_new = 0
+
+    def new_scene():
+        b = int(rng.integers(len(scs)))
+        tape = S.jitter_tape(wides[b], rng)
+        dims, k = chosen[b]
+        # jittered sizes change the surface by up to ~20 %: start with more pool
+        return srv.add_scene(tape, dims, scs[b].low_vertex, scs[b].world_size,
+                             node_words=int(pools[b].node_words * 1.5) + 4096,
+                             tape_words=int(pools[b].tape_words * 1.5) + 4096, point_cells_per_lane=k)
+
+    for i in range(n_req):
+        if recent and rng.random() < 0.3:
+            sid = recent[int(rng.integers(len(recent)))]
+        else:
+            sid = new_scene()
+            n_new += 1
+        recent.append(sid)
+        plan.append((sid, S.orbit_camera(rng)))
+    ring = min(n_req, 4096)  # pinned host images in rotation (4 GB at 512x512)
+    bufs = [torch.empty((H, W, 4), dtype=torch.uint8, pin_memory=True) for _ in range(ring)]
+    # warm-up (plans, upload areas, first trees): not measured
+    warm = [srv.submit(new_scene(), S.orbit_camera(rng), 0.0, W, H, bufs[i % ring]) for i in range(min(64, ring))]
+    srv.drain(600000)
+    before = srv.stats(reset=True)
+    ids = [0] * n_req
+    lag = np.zeros(n_req)  # submit - scheduled arrival
+    t0 = time.perf_counter()
+    for i, (sid, cam) in enumerate(plan):
+        target = t0 + arrivals[i]
+        while True:
+            now = time.perf_counter()
+            if now >= target:
+                break
+            time.sleep(min(target - now, 0.0005))
+        if i >= ring:
+            srv.wait(ids[i - ring], 600000)  # the host buffer is reused
+        lag[i] = time.perf_counter() - target
+        ids[i] = srv.submit(sid, cam, 0.0, W, H, bufs[i % ring])
+    srv.drain(600000)
+    st = srv.stats()
+    # open-loop latency: from the scheduled arrival, so that a late submit counts
+    server_ms = np.array([srv.poll(r).latency_ms for r in ids])
+    open_ms = server_ms + 1e3 * lag
+    for r in ids:
+        srv.release(r)
+    failed = st["failed"]
+    srv.close()
+    return {
+        "rate_req_s": args.serve_rate, "seconds": args.serve_seconds, "requests": n_req,
+        "new_scenes": n_new, "resolution": [W, H], "arena_gb": args.serve_budget_gb,
+        "p50_ms": float(np.percentile(open_ms, 50)), "p99_ms": float(np.percentile(open_ms, 99)),
+        "mean_ms": float(open_ms.mean()), "max_ms": float(open_ms.max()),
+        "server_p50_ms": st["p50_ms"], "server_p99_ms": st["p99_ms"],
+        "scenes_per_s": st["scenes_per_s"], "completed": st["completed"] - before["completed"],
+        "failed": failed - before["failed"], "voxelized": st["voxelized"] - before["voxelized"],
+        "rerendered": st["rerendered"] - before["rerendered"], "evictions": st["evictions"] - before["evictions"],
+        "steps": st["steps"] - before["steps"], "max_submit_lag_ms": float(1e3 * lag.max()),
+        "latency": "scheduled arrival -> image in pinned host memory (p50/p99_ms); server_*: submit -> image",
+    }
+
+
 def run_ours_batch(args, world, rank, local):
     import numpy as np
     import torch
@@ -595,6 +685,12 @@ def run_ours_batch(args, world, rank, local):
         "clocks": clocks.summary(),
         "gpu_launches": int((binfo.voxelize_launches + 1) * args.steps),
     }
+    batch.close()
+    for vs in storages:
+        vs.cleanup()
+    if args.serve_seconds > 0:
+        torch.cuda.synchronize()
+        line["serving"] = serve_phase(args, ctx, scs, chosen, pools, tuner.warps)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         order = cpu_sample_order(n)
@@ -608,9 +704,6 @@ def run_ours_batch(args, world, rank, local):
                                           f"voxelize + {W}x{H} render each, oracle C++ port, {threads} threads"}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    batch.close()
-    for vs in storages:
-        vs.cleanup()
     ctx.close()
 
 

@@ -80,6 +80,19 @@ frep_status frep_tape_from_reference(const uint32_t* instrs, uint32_t n_instr, c
     return FREP_OK;
 }
 
+frep_status frep_tape_from_wide(const uint64_t* instrs, uint32_t n_instr, frep_tape** out) {
+    if (!instrs || !out) return fail(FREP_ERR_INVALID_ARG, "frep_tape_from_wide: null argument");
+    auto* t = new frep_tape();
+    std::string err = frep::import_wide_tape(instrs, n_instr, &t->ct);
+    if (!err.empty()) {
+        delete t;
+        return fail(FREP_ERR_INVALID_ARG, "frep_tape_from_wide: %s", err.c_str());
+    }
+    t->build_record();
+    *out = t;
+    return FREP_OK;
+}
+
 frep_status frep_tape_get_info(const frep_tape* tape, frep_tape_info* info) {
     if (!tape || !info) return fail(FREP_ERR_INVALID_ARG, "frep_tape_get_info: null argument");
     info->n_instr = (uint32_t)tape->ct.instrs.size();

@@ -95,6 +95,7 @@ struct Scene {
     uint64_t bad_gen = ~0ull;  // a voxelization that overflowed
     uint64_t last_used = 0;  // LRU tick
     uint64_t step = 0;       // last step that referenced the tree
+    bool rebuild = false;    // pools grew after an overflow: recreate the tree
 };
 
 struct Request {
@@ -259,16 +260,28 @@ void finish_request(frep_server* sv, Request& R, int32_t state, int32_t status, 
     }
 }
 
-// Forms and enqueues one step from the pending requests (lock held).
-// Returns false when nothing could be scheduled.
-bool form_step(frep_server* sv) {
-    const uint64_t step_id = sv->next_step;
-    sv->tick++;
-    Step st;
-    st.id = step_id;
+// What one step enqueues, gathered under the lock so that the enqueue itself
+// runs without it (Request objects may move when the request map grows; the
+// Scene objects and their trees do not, and only the scheduler thread
+// creates or destroys trees).
+struct StepPlan {
+    Step step;
     std::vector<const frep_tape*> vtapes;
     std::vector<frep_tree*> vtrees;
     std::vector<float> vtimes;
+    std::vector<const frep_tree*> ftrees;
+    std::vector<frep_camera> cams;
+    std::vector<float> ftimes;
+    std::vector<uint8_t*> dst;
+};
+
+// Chooses the step's requests from the pending queue and places their trees
+// (lock held). Returns false when nothing could be scheduled.
+bool plan_step(frep_server* sv, StepPlan* P) {
+    const uint64_t step_id = sv->next_step;
+    sv->tick++;
+    Step& st = P->step;
+    st.id = step_id;
     std::unordered_map<uint64_t, float> vox_time;
     std::deque<uint64_t> deferred;
     const uint32_t max_batch = sv->cfg.max_batch;
@@ -277,6 +290,13 @@ bool form_step(frep_server* sv) {
         sv->pending.pop_front();
         Request& R = sv->requests[rid];
         Scene& S = *sv->scenes[R.req.scene];
+        if (S.rebuild && S.tree && S.step != step_id) {
+            // an overflowed voxelization: rebuild at the grown size
+            frep_tree_destroy(S.tree);
+            sv->arena.release(S.arena_off, S.arena_bytes);
+            S.tree = nullptr;
+            S.rebuild = false;
+        }
         const float t = R.req.tape_time;
         const bool tdep = S.tape.ct.uses_time;
         auto same = [&](float a) { return !tdep || a == t; };
@@ -308,9 +328,9 @@ bool form_step(frep_server* sv) {
             S.valid = true;
             S.time = t;
             S.gen++;
-            vtapes.push_back(&S.tape);
-            vtrees.push_back(S.tree);
-            vtimes.push_back(t);
+            P->vtapes.push_back(&S.tape);
+            P->vtrees.push_back(S.tree);
+            P->vtimes.push_back(t);
             st.vox_scenes.push_back(R.req.scene);
             st.vox_gens.push_back(S.gen);
             R.voxelized = 1;
@@ -320,71 +340,72 @@ bool form_step(frep_server* sv) {
         R.gen = S.gen;
         R.state = FREP_REQ_RUNNING;
         st.requests.push_back(rid);
+        P->ftrees.push_back(S.tree);
+        P->cams.push_back(R.req.camera);
+        P->ftimes.push_back(t);
+        P->dst.push_back(R.req.rgba8);
     }
     while (!deferred.empty()) {
         sv->pending.push_front(deferred.back());
         deferred.pop_back();
     }
     if (st.requests.empty()) return false;
+    sv->next_step++;
+    st.ring = sv->ring_next;
+    sv->ring_next = (sv->ring_next + 1) % kRing;
+    return true;
+}
 
-    // ---- enqueue on the device ----
+// Enqueues a planned step on the server's stream (no lock held; only the
+// scheduler thread runs this and it owns the batch, frame area and ring).
+frep_status enqueue_step(frep_server* sv, StepPlan& P) {
     frep_status r = FREP_OK;
     cudaStream_t s = sv->stream;
-    if (!vtrees.empty()) {
+    Step& st = P.step;
+    if (!P.vtrees.empty()) {
         if (!sv->batch) {
-            r = frep_batch_create(sv->ctx, vtrees.data(), (uint32_t)vtrees.size(), &sv->batch);
+            r = frep_batch_create(sv->ctx, P.vtrees.data(), (uint32_t)P.vtrees.size(), &sv->batch);
             if (r == FREP_OK && (sv->cfg.interval_warps_per_block || sv->cfg.point_warps_per_block))
                 r = frep_batch_set_tuning(sv->batch, sv->cfg.interval_warps_per_block, sv->cfg.point_warps_per_block);
         } else {
-            r = frep_batch_set_trees(sv->batch, vtrees.data(), (uint32_t)vtrees.size());
+            r = frep_batch_set_trees(sv->batch, P.vtrees.data(), (uint32_t)P.vtrees.size());
         }
-        if (r == FREP_OK) r = frep_batch_voxelize(sv->batch, vtapes.data(), vtimes.data(), s);
+        if (r == FREP_OK) r = frep_batch_voxelize(sv->batch, P.vtapes.data(), P.vtimes.data(), s);
     }
-    const uint32_t nf = (uint32_t)st.requests.size();
-    std::vector<const frep_tree*> ftrees(nf);
-    std::vector<frep_camera> cams(nf);
-    std::vector<float> ftimes(nf);
+    const uint32_t nf = (uint32_t)P.cams.size();
     std::vector<frep_image> imgs(nf);
     std::vector<uint64_t> ofs(nf);
     uint64_t total = 0;
     for (uint32_t i = 0; i < nf; i++) {
-        const Request& R = sv->requests[st.requests[i]];
         ofs[i] = total;
-        total += align_up((uint64_t)R.req.camera.width * R.req.camera.height * 4, 256);
+        total += align_up((uint64_t)P.cams[i].width * P.cams[i].height * 4, 256);
     }
     if (r == FREP_OK) r = ensure_frames(sv, total);
     if (r == FREP_OK && !sv->batch) r = fail(FREP_ERR_INVALID_ARG, "frep_server: no voxelized tree to render");
     if (r == FREP_OK) {
         for (uint32_t i = 0; i < nf; i++) {
-            const Request& R = sv->requests[st.requests[i]];
-            ftrees[i] = sv->scenes[R.req.scene]->tree;
-            cams[i] = R.req.camera;
-            ftimes[i] = R.req.tape_time;
             imgs[i].rgba8 = sv->d_frames + ofs[i];
             imgs[i].hits = nullptr;
         }
-        r = frep_batch_render_frames(sv->batch, ftrees.data(), nf, cams.data(), &sv->lights, ftimes.data(),
+        r = frep_batch_render_frames(sv->batch, P.ftrees.data(), nf, P.cams.data(), &sv->lights, P.ftimes.data(),
                                      imgs.data(), s);
     }
     // pool use of the voxelized trees, read back in the step
-    st.ring = sv->ring_next;
-    sv->ring_next = (sv->ring_next + 1) % kRing;
-    if (r == FREP_OK) r = ensure_ring(sv, (uint32_t)vtrees.size());
-    if (r == FREP_OK && !vtrees.empty()) {
-        for (size_t i = 0; i < vtrees.size(); i++) sv->h_tab[st.ring][i] = vtrees[i]->hdr;
-        cudaError_t e = cudaMemcpyAsync(sv->d_tab[st.ring], sv->h_tab[st.ring], sizeof(void*) * vtrees.size(),
+    if (r == FREP_OK) r = ensure_ring(sv, (uint32_t)P.vtrees.size());
+    if (r == FREP_OK && !P.vtrees.empty()) {
+        for (size_t i = 0; i < P.vtrees.size(); i++) sv->h_tab[st.ring][i] = P.vtrees[i]->hdr;
+        cudaError_t e = cudaMemcpyAsync(sv->d_tab[st.ring], sv->h_tab[st.ring], sizeof(void*) * P.vtrees.size(),
                                         cudaMemcpyHostToDevice, s);
         if (e == cudaSuccess)
-            e = frep::launch_gather_usage(sv->d_tab[st.ring], (uint32_t)vtrees.size(), sv->d_use[st.ring], s);
+            e = frep::launch_gather_usage(sv->d_tab[st.ring], (uint32_t)P.vtrees.size(), sv->d_use[st.ring], s);
         if (e == cudaSuccess)
-            e = cudaMemcpyAsync(sv->h_use[st.ring], sv->d_use[st.ring], sizeof(unsigned long long) * 3 * vtrees.size(),
-                                cudaMemcpyDeviceToHost, s);
+            e = cudaMemcpyAsync(sv->h_use[st.ring], sv->d_use[st.ring],
+                                sizeof(unsigned long long) * 3 * P.vtrees.size(), cudaMemcpyDeviceToHost, s);
         if (e != cudaSuccess) r = cuda_fail(e, "frep_server: pool use read-back");
     }
     for (uint32_t i = 0; i < nf && r == FREP_OK; i++) {
-        const Request& R = sv->requests[st.requests[i]];
-        cudaError_t e = cudaMemcpyAsync(R.req.rgba8, sv->d_frames + ofs[i],
-                                        (size_t)R.req.camera.width * R.req.camera.height * 4, cudaMemcpyDeviceToHost, s);
+        cudaError_t e = cudaMemcpyAsync(P.dst[i], sv->d_frames + ofs[i], (size_t)P.cams[i].width * P.cams[i].height * 4,
+                                        cudaMemcpyDeviceToHost, s);
         if (e != cudaSuccess) r = cuda_fail(e, "frep_server: image copy");
     }
     if (r == FREP_OK) {
@@ -392,20 +413,7 @@ bool form_step(frep_server* sv) {
         if (e == cudaSuccess) e = cudaEventRecord(st.done, s);
         if (e != cudaSuccess) r = cuda_fail(e, "frep_server: step event");
     }
-    if (r != FREP_OK) {
-        // The step could not be enqueued: fail its requests, invalidate what it touched.
-        const auto now = Clock::now();
-        for (uint64_t rid : st.requests) finish_request(sv, sv->requests[rid], FREP_REQ_FAILED, r, now);
-        for (uint64_t sc : st.vox_scenes) sv->scenes[sc]->valid = false;
-        if (st.done) cudaEventDestroy(st.done);
-        sv->cv_done.notify_all();
-        return true;
-    }
-    sv->next_step++;
-    sv->steps++;
-    sv->inflight.push_back(std::move(st));
-    sv->cv_steps.notify_all();
-    return true;
+    return r;
 }
 
 void scheduler_main(frep_server* sv) {
@@ -416,7 +424,8 @@ void scheduler_main(frep_server* sv) {
             return sv->stop || (!sv->pending.empty() && sv->inflight.size() < sv->cfg.max_inflight);
         });
         if (sv->stop) break;
-        if (!form_step(sv)) {
+        StepPlan P;
+        if (!plan_step(sv, &P)) {
             // Nothing could be placed, although every tree outside the step
             // being formed may be evicted: the arena is exhausted for good.
             const auto now = Clock::now();
@@ -425,7 +434,24 @@ void scheduler_main(frep_server* sv) {
                 sv->pending.pop_front();
             }
             sv->cv_done.notify_all();
+            continue;
         }
+        lock.unlock();
+        const frep_status r = enqueue_step(sv, P);
+        lock.lock();
+        Step& st = P.step;
+        if (r != FREP_OK) {
+            // The step could not be enqueued: fail its requests, invalidate what it touched.
+            const auto now = Clock::now();
+            for (uint64_t rid : st.requests) finish_request(sv, sv->requests[rid], FREP_REQ_FAILED, r, now);
+            for (uint64_t sc : st.vox_scenes) sv->scenes[sc]->valid = false;
+            if (st.done) cudaEventDestroy(st.done);
+            sv->cv_done.notify_all();
+            continue;
+        }
+        sv->steps++;
+        sv->inflight.push_back(std::move(st));
+        sv->cv_steps.notify_all();
     }
 }
 
@@ -457,15 +483,11 @@ void completer_main(frep_server* sv) {
                 if (u[0] & 2u) S.tape_words *= 2;
                 S.bad_gen = st.vox_gens[i];
                 if (S.gen == st.vox_gens[i]) {
-                    // Rebuild at the new size on the next admission. Steps
-                    // already enqueued that use the tree run before any step
-                    // that reuses its memory (one stream).
+                    // The scheduler rebuilds the tree at the new size when the
+                    // scene is next requested (steps already enqueued that use
+                    // it run first: one stream).
                     S.valid = false;
-                    if (S.tree) {
-                        frep_tree_destroy(S.tree);
-                        sv->arena.release(S.arena_off, S.arena_bytes);
-                        S.tree = nullptr;
-                    }
+                    S.rebuild = true;
                 }
             } else if (!S.opts.node_words) {
                 // refit: what this voxelization used, plus headroom
@@ -598,13 +620,14 @@ frep_status frep_server_submit(frep_server* sv, const frep_request* req, uint64_
     if (!sv || !req || !request_id || !req->rgba8) return fail(FREP_ERR_INVALID_ARG, "frep_server_submit: null argument");
     if (req->camera.width == 0 || req->camera.height == 0 || req->camera.projection > 1)
         return fail(FREP_ERR_INVALID_ARG, "frep_server_submit: bad camera");
+    const auto submitted_at = Clock::now();  // latency includes any wait for the lock
     std::lock_guard<std::mutex> lock(sv->mu);
     if (sv->fatal != FREP_OK) return fail(sv->fatal, "frep_server: a step failed on the device");
     if (req->scene >= sv->scenes.size()) return fail(FREP_ERR_INVALID_ARG, "frep_server_submit: unknown scene");
     const uint64_t id = sv->next_request++;
     Request& R = sv->requests[id];
     R.req = *req;
-    R.submit = Clock::now();
+    R.submit = submitted_at;
     if (!sv->window_open) {
         sv->window_open = true;
         sv->window_start = R.submit;
@@ -645,6 +668,18 @@ frep_status frep_server_wait(frep_server* sv, uint64_t request_id, uint32_t time
     if (status) fill_status(it->second, status);
     if (!ok) return fail(FREP_ERR_TIMEOUT, "frep_server_wait: request %llu not finished after %u ms",
                          (unsigned long long)request_id, timeout_ms);
+    return FREP_OK;
+}
+
+frep_status frep_server_release(frep_server* sv, uint64_t request_id) {
+    if (!sv) return fail(FREP_ERR_INVALID_ARG, "frep_server_release: null server");
+    std::lock_guard<std::mutex> lock(sv->mu);
+    auto it = sv->requests.find(request_id);
+    if (it == sv->requests.end()) return fail(FREP_ERR_INVALID_ARG, "frep_server_release: unknown request");
+    if (it->second.state != FREP_REQ_DONE && it->second.state != FREP_REQ_FAILED)
+        return fail(FREP_ERR_INVALID_ARG, "frep_server_release: request %llu is not finished",
+                    (unsigned long long)request_id);
+    sv->requests.erase(it);
     return FREP_OK;
 }
 

@@ -425,6 +425,38 @@ std::string import_reference_tape(const uint32_t* instrs, uint32_t n, const floa
     return "";
 }
 
+std::string import_wide_tape(const uint64_t* instrs, uint32_t n, CompiledTape* out) {
+    if (!instrs || n == 0) return "empty tape";
+    out->instrs.assign(instrs, instrs + n);
+    out->ref_instrs.clear();
+    out->const_pool.clear();
+    out->fits_reference = false;
+    out->n_minmax = 0;
+    out->uses_time = false;
+    uint32_t max_slot = 3;
+    bool t_written = false;  // slot 3 holds T until an instruction writes it
+    for (uint32_t i = 0; i < n; i++) {
+        const uint64_t w = instrs[i];
+        const uint32_t op = instr_op(w), o = instr_out(w);
+        if (op >= OP_COUNT || (w & 0xFF00ull)) return "unknown opcode at instruction " + std::to_string(i);
+        max_slot = std::max(max_slot, o);
+        if (op != OP_CONST) {
+            const bool binary = op == OP_ADD || op == OP_SUB || op == OP_MUL || op == OP_DIV ||
+                                op == OP_MIN || op == OP_MAX;
+            const uint32_t a = instr_a(w), b = instr_b(w);
+            max_slot = std::max(max_slot, a);
+            if (binary) max_slot = std::max(max_slot, b);
+            if (!t_written && (a == 3 || (binary && b == 3))) out->uses_time = true;
+            if (op == OP_MIN || op == OP_MAX) out->n_minmax++;
+        }
+        if (o == 3) t_written = true;
+    }
+    if (instr_out(instrs[n - 1]) != 0) return "the last instruction does not write slot 0";
+    if (max_slot > 0xFFFE) return "more than 65535 slots";
+    out->n_slots = max_slot + 1;
+    return "";
+}
+
 float eval_point_host(const std::vector<uint64_t>& instrs, uint32_t n_slots, float x, float y,
                       float z, float t) {
     std::vector<float> s(std::max<uint32_t>(n_slots, 4), 0.0f);

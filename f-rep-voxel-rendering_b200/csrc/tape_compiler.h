@@ -72,6 +72,11 @@ struct CompiledTape {
 // topologically ordered (inputs before users) with root < n.
 std::string compile_tape(const DagNode* nodes, uint32_t n, uint32_t root, CompiledTape* out);
 
+// Imports a tape in the wide encoding (as frep_tape_get_instrs returns it):
+// validates the opcodes and derives the slot count, MIN/MAX count and whether
+// T is read.
+std::string import_wide_tape(const uint64_t* instrs, uint32_t n, CompiledTape* out);
+
 // Imports a tape in the reference's 8-bit encoding with its constant pool.
 std::string import_reference_tape(const uint32_t* instrs, uint32_t n, const float* consts,
                                   uint32_t n_consts, CompiledTape* out);

@@ -73,6 +73,14 @@ class Tape:
         return cls(_handle=h)
 
     @classmethod
+    def from_wide(cls, instrs) -> "Tape":
+        """A tape in the wide encoding (Tape.wide())."""
+        instrs = np.ascontiguousarray(instrs, np.uint64)
+        h = C.c_void_p()
+        L.check(L.lib().frep_tape_from_wide(_ptr(instrs), len(instrs), C.byref(h)))
+        return cls(_handle=h)
+
+    @classmethod
     def from_dag(cls, ops, in0, in1, consts, root) -> "Tape":
         ops = np.ascontiguousarray(ops, np.uint8)
         in0 = np.ascontiguousarray(in0, np.uint32)
@@ -534,6 +542,11 @@ class Server:
         L.check(L.lib().frep_server_wait(self._h, rid, timeout_ms, C.byref(st)))
         self._keep.pop(rid, None)
         return st
+
+    def release(self, rid: int) -> None:
+        """Forgets a finished request."""
+        L.check(L.lib().frep_server_release(self._h, rid))
+        self._keep.pop(rid, None)
 
     def drain(self, timeout_ms: int = 600000) -> None:
         L.check(L.lib().frep_server_drain(self._h, timeout_ms))

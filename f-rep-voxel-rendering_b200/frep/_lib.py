@@ -135,6 +135,7 @@ _SIGS = {
     "frep_batch_run": (C.c_int, [_P, _P, _P, _P, C.POINTER(LightsStruct), _P, C.c_int, _P]),
     "frep_batch_set_profiling": (C.c_int, [_P, C.c_int]),
     "frep_batch_set_trees": (C.c_int, [_P, _P, C.c_uint32]),
+    "frep_tape_from_wide": (C.c_int, [_P, C.c_uint32, C.POINTER(_P)]),
     "frep_server_create": (C.c_int, [_P, C.POINTER(ServerConfig), C.POINTER(LightsStruct), C.POINTER(_P)]),
     "frep_server_destroy": (None, [_P]),
     "frep_server_add_scene": (C.c_int, [_P, _P, C.POINTER(Grid), C.POINTER(VoxelizeOpts), C.POINTER(C.c_uint64)]),
@@ -142,6 +143,7 @@ _SIGS = {
     "frep_server_poll": (C.c_int, [_P, C.c_uint64, C.POINTER(RequestStatus)]),
     "frep_server_wait": (C.c_int, [_P, C.c_uint64, C.c_uint32, C.POINTER(RequestStatus)]),
     "frep_server_drain": (C.c_int, [_P, C.c_uint32]),
+    "frep_server_release": (C.c_int, [_P, C.c_uint64]),
     "frep_server_get_stats": (C.c_int, [_P, C.c_int, C.POINTER(ServerStats)]),
     "frep_batch_render_frames": (C.c_int, [_P, _P, C.c_uint32, _P, C.POINTER(LightsStruct), _P, _P, _P]),
     "frep_batch_set_tuning": (C.c_int, [_P, C.c_uint32, C.c_uint32]),

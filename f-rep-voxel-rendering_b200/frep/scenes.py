@@ -283,3 +283,17 @@ def batch_workload(n_scenes: int = 512, seed: int = 3, width: int = 512, height:
     for sc in out:
         sc.shape = Tape.from_dag(*sc.shape)
     return out
+
+
+def jitter_tape(wide: np.ndarray, rng, rel: float = 0.1):
+    """A new scene of the same structure: the wide tape `wide` with every
+    constant (centres, sizes, blend radii) scaled by U[1 - rel, 1 + rel].
+    Returns a compiled frep.Tape. Used to draw many distinct scenes of the
+    batching distribution without building their expressions again."""
+    from . import Tape
+    w = np.array(wide, dtype=np.uint64, copy=True)
+    is_const = (w & np.uint64(0xFF)) == np.uint64(0)
+    bits = (w[is_const] >> np.uint64(32)).astype(np.uint32)
+    vals = bits.view(np.float32) * rng.uniform(1.0 - rel, 1.0 + rel, bits.size).astype(np.float32)
+    w[is_const] = (w[is_const] & np.uint64(0xFFFFFFFF)) | (vals.view(np.uint32).astype(np.uint64) << np.uint64(32))
+    return Tape.from_wide(w)

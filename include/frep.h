@@ -91,6 +91,11 @@ frep_status frep_tape_compile(const frep_dag* dag, frep_tape** out);
 frep_status frep_tape_from_reference(const uint32_t* instrs, uint32_t n_instr, const float* consts,
                                      uint32_t n_consts, frep_tape** out);
 
+/* Accepts a tape in this library's wide encoding (frep_tape_get_instrs), e.g.
+ * one saved earlier or edited (new constants, same structure). No
+ * counterpart in the reference. */
+frep_status frep_tape_from_wide(const uint64_t* instrs, uint32_t n_instr, frep_tape** out);
+
 frep_status frep_tape_get_info(const frep_tape* tape, frep_tape_info* info);
 
 /* Wide instruction words (8 bytes each): op bits 0-7, out 16-31, inA 32-47,
@@ -431,6 +436,9 @@ frep_status frep_server_poll(frep_server* server, uint64_t request_id, frep_requ
  * (FREP_ERR_TIMEOUT). */
 frep_status frep_server_wait(frep_server* server, uint64_t request_id, uint32_t timeout_ms,
                              frep_request_status* status);
+/* Forgets a finished request (its status can no longer be polled). A
+ * long-running caller releases every request it has waited for. */
+frep_status frep_server_release(frep_server* server, uint64_t request_id);
 /* Waits until every submitted request is done or failed. */
 frep_status frep_server_drain(frep_server* server, uint32_t timeout_ms);
 /* Statistics; reset != 0 clears the latency record and throughput window. */

@@ -115,3 +115,31 @@ def test_reference_tape_import_roundtrip():
     bad[0] = (int(bad[0]) & 0xFFFFFF00) | 0x3F  # unknown opcode
     with pytest.raises(frep.FrepError):
         frep.Tape.from_reference(bad, g["ref_consts"])
+
+
+def test_wide_import_round_trip():
+    """frep_tape_from_wide accepts what frep_tape_get_instrs returns and
+    derives the same slot count, MIN/MAX count and time use."""
+    from frep import scenes
+    for expr in (scenes.random_csg(12, seed=8).shape, scenes.Morph(), scenes.TwistedTower(2)):
+        a = frep.Tape(expr)
+        b = frep.Tape.from_wide(a.wide())
+        np.testing.assert_array_equal(a.wide(), b.wide())
+        assert (b.n_slots, b.n_minmax, b.uses_time) == (a.n_slots, a.n_minmax, a.uses_time)
+        assert not b.fits_reference
+        pts = np.random.default_rng(0).uniform(-2, 2, (64, 4)).astype(np.float32)
+        np.testing.assert_array_equal(a.eval_points(pts), b.eval_points(pts))
+
+
+def test_wide_import_rejects_bad_tapes():
+    a = frep.Tape(frep.csg.X() * frep.csg.Y() + 1.0).wide()
+    bad_op = a.copy()
+    bad_op[0] = (bad_op[0] & ~np.uint64(0xFF)) | np.uint64(13)
+    not_slot0 = a[:-1] if len(a) > 1 else a
+    with pytest.raises(frep.FrepError):
+        frep.Tape.from_wide(bad_op)
+    with pytest.raises(frep.FrepError):
+        frep.Tape.from_wide(np.zeros(0, np.uint64))
+    if len(a) > 1 and ((int(a[-2]) >> 16) & 0xFFFF) != 0:
+        with pytest.raises(frep.FrepError):
+            frep.Tape.from_wide(not_slot0)

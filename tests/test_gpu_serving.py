@@ -150,6 +150,11 @@ def test_overflow_retry(ctx, world):
     st = srv.wait(srv.submit(sid, _cam(w, 2, 1), 0.0, W, H, buf), 120000)
     assert st.state == frep.REQ_DONE and st.retries > 0
     np.testing.assert_array_equal(buf.numpy(), w["expected"][(2, 1, 0.0)])
+    rid = srv.submit(sid, _cam(w, 2, 0), 0.0, W, H, _pinned())
+    srv.wait(rid, 60000)
+    srv.release(rid)
+    with pytest.raises(frep.FrepError):
+        srv.poll(rid)
     srv.close()
 
 
