@@ -52,7 +52,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=("batch", "large"), default="batch")
+    ap.add_argument("--workload", choices=("batch", "large", "stress"), default="batch")
+    ap.add_argument("--frames", type=int, default=30, help="stress: animation frames (T = frame / frames)")
     ap.add_argument("--scenes", type=int, default=512, help="batch: number of scenes")
     ap.add_argument("--plain-steps", type=int, default=2, help="batch: timed passes of the plain launch loop")
     ap.add_argument("--no-tune", action="store_true", help="batch: default branching, no autotuning")
@@ -62,11 +63,13 @@ def parse():
                     help="batch: seconds of the serving run after the batch measurements (0 = none)")
     ap.add_argument("--serve-rate", type=float, default=1000.0, help="batch: Poisson request rate, requests/s")
     ap.add_argument("--serve-budget-gb", type=int, default=120, help="batch: tree arena of the server, GB")
-    ap.add_argument("--grid", default="16,16,8",
-                    help="large: tree branching per level (profiling uses a smaller grid of the same scene)")
+    ap.add_argument("--grid", default=None,
+                    help="large / stress: tree branching per level (default 16,16,8 / 16,16,4,4)")
     ap.add_argument("--res", default=None, help="render resolution WxH (batch 512x512, large 1920x1080)")
     ap.add_argument("--pool-mb", type=int, default=3072, help="large: node + tape pool size of the tree, MB")
     args = ap.parse_args()
+    if args.grid is None:
+        args.grid = "16,16,4,4" if args.workload == "stress" else "16,16,8"
     args.grid_dims = tuple(int(v) for v in args.grid.split(","))
     if args.res is None:
         args.res = "512x512" if args.workload == "batch" else "1920x1080"
@@ -76,6 +79,9 @@ def parse():
         fine *= d
     if args.workload == "batch":
         args.workload_name = (f"batch_{args.scenes}scenes_4-1024prim_64-1024cube_{args.width}x{args.height}_shadow")
+    elif args.workload == "stress":
+        args.workload_name = (f"stress_twisted_gyroid_64spheres_{fine}cube_{args.width}x{args.height}_shadow_"
+                              f"{args.frames}frames")
     else:
         args.workload_name = f"random_csg_256prim_{fine}cube_{args.width}x{args.height}_shadow"
     return args
@@ -175,25 +181,35 @@ def measured_peaks():
     return {"hbm_gbs": 6650.0, "sm_max_mhz": 1965.0, "fallback": True}
 
 
-def make_scene(args):
+def make_scene(args, grid_dims=None):
     from frep import scenes
-    return scenes.random_csg(256, seed=2, grid_dims=args.grid_dims, width=args.width, height=args.height,
-                             shadows=True)
+    dims = grid_dims or args.grid_dims
+    if args.workload == "stress":
+        return scenes.stress_gyroid(grid_dims=dims, width=args.width, height=args.height)
+    return scenes.random_csg(256, seed=2, grid_dims=dims, width=args.width, height=args.height, shadows=True)
 
 
-def cpu_baseline(scene, threads: int):
+def frame_times(args):
+    """Tape time of each step: the stress animation sweeps T over [0, 1)."""
+    if args.workload == "stress":
+        return [f / args.frames for f in range(args.frames)]
+    return [0.0]
+
+
+def cpu_baseline(scene, threads: int, tape_time: float = 0.0):
     """The oracle (C++ restatement of the reference's shaders) on the host:
     one full voxelization + one full render, all host threads."""
     sys.path.insert(0, str(REPO / "oracle"))
     import oracle
     import frep
-    tape = frep.Tape(scene.shape)
+    tape = scene.shape if isinstance(scene.shape, frep.Tape) else frep.Tape(scene.shape)
     t0 = time.perf_counter()
     tree = oracle.OracleTree(tape.wide(), tape.n_slots, scene.grid_dims, scene.low_vertex, scene.world_size,
-                             rounding=1, threads=threads)
+                             tape_time=tape_time, rounding=1, threads=threads)
     t1 = time.perf_counter()
     lights = frep.Lights(shadow_mask=scene.shadow_mask)
-    tree.render(oracle.camera_vector(scene.camera, scene.width, scene.height), lights, threads=threads)
+    tree.render(oracle.camera_vector(scene.camera, scene.width, scene.height), lights, tape_time=tape_time,
+                threads=threads)
     t2 = time.perf_counter()
     return t2 - t0, t1 - t0, t2 - t1
 
@@ -202,11 +218,15 @@ def run_reference(args, world, rank):
     """--impl reference: the CPU path on the host cores, same metric/config."""
     if rank != 0:
         return
-    scene = make_scene(args)
+    # the stress scene at 4096^3 would take hours on the host: its sample is the
+    # same scene and frames on the first three levels of the grid (1024^3)
+    sample_dims = args.grid_dims[:3] if args.workload == "stress" else args.grid_dims
+    scene = make_scene(args, sample_dims)
     threads = os.cpu_count() or 1
+    tt = frame_times(args)
     if args.warmup > 0:
-        cpu_baseline(scene, threads)  # one warm-up scene (the oracle has no caches to warm)
-    times = [cpu_baseline(scene, threads)[0] for _ in range(args.steps)]
+        cpu_baseline(scene, threads, tt[0])  # one warm-up scene (the oracle has no caches to warm)
+    times = [cpu_baseline(scene, threads, tt[i % len(tt)])[0] for i in range(args.steps)]
     total = sum(times)
     value = args.steps / total
     line = {
@@ -217,8 +237,8 @@ def run_reference(args, world, rank):
         "config": {"workload": args.workload_name, "grid": list(args.grid_dims), "resolution": [args.width, args.height],
                    "shadow_rays": 1, "rounding": "outward"},
         "cpu_baseline": {"value": value, "unit": "scenes/s", "cores": threads, "kind": "port",
-                         "sample": f"{args.steps} full scenes (voxelize + 1080p render), oracle C++ port, "
-                                   f"{threads} threads"},
+                         "sample": f"{args.steps} scenes on grid {list(sample_dims)} (voxelize + "
+                                   f"{args.width}x{args.height} render), oracle C++ port, {threads} threads"},
         "e2e": {"value": value, "unit": "scenes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -231,10 +251,22 @@ def run_ours(args, world, rank, local):
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     scene = make_scene(args)
-    ctx = frep.Context(local, hbm_budget_bytes=48 << 30)
-    pool = args.pool_mb << 20
+    tt = frame_times(args)
+    if args.workload == "stress":
+        from frep.autotune import fit_pools
+        ctx = frep.Context(local, hbm_budget_bytes=args.budget_gb << 30)
+        tape = frep.Tape(scene.shape)
+        fits = fit_pools(ctx, [tape] * 4, [scene.grid_dims] * 4, scene.low_vertex, scene.world_size,
+                         tape_times=[tt[i * len(tt) // 4] for i in range(4)], start_bytes=8 << 30)
+        node_words = int(max(p.node_words for p in fits) * 1.15)
+        tape_words = int(max(p.tape_words for p in fits) * 1.15)
+        scene.shape = tape
+    else:
+        ctx = frep.Context(local, hbm_budget_bytes=48 << 30)
+        pool = args.pool_mb << 20
+        node_words, tape_words = pool // 4 // 4, pool * 3 // 4 // 8
     vs = frep.VoxelStorage(scene.grid_dims, scene.low_vertex, scene.world_size, rounding=frep.ROUND_OUTWARD,
-                           node_words=pool // 4 // 4, tape_words=pool * 3 // 4 // 8)
+                           node_words=node_words, tape_words=tape_words)
     vs.init(ctx, scene.shape)
     vox = frep.Voxelizer(ctx, vs)
     rt = frep.Raytracer(ctx, vs)
@@ -245,15 +277,18 @@ def run_ours(args, world, rank, local):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
     stream = torch.cuda.current_stream()
 
+    frame = [0]
+
     def step():
-        vox.voxelize(0.0, stream)
-        rt.trace(scene.camera, 0.0, W, H, out=(rgba, None), stream=stream)
+        t = tt[frame[0] % len(tt)]
+        frame[0] += 1
+        vox.voxelize(t, stream)
+        rt.trace(scene.camera, t, W, H, out=(rgba, None), stream=stream)
 
     for _ in range(args.warmup):
         step()
     info = vs.sync()
-    fp32_ops = vs.fp32_ops()
-    cell_instr = vs.work()
+    frame[0] = 0
     launches_per_step = 1 + 2 * vs.grid_levels + 1  # init + (work scan + level pass) per level + render
 
     # ---- device-resident timing (value) -------------------------------------
@@ -279,26 +314,29 @@ def run_ours(args, world, rank, local):
     reps = max(3, min(args.steps, 10))
     for _ in range(reps):
         flush.fill_(1)
-        vox.voxelize(0.0, stream)
+        vox.voxelize(tt[0], stream)
         rs, re_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         rs.record(stream)
-        rt.trace(scene.camera, 0.0, W, H, out=(rgba, None), stream=stream)
+        rt.trace(scene.camera, tt[0], W, H, out=(rgba, None), stream=stream)
         re_.record(stream)
         lt = vs.level_timings()
         torch.cuda.synchronize()
         level_ms = [a + b / reps for a, b in zip(level_ms, lt)]
         render_ms += rs.elapsed_time(re_) / reps
     vs.set_profiling(False)
+    fp32_ops = vs.fp32_ops()   # of the profiled voxelization (tape time tt[0])
+    cell_instr = vs.work()
 
     # ---- end to end through the public API with host buffers ---------------
     torch.cuda.synchronize()
     barrier(world)
     e2e_evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    for s, e in e2e_evs:
+    for i, (s, e) in enumerate(e2e_evs):
         flush.fill_(1)
+        t = tt[i % len(tt)]
         s.record(stream)
-        vox.voxelize(0.0, stream)   # host tape -> device (pinned staging + H2D)
-        rt.trace(scene.camera, 0.0, W, H, out=(rgba, None), stream=stream)
+        vox.voxelize(t, stream)   # host tape -> device (pinned staging + H2D)
+        rt.trace(scene.camera, t, W, H, out=(rgba, None), stream=stream)
         host_img.copy_(rgba, non_blocking=True)  # result -> host
         e.record(stream)
     torch.cuda.synchronize()
@@ -341,10 +379,11 @@ def run_ours(args, world, rank, local):
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        total, t_vox, t_ren = cpu_baseline(scene, threads)
+        sample_dims = args.grid_dims[:3] if args.workload == "stress" else args.grid_dims
+        total, t_vox, t_ren = cpu_baseline(make_scene(args, sample_dims), threads, tt[0])
         line["cpu_baseline"] = {"value": 1.0 / total, "unit": "scenes/s", "cores": threads, "kind": "port",
-                                "sample": f"1 full scene (voxelize {t_vox:.2f} s + 1080p render {t_ren:.2f} s), "
-                                          f"oracle C++ port, {threads} threads"}
+                                "sample": f"1 scene on grid {list(sample_dims)} (voxelize {t_vox:.2f} s + "
+                                          f"{W}x{H} render {t_ren:.2f} s), oracle C++ port, {threads} threads"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     vs.cleanup()
@@ -553,6 +592,7 @@ def run_ours_batch(args, world, rank, local):
     # ---- batched, device-resident (value) ------------------------------------
     barrier(world)
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    torch.cuda.nvtx.range_push("batched_steps")  # lets a profiler select the timed launches
     with ClockSampler(local) as clocks:
         for s, e in evs:
             flush.fill_(1)
@@ -560,6 +600,7 @@ def run_ours_batch(args, world, rank, local):
             step()
             e.record(stream)
         torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
     barrier(world)
     t_ms = max_over_ranks(world, sum(s.elapsed_time(e) for s, e in evs))
     value = world * n * args.steps / (t_ms / 1e3)
@@ -582,12 +623,14 @@ def run_ours_batch(args, world, rank, local):
     barrier(world)
     pevs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
             for _ in range(args.plain_steps)]
+    torch.cuda.nvtx.range_push("plain_passes")
     for s, e in pevs:
         flush.fill_(1)
         s.record(stream)
         plain_pass()
         e.record(stream)
     torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
     barrier(world)
     p_ms = max_over_ranks(world, sum(s.elapsed_time(e) for s, e in pevs))
     plain_value = world * n * args.plain_steps / (p_ms / 1e3)

@@ -670,6 +670,40 @@ frep_status frep_render(frep_ctx* ctx, const frep_tree* tree, const frep_camera*
     return FREP_OK;
 }
 
+frep_status frep_resolve_layers(const uint8_t* layers, uint32_t n_layers, uint32_t width, uint32_t height,
+                                uint8_t* out, void* stream_ptr) {
+    if (!layers || !out || n_layers == 0) return fail(FREP_ERR_INVALID_ARG, "frep_resolve_layers: bad arguments");
+    if (((uintptr_t)layers & 3) || ((uintptr_t)out & 3))
+        return fail(FREP_ERR_INVALID_ARG, "frep_resolve_layers: buffers must be 4-byte aligned");
+    if (n_layers > (1u << 22)) return fail(FREP_ERR_INVALID_ARG, "frep_resolve_layers: too many layers");
+    cudaError_t e = frep::launch_resolve_layers(layers, n_layers, width * height, out, (cudaStream_t)stream_ptr);
+    if (e != cudaSuccess) return cuda_fail(e, "resolve_layers_kernel");
+    return FREP_OK;
+}
+
+frep_status frep_render_temporal(frep_ctx* ctx, const frep_tree* tree, const frep_camera* cam,
+                                 const frep_lights* lights, float tape_time, uint32_t n_samples, uint8_t* layers,
+                                 uint8_t* rgba8, void* stream_ptr) {
+    if (!ctx || !tree || !cam || !layers || !rgba8 || n_samples == 0)
+        return fail(FREP_ERR_INVALID_ARG, "frep_render_temporal: bad arguments");
+    FREP_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t s = (cudaStream_t)stream_ptr;
+    const size_t frame = (size_t)cam->width * cam->height * 4;
+    for (uint32_t i = 0; i < n_samples; i++) {
+        frep_camera c = *cam;
+        c.jitter = 1;
+        c.jitter_seed = cam->jitter_seed + (float)i;
+        frep_image img{layers + i * frame, nullptr};
+        frep::RenderArgs a{};
+        frep_status st = frep::detail::fill_render_args(tree, &c, lights, tape_time, &img, &a);
+        if (st != FREP_OK) return st;
+        cudaError_t e = frep::launch_render(a, s);
+        if (e == cudaErrorInvalidValue) return fail(FREP_ERR_UNSUPPORTED, "frep_render_temporal: more than 1024 slots");
+        if (e != cudaSuccess) return cuda_fail(e, "render_kernel");
+    }
+    return frep_resolve_layers(layers, n_samples, cam->width, cam->height, rgba8, stream_ptr);
+}
+
 }  // extern "C"
 
 // ---- voxelization without allocation -------------------------------------------

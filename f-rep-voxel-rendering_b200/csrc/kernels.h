@@ -108,6 +108,10 @@ struct RenderArgs {
 };
 
 cudaError_t launch_render(const RenderArgs& a, cudaStream_t stream);
+// out[p] = rounded mean of the n layers' rgb at pixel p, alpha 255 (layers:
+// n consecutive rgba8 images of `pixels` pixels).
+cudaError_t launch_resolve_layers(const uint8_t* layers, uint32_t n, uint32_t pixels, uint8_t* out,
+                                  cudaStream_t stream);
 // Renders n frames in one launch: args is a device array of n RenderArgs,
 // max_w / max_h bound every frame's size.
 cudaError_t launch_render_batch(const RenderArgs* args, uint32_t n, uint32_t max_w, uint32_t max_h,

@@ -8,6 +8,7 @@
 //
 // Blocks are 8 x 8 pixel tiles, so that neighbouring rays (which walk the same
 // nodes and usually share the hit node's tape) sit in the same warp.
+#include <algorithm>
 #include "device_common.cuh"
 #include "kernels.h"
 
@@ -305,7 +306,36 @@ __global__ void __launch_bounds__(64) render_batch_kernel(const RenderArgs* args
     render_pixel<NS>(A, x, y);
 }
 
+// Temporal resolve (renderer/triangle.frag:14-23): the pixel is the mean of
+// the layers' rgb with alpha 1. The mean is exact (integer sum) and rounded
+// to nearest, ties up: (2 sum + n) / 2n; the reference leaves the float ->
+// unorm rounding to the driver. One thread per pixel, 4 bytes each.
+__global__ void resolve_layers_kernel(const uchar4* __restrict__ layers, uint32_t n, uint32_t pixels,
+                                      uchar4* __restrict__ out) {
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < pixels; p += gridDim.x * blockDim.x) {
+        uint32_t r = 0, g = 0, b = 0;
+        for (uint32_t i = 0; i < n; i++) {
+            const uchar4 v = layers[(size_t)i * pixels + p];
+            r += v.x;
+            g += v.y;
+            b += v.z;
+        }
+        const uint32_t den = 2 * n;
+        out[p] = make_uchar4((uint8_t)((2 * r + n) / den), (uint8_t)((2 * g + n) / den), (uint8_t)((2 * b + n) / den),
+                             255);
+    }
+}
+
 }  // namespace dev
+
+cudaError_t launch_resolve_layers(const uint8_t* layers, uint32_t n, uint32_t pixels, uint8_t* out,
+                                  cudaStream_t stream) {
+    if (n == 0 || pixels == 0) return cudaSuccess;
+    const uint32_t blocks = (uint32_t)std::min<uint64_t>((pixels + 255) / 256, 148ull * 16);
+    dev::resolve_layers_kernel<<<blocks, 256, 0, stream>>>(reinterpret_cast<const uchar4*>(layers), n, pixels,
+                                                            reinterpret_cast<uchar4*>(out));
+    return cudaGetLastError();
+}
 
 cudaError_t launch_render(const RenderArgs& a, cudaStream_t stream) {
     const dim3 grid((a.width + 7) / 8, (a.height + 7) / 8);

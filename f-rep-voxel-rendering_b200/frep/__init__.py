@@ -392,6 +392,31 @@ class Raytracer:
                                     float(tape_time), C.byref(img), _stream_ptr(stream)))
         return rgba, hit_buf
 
+    def trace_temporal(self, camera: Camera, tape_time: float = 0.0, width: int = 256, height: int = 256,
+                       n_samples: int = 4, stream=None):
+        """n_samples jittered frames (seeds camera.jitter_seed + i) averaged
+        into one rgba8 image (the reference's temporal accumulation over an
+        image array, renderer/triangle.frag). Returns (image, layers)."""
+        import torch
+        dev = torch.device("cuda", self.ctx.device)
+        layers = torch.empty((n_samples, height, width, 4), dtype=torch.uint8, device=dev)
+        rgba = torch.empty((height, width, 4), dtype=torch.uint8, device=dev)
+        cam = camera.struct(width, height)
+        lights = self.lights.struct()
+        L.check(L.lib().frep_render_temporal(self.ctx._h, self.voxels.tree, C.byref(cam), C.byref(lights),
+                                             float(tape_time), n_samples, layers.data_ptr(), rgba.data_ptr(),
+                                             _stream_ptr(stream)))
+        return rgba, layers
+
+
+def resolve_layers(layers, stream=None):
+    """Mean of rgba8 layers (device tensor (n, H, W, 4)) -> (H, W, 4)."""
+    import torch
+    n, h, w, _ = layers.shape
+    out = torch.empty((h, w, 4), dtype=torch.uint8, device=layers.device)
+    L.check(L.lib().frep_resolve_layers(layers.data_ptr(), n, w, h, out.data_ptr(), _stream_ptr(stream)))
+    return out
+
 
 class Batch:
     """Many scenes voxelized and rendered together (frep_batch): one launch per

@@ -136,6 +136,9 @@ _SIGS = {
     "frep_batch_set_profiling": (C.c_int, [_P, C.c_int]),
     "frep_batch_set_trees": (C.c_int, [_P, _P, C.c_uint32]),
     "frep_tape_from_wide": (C.c_int, [_P, C.c_uint32, C.POINTER(_P)]),
+    "frep_resolve_layers": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_uint32, _P, _P]),
+    "frep_render_temporal": (C.c_int, [_P, _P, C.POINTER(CameraStruct), C.POINTER(LightsStruct), C.c_float,
+                                       C.c_uint32, _P, _P, _P]),
     "frep_server_create": (C.c_int, [_P, C.POINTER(ServerConfig), C.POINTER(LightsStruct), C.POINTER(_P)]),
     "frep_server_destroy": (None, [_P]),
     "frep_server_add_scene": (C.c_int, [_P, _P, C.POINTER(Grid), C.POINTER(VoxelizeOpts), C.POINTER(C.c_uint64)]),

@@ -297,3 +297,41 @@ def jitter_tape(wide: np.ndarray, rng, rel: float = 0.1):
     vals = bits.view(np.float32) * rng.uniform(1.0 - rel, 1.0 + rel, bits.size).astype(np.float32)
     w[is_const] = (w[is_const] & np.uint64(0xFFFFFFFF)) | (vals.view(np.uint32).astype(np.uint64) << np.uint64(32))
     return Tape.from_wide(w)
+
+
+# ---- stress workload ---------------------------------------------------------------
+
+def stress_gyroid(n_spheres: int = 64, seed: int = 5, period: float = 0.05, thickness: float = 0.3,
+                  grid_dims=(16, 16, 4, 4), width: int = 1920, height: int = 1080) -> Scene:
+    """A gyroid lattice sin(kx)cos(ky) + sin(ky)cos(kz) + sin(kz)cos(kx),
+    k = 2 pi / period, as a sheet |g| - thickness, domain-warped by a z-twist
+    (x, y rotated about z by 2 pi T z: T in [0, 1) sweeps the twist through
+    one full turn per unit of z), intersected (max) with the box [-1, 1]^3 and
+    smooth-unioned (k = 0.05) with n_spheres random spheres (centres U[-1.2,
+    1.2]^3, radii U[0.05, 0.2]). Default grid {16, 16, 4, 4} = 4096^3 over
+    [-1.3, 1.3]^3; perspective camera at 60 degrees with a shadow ray per
+    hit. Animated: re-voxelize per frame at T = frame / frames."""
+    from . import Camera
+    rng = np.random.default_rng(seed)
+    k = 2.0 * np.pi / period
+    ang = f32(2.0 * np.pi) * T() * Z()
+    c, s = Cos(ang), Sin(ang)
+    xt = c * X() - s * Y()
+    yt = s * X() + c * Y()
+    kx, ky, kz = f32(k) * xt, f32(k) * yt, f32(k) * Z()
+    g = Sin(kx) * Cos(ky) + Sin(ky) * Cos(kz) + Sin(kz) * Cos(kx)
+    sheet = (Abs(g) - f32(thickness)) / f32(k)
+    box = Max(Max(Abs(X()), Abs(Y())), Abs(Z())) - 1.0
+    shape = Max(sheet, box)
+    centers = rng.uniform(-1.2, 1.2, (n_spheres, 3))
+    radii = rng.uniform(0.05, 0.2, n_spheres)
+    balls = [Sqrt(Dist2(Axes(), Vector3(*map(float, cc)))) - float(r) for cc, r in zip(centers, radii)]
+    while len(balls) > 1:  # balanced smooth-union tree
+        nxt = [smooth_min(balls[i], balls[i + 1], 0.05) for i in range(0, len(balls) - 1, 2)]
+        if len(balls) % 2:
+            nxt.append(balls[-1])
+        balls = nxt
+    shape = smooth_min(shape, balls[0], 0.05)
+    cam = Camera(position=(2.4, 1.7, 3.0), forward=(-2.4, -1.7, -3.0), initial_up=(0.0, 1.0, 0.0), fov_deg=60.0)
+    return Scene("stress_gyroid", shape, list(grid_dims), (-1.3, -1.3, -1.3), 2.6, cam, width, height,
+                 shadow_mask=1, meta={"n_spheres": n_spheres, "seed": seed, "period": period})

@@ -296,6 +296,22 @@ frep_status frep_render(frep_ctx* ctx, const frep_tree* tree, const frep_camera*
                         const frep_lights* lights, float tape_time, const frep_image* out,
                         void* stream);
 
+/* Temporal multi-sample resolve (renderer/triangle.frag:14-23 with
+ * render_target.cpp:36-56 and raytracer.cpp:163-164): the reference renders
+ * one jittered frame per display frame into layer (frame % count) of an
+ * image array and the fragment shader averages the layers. Here:
+ *   frep_resolve_layers — out = mean of n_layers consecutive rgba8 images
+ *     (device memory, width*height*4 bytes each): rgb rounded to nearest
+ *     (ties up) from the exact sum, alpha 255;
+ *   frep_render_temporal — renders n_samples jittered frames of the tree into
+ *     `layers` (device, n_samples*width*height*4 bytes; sample i uses jitter
+ *     seed camera->jitter_seed + i) and resolves them into rgba8. */
+frep_status frep_resolve_layers(const uint8_t* layers, uint32_t n_layers, uint32_t width, uint32_t height,
+                                uint8_t* out, void* stream);
+frep_status frep_render_temporal(frep_ctx* ctx, const frep_tree* tree, const frep_camera* camera,
+                                 const frep_lights* lights, float tape_time, uint32_t n_samples, uint8_t* layers,
+                                 uint8_t* rgba8, void* stream);
+
 /* ---------------------------------------------------------------------------
  * Batching: many scenes per launch
  * ------------------------------------------------------------------------- */

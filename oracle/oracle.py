@@ -344,3 +344,16 @@ def hit_cells(hits: np.ndarray, dims, node_offset, node_size, nodes) -> np.ndarr
         out[m, 2] = nodes[rec + 2].astype(np.int64) * dim + (c // dim) % dim
         out[m, 3] = nodes[rec + 3].astype(np.int64) * dim + c % dim
     return out
+
+
+def resolve_layers(layers: np.ndarray) -> np.ndarray:
+    """Temporal resolve (renderer/triangle.frag:14-23): the mean of the layers'
+    rgb with alpha 1. layers: (n, H, W, 4) uint8. The mean is taken exactly
+    and rounded to nearest, ties up, as the library defines it (the
+    reference's float -> unorm rounding is the driver's)."""
+    n = layers.shape[0]
+    s = layers[..., :3].astype(np.int64).sum(axis=0)
+    out = np.empty(layers.shape[1:], np.uint8)
+    out[..., :3] = (2 * s + n) // (2 * n)
+    out[..., 3] = 255
+    return out

@@ -129,3 +129,20 @@ def test_pool_overflow_reports_capacity_error(ctx):
     with pytest.raises(frep.FrepError) as e:
         vs2.sync()
     assert e.value.status == frep._lib.ERR_CAPACITY
+
+
+@pytest.mark.parametrize("rounding,t", [(1, 0.37), (0, 0.81)])
+def test_stress_gyroid_small(ctx, rounding, t):
+    """The stress scene (twisted gyroid lattice with SIN/COS in interval
+    arithmetic, smooth-unioned with 64 spheres) on a reduced grid at a tape
+    time T > 0: trees, hits and pixels as the oracle's."""
+    sc = scenes.stress_gyroid(grid_dims=(8, 8), width=120, height=72)
+    vs = device_tree(ctx, sc, rounding=rounding, tape_time=t)
+    exp = vs.export()
+    orc = oracle_tree(sc, vs.tape, rounding=rounding, tape_time=t)
+    assert compare_trees(exp, orc) == []
+    lights = frep.Lights(shadow_mask=1)
+    d_rgba, d_hits, o_rgba, o_hits = render_both(ctx, vs, orc, sc, lights, tape_time=t)
+    assert compare_hits(d_hits, o_hits, exp, orc) == []
+    np.testing.assert_array_equal(d_rgba, o_rgba)
+    assert sum(exp.node_count) > 100
