@@ -172,17 +172,19 @@ __device__ __forceinline__ LevelTree load_tree(TreeHeader* H, uint32_t L, bool p
 }
 
 // Stages the prefetched chunk `pre` (lane l of group q holds instruction
-// q*32 + l of the chunk), decoded, into stage[]. FWD: mark operands forwarded
-// from the previous instruction (never for the first instruction of a chunk).
-// Entries past the tape's end decode to a CONST that is never executed;
-// stage[STAGE] is the same kind of entry, read (not executed) one past a full
-// chunk.
+// q*32 + l of the chunk), decoded, into stage[]: only the 32-entry groups that
+// hold the chunk's m instructions (short leaf tapes need one or two). FWD:
+// mark operands forwarded from the previous instruction (never for the first
+// instruction of a chunk). Entries past the tape's end decode to a CONST that
+// is never executed; the interpreter reads one entry past the last one (not
+// executing it), which may be left from an earlier tape or be stage[STAGE].
 template <bool FWD>
 __device__ __forceinline__ void stage_chunk(uint4* stage, const uint64_t (&pre)[STAGE / 32], uint32_t row_bytes,
-                                            uint32_t lane) {
+                                            uint32_t lane, uint32_t m) {
     uint32_t prev_group_last = 0xFFFFFFFFu;
 #pragma unroll
     for (int q = 0; q < (int)(STAGE / 32); q++) {
+        if ((uint32_t)q * 32u >= m) break;
         uint32_t prev = 0xFFFFFFFFu;
         if constexpr (FWD) {
             const uint32_t out = w_out(pre[q]);
@@ -240,7 +242,10 @@ __device__ __forceinline__ float2 iv_exec(const uint4 d, uint32_t lane_base, uin
 // and in shared memory they would cap the resident warps for every tree of a
 // batch at what its longest tape allows.
 template <int ROUND, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32)
+// At least 20 warps per SM (5 blocks of 4 or 20 of 1): caps registers at 96,
+// which measured ~11 % faster than the unbounded 128 (more warps hide the
+// shared-memory and branch latencies of the interpreter); a cap of 80 spills.
+__global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 5 : 20)
 interval_level_kernel(LevelLaunch p) {
     extern __shared__ __align__(16) unsigned char smem[];
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -324,7 +329,7 @@ interval_level_kernel(LevelLaunch p) {
             for (uint32_t base = 0; base < n; base += STAGE) {
                 const uint32_t m = min(STAGE, n - base);
                 __syncwarp();
-                stage_chunk<false>(stage, pre, 8, lane);
+                stage_chunk<false>(stage, pre, 8, lane, m);
                 prefetch_chunk(pre, tape, base + STAGE, n, lane);
                 __syncwarp();
                 // The decode word of j+1 is read one instruction early.
@@ -655,7 +660,7 @@ point_level_kernel(LevelLaunch p) {
                 const uint32_t m = min(STAGE, n - base);
                 if (!resident) {
                     __syncwarp();
-                    stage_chunk<true>(stage, pre, ROW, lane);
+                    stage_chunk<true>(stage, pre, ROW, lane, m);
                     prefetch_chunk(pre, tape, base + STAGE, n, lane);
                     __syncwarp();
                 }
