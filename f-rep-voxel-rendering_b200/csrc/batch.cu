@@ -224,8 +224,19 @@ frep_status prepare_voxelize(frep_batch* b, const frep_tape* const* tapes, TapeS
     if (r == FREP_OK)
         r = ensure_keep(b, (uint64_t)std::max(b->plan4.blocks * b->plan4.warps_per_block,
                                               b->plan2.blocks * b->plan2.warps_per_block) *
-                               frep::warp_scratch(st->longest, st->mm).stride);
+                               frep::warp_scratch(st->longest, st->mm, (uint32_t)b->plan4.interval_ki).stride);
     return r;
+}
+
+// Cells per lane of the level-0 interval pass. Level 0 is one node per tree;
+// with few trees two cells per lane would leave too few items to fill the
+// GPU, so it keeps one there.
+int level0_cells(const frep_batch* b) {
+    uint64_t items0 = 0;
+    for (const frep_tree* t : b->trees)
+        if (t->grid.levels > 1) items0 += (uint64_t)t->grid.dims[0] * t->grid.dims[0] * t->grid.dims[0] / 32;
+    const uint64_t warps = (uint64_t)b->plan4.blocks * b->plan4.warps_per_block;
+    return items0 < 4 * warps ? 1 : b->plan4.interval_ki;
 }
 
 // Enqueues the voxelization of every tree of the set: root copy + header
@@ -249,15 +260,17 @@ frep_status enqueue_voxelize(frep_batch* b, const uint8_t* d_area, const TapeSta
     a.cursor = b->d_cursor;
     a.n_trees = n;
     a.keep_scratch = b->keep;
-    const frep::WarpScratch ws = frep::warp_scratch(st.longest, st.mm);
+    const frep::WarpScratch ws = frep::warp_scratch(st.longest, st.mm, (uint32_t)b->plan4.interval_ki);
     a.keep_stride = ws.stride;
     a.mm_ofs = ws.mm_ofs;
     a.n_slots = st.slots;
     a.mm_cap = st.mm;
+    const int ki0 = level0_cells(b);
     for (uint32_t l = 0; l < st.max_levels; l++) {
         a.level = l;
-        e = frep::launch_level_scan(a, false, 4, s);
-        if (e == cudaSuccess) e = frep::launch_level(a, b->plan4, b->rounding, false, s);
+        const int ki = l == 0 ? ki0 : b->plan4.interval_ki;
+        e = frep::launch_level_scan(a, false, ki, s);
+        if (e == cudaSuccess) e = frep::launch_level(a, b->plan4, b->rounding, false, s, ki);
         if (e != cudaSuccess) return cuda_fail(e, "batched interval pass");
         if (prof) FREP_CUDA(cudaEventRecord(b->ev[2 + 3 * l], s));
         if (st.any_k4) {
@@ -510,7 +523,8 @@ frep_status frep_batch_run(frep_batch* b, const frep_tape* const* tapes, const f
     std::vector<uint64_t> key = {L.total, n, st.slots, st.mm, st.longest, st.max_levels, st.any_k4, st.any_k2,
                                  fd.max_w, fd.max_h, fd.max_slots, (uint64_t)b->plan4.blocks,
                                  (uint64_t)b->plan4.warps_per_block, (uint64_t)b->plan4.point_warps_per_block,
-                                 (uint64_t)b->plan2.point_warps_per_block, (uint64_t)(uintptr_t)b->keep,
+                                 (uint64_t)b->plan2.point_warps_per_block, (uint64_t)b->plan4.interval_ki,
+                                 (uint64_t)level0_cells(b), (uint64_t)(uintptr_t)b->keep,
                                  (uint64_t)(uintptr_t)b->d_prefix, (uint64_t)(uintptr_t)A.d};
     for (uint32_t i = 0; i < n; i++) key.push_back(L.root_ofs[i]);
     if (!A.graph || key != A.graph_key) {

@@ -390,9 +390,12 @@ frep_status enqueue_tree_levels(frep_tree* tree, const frep_tape* tape, float ta
     for (uint32_t l = 0; l < g.levels; l++) {
         const bool point = l == g.levels - 1;
         a.level = l;
-        e = frep::launch_level_scan(a, point, plan.point_k, stream);
+        // Level 0 of one tree is one node: too few items to fill the GPU with
+        // two cells per lane, so it keeps one (latency, not issue, bounds it).
+        const int ki = l == 0 ? 1 : plan.interval_ki;
+        e = frep::launch_level_scan(a, point, point ? plan.point_k : ki, stream);
         if (e != cudaSuccess) return cuda_fail(e, "level_scan_kernel");
-        e = frep::launch_level(a, plan, (int)tree->opts.rounding, point, stream);
+        e = frep::launch_level(a, plan, (int)tree->opts.rounding, point, stream, ki);
         if (e != cudaSuccess) return cuda_fail(e, "level kernel");
         if (tree->profile) FREP_CUDA(cudaEventRecord(tree->ev[l + 1], stream));
     }
@@ -419,7 +422,7 @@ frep_status frep_voxelize(frep_ctx* ctx, frep_tree* tree, const frep_tape* tape,
     frep_status pst = ensure_plan(tree, tape, "frep_voxelize");
     if (pst != FREP_OK) return pst;
     // Per-warp scratch: a keep mask per instruction, a choice-mask pair per MIN/MAX.
-    const frep::WarpScratch ws = frep::warp_scratch(n, tape->ct.n_minmax);
+    const frep::WarpScratch ws = frep::warp_scratch(n, tape->ct.n_minmax, (uint32_t)tree->plan.interval_ki);
     const uint64_t keep_words = (uint64_t)tree->plan.blocks * tree->plan.warps_per_block * ws.stride;
     if (keep_words > tree->keep_words) {
         if (tree->keep) {
@@ -767,7 +770,7 @@ extern "C" frep_status frep_voxelize_static_scratch(frep_ctx* ctx, frep_tree* tr
     // Each resident warp owns ws.stride words of the array (a keep mask per
     // instruction, a choice-mask pair per MIN/MAX); launch only as many blocks
     // as fit, and refuse tapes too long for even one block.
-    const frep::WarpScratch ws = frep::warp_scratch(n, tape->ct.n_minmax);
+    const frep::WarpScratch ws = frep::warp_scratch(n, tape->ct.n_minmax, (uint32_t)tree->plan.interval_ki);
     const uint64_t per_block = (uint64_t)tree->plan.warps_per_block * ws.stride;
     if (per_block > kStaticScratchWords)
         return fail(FREP_ERR_UNSUPPORTED,

@@ -32,17 +32,22 @@ struct WarpScratch {
     uint32_t stride;  // words per warp
     uint32_t mm_ofs;  // where the choice masks start
 };
-inline WarpScratch warp_scratch(uint32_t longest, uint32_t mm_cap) {
-    const uint32_t k = ((longest ? longest : 1u) + 31u) / 32u * 32u;
-    const uint32_t m = (2u * (mm_cap ? mm_cap : 1u) + 31u) / 32u * 32u;
+// ki: cells per lane of the interval pass (a keep mask and a choice-mask pair
+// per group of 32 cells).
+inline WarpScratch warp_scratch(uint32_t longest, uint32_t mm_cap, uint32_t ki) {
+    const uint32_t k = (ki * (longest ? longest : 1u) + 31u) / 32u * 32u;
+    const uint32_t m = (2u * ki * (mm_cap ? mm_cap : 1u) + 31u) / 32u * 32u;
     return WarpScratch{k + m, k};
 }
+
+
 
 // Launch geometry of the level passes for one (slot count, MIN/MAX count).
 struct LevelPlan {
     int warps_per_block;
     int blocks;                        // persistent grid
     uint32_t smem_per_warp;
+    int interval_ki;                   // cells per lane in the interval passes (1 or 2)
     int point_k;                       // cells per lane in the point pass
     int point_warps_per_block;
     int point_blocks;
@@ -53,8 +58,9 @@ struct LevelPlan {
 int point_k_for(uint32_t dim);
 // interval_warps / point_warps: warps (tapes) per block, 0 = chosen from the
 // shared memory a warp needs, 1 or 4 = that many where shared memory allows.
+// interval_ki: cells per lane of the interval passes, 1 or 2 (0 = default).
 cudaError_t plan_levels(uint32_t n_slots, uint32_t mm_cap, int point_k, int rounding, LevelPlan* plan,
-                        int interval_warps = 0, int point_warps = 0);
+                        int interval_warps = 0, int point_warps = 0, int interval_ki = 0);
 
 // Resets the headers of n trees (tape time from `tape_times`, or `tape_time`
 // when it is null) and writes their root nodes. Each tree's root tape must
@@ -73,7 +79,8 @@ cudaError_t launch_tree_init_staged(dev::TreeHeader* const* trees, uint32_t n, c
 cudaError_t launch_gather_usage(dev::TreeHeader* const* trees, uint32_t n, unsigned long long* out,
                                 cudaStream_t stream);
 cudaError_t launch_level_scan(const LevelLaunch& a, bool point, int point_k, cudaStream_t stream);
-cudaError_t launch_level(const LevelLaunch& a, const LevelPlan& plan, int rounding, bool point, cudaStream_t stream);
+cudaError_t launch_level(const LevelLaunch& a, const LevelPlan& plan, int rounding, bool point,
+                         cudaStream_t stream, int interval_ki = 0);
 
 // Op-weighted work of every node of `level` (interval or point weights),
 // added to the header's fp32_ops[level].

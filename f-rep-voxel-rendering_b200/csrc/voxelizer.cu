@@ -204,55 +204,108 @@ __device__ __forceinline__ void prefetch_chunk(uint64_t (&pre)[STAGE / 32], cons
     }
 }
 
-// One interval instruction (any opcode but CONST), dispatched by frequency.
-// MIN/MAX also record each lane's choice (interval.comp:140-155) as two
-// ballots: bit 0 = the first operand may be the result, bit 1 = the second.
-template <int ROUND>
-__device__ __forceinline__ float2 iv_exec(const uint4 d, uint32_t lane_base, uint32_t lane, uint2* mmb,
-                                          uint32_t& mm, uint32_t mm_cap) {
+// KI intervals per lane (one per cell): slot rows of 8 * KI bytes per lane.
+template <int KI>
+struct IVK {
+    float2 v[KI];
+};
+template <int KI>
+__device__ __forceinline__ IVK<KI> lds_iv(uint32_t a) {
+    IVK<KI> r;
+    if constexpr (KI == 1) {
+        r.v[0] = lds_f2(a);
+    } else {
+        const float4 t = lds_f4(a);
+        r.v[0] = make_float2(t.x, t.y);
+        r.v[1] = make_float2(t.z, t.w);
+    }
+    return r;
+}
+template <int KI>
+__device__ __forceinline__ void sts_iv(uint32_t a, const IVK<KI>& r) {
+    if constexpr (KI == 1) sts_f2(a, r.v[0]);
+    else sts_f4(a, make_float4(r.v[0].x, r.v[0].y, r.v[1].x, r.v[1].y));
+}
+
+// One interval instruction (any opcode but CONST) on KI cells per lane,
+// dispatched by frequency. MIN/MAX also record each cell's choice
+// (interval.comp:140-155) as two ballots per group of 32 cells: bit 0 = the
+// first operand may be the result, bit 1 = the second.
+template <int ROUND, int KI>
+__device__ __forceinline__ IVK<KI> iv_exec(const uint4 d, uint32_t lane_base, uint32_t lane, uint2* mmb,
+                                           uint32_t& mm, uint32_t mm_cap) {
     const uint32_t op = d.x;
-    const float2 a = lds_f2(lane_base + d.y);
-    const float2 b = lds_f2(lane_base + d.z);
-    if (op == OP_SUB)
-        return ROUND ? make_float2(__fsub_rd(a.x, b.y), __fsub_ru(a.y, b.x))
-                     : make_float2(__fsub_rn(a.x, b.y), __fsub_rn(a.y, b.x));
-    if (op == OP_MUL) return iv_mul<ROUND>(a, b);
-    if (op == OP_ADD)
-        return ROUND ? make_float2(__fadd_rd(a.x, b.x), __fadd_ru(a.y, b.y))
-                     : make_float2(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y));
+    const IVK<KI> a = lds_iv<KI>(lane_base + d.y);
+    const IVK<KI> b = lds_iv<KI>(lane_base + d.z);
+    IVK<KI> r;
+    if (op == OP_SUB) {
+#pragma unroll
+        for (int h = 0; h < KI; h++)
+            r.v[h] = ROUND ? make_float2(__fsub_rd(a.v[h].x, b.v[h].y), __fsub_ru(a.v[h].y, b.v[h].x))
+                           : make_float2(__fsub_rn(a.v[h].x, b.v[h].y), __fsub_rn(a.v[h].y, b.v[h].x));
+        return r;
+    }
+    if (op == OP_MUL) {
+#pragma unroll
+        for (int h = 0; h < KI; h++) r.v[h] = iv_mul<ROUND>(a.v[h], b.v[h]);
+        return r;
+    }
+    if (op == OP_ADD) {
+#pragma unroll
+        for (int h = 0; h < KI; h++)
+            r.v[h] = ROUND ? make_float2(__fadd_rd(a.v[h].x, b.v[h].x), __fadd_ru(a.v[h].y, b.v[h].y))
+                           : make_float2(__fadd_rn(a.v[h].x, b.v[h].x), __fadd_rn(a.v[h].y, b.v[h].y));
+        return r;
+    }
     if (op == OP_MIN || op == OP_MAX) {
         const bool mx = op == OP_MAX;
-        const bool first_low = a.y < b.x, second_low = b.y < a.x;
-        uint32_t c = first_low ? (mx ? MM_SECOND : MM_FIRST) : (second_low ? (mx ? MM_FIRST : MM_SECOND) : MM_BOTH);
-        const uint32_t b0 = __ballot_sync(0xFFFFFFFFu, c & 1u);
-        const uint32_t b1 = __ballot_sync(0xFFFFFFFFu, c & 2u);
-        if (lane == 0 && mm < mm_cap) mmb[mm] = make_uint2(b0, b1);
+        uint2 ch[KI];
+#pragma unroll
+        for (int h = 0; h < KI; h++) {
+            const bool first_low = a.v[h].y < b.v[h].x, second_low = b.v[h].y < a.v[h].x;
+            const uint32_t c =
+                first_low ? (mx ? MM_SECOND : MM_FIRST) : (second_low ? (mx ? MM_FIRST : MM_SECOND) : MM_BOTH);
+            ch[h] = make_uint2(__ballot_sync(0xFFFFFFFFu, c & 1u), __ballot_sync(0xFFFFFFFFu, c & 2u));
+            r.v[h] = mx ? make_float2(max_sel(a.v[h].x, b.v[h].x), max_sel(a.v[h].y, b.v[h].y))
+                        : make_float2(min_sel(a.v[h].x, b.v[h].x), min_sel(a.v[h].y, b.v[h].y));
+        }
+        if (lane == 0 && mm < mm_cap) {
+            if constexpr (KI == 1) mmb[mm] = ch[0];
+            else reinterpret_cast<uint4*>(mmb)[mm] = make_uint4(ch[0].x, ch[0].y, ch[1].x, ch[1].y);
+        }
         mm++;
-        return mx ? make_float2(max_sel(a.x, b.x), max_sel(a.y, b.y))
-                  : make_float2(min_sel(a.x, b.x), min_sel(a.y, b.y));
+        return r;
     }
-    return iv_apply<ROUND>(op, 0ull, a, b);
+#pragma unroll
+    for (int h = 0; h < KI; h++) r.v[h] = iv_apply<ROUND>(op, 0ull, a.v[h], b.v[h]);
+    return r;
 }
 
 // ---- interval level pass -------------------------------------------------------
 //
-// Per-warp shared memory: slots [n_slots][32] float2 | stage [STAGE] uint4 |
-// live [n_slots] u32. Per-warp global scratch: keep masks (one per
-// instruction) | choice masks (a uint2 per MIN/MAX): they grow with the tape,
-// and in shared memory they would cap the resident warps for every tree of a
-// batch at what its longest tape allows.
-template <int ROUND, int WARPS>
+// A work item is KI whole mask words of a node (32 * KI cells); lane l
+// evaluates cells grp*32*KI + h*32 + l, h < KI, so one decoded instruction
+// drives 32 * KI interval evaluations and the backward liveness walk covers
+// 32 * KI cells per step.
+//
+// Per-warp shared memory: slots [n_slots][32 lanes][KI] float2 | stage
+// [STAGE] uint4 | live [n_slots][KI] u32. Per-warp global scratch: keep masks
+// (KI words per instruction) | choice masks (KI uint2 per MIN/MAX): they grow
+// with the tape, and in shared memory they would cap the resident warps for
+// every tree of a batch at what its longest tape allows.
+template <int ROUND, int WARPS, int KI>
 // At least 20 warps per SM (5 blocks of 4 or 20 of 1): caps registers at 96,
 // which measured ~11 % faster than the unbounded 128 (more warps hide the
 // shared-memory and branch latencies of the interpreter); a cap of 80 spills.
 __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 5 : 20)
 interval_level_kernel(LevelLaunch p) {
     extern __shared__ __align__(16) unsigned char smem[];
+    constexpr uint32_t ROWB = 8 * KI;  // bytes per lane per slot
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned char* wbase = smem + (size_t)warp * p.smem_per_warp;
-    const uint32_t lane_base = smem_addr(wbase) + lane * 8;
-    uint4* stage = reinterpret_cast<uint4*>(wbase + (size_t)p.n_slots * 256);
-    uint32_t* live = reinterpret_cast<uint32_t*>(wbase + (size_t)p.n_slots * 256 + (STAGE + 1) * 16);
+    const uint32_t lane_base = smem_addr(wbase) + lane * ROWB;
+    uint4* stage = reinterpret_cast<uint4*>(wbase + (size_t)p.n_slots * 32 * ROWB);
+    uint32_t* live = reinterpret_cast<uint32_t*>(wbase + (size_t)p.n_slots * 32 * ROWB + (STAGE + 1) * 16);
     if (lane == 0) stage[STAGE] = make_uint4(0u, 0u, 0u, 0u);  // sentinel past a full chunk
 
     const uint32_t L = p.level;
@@ -299,7 +352,8 @@ interval_level_kernel(LevelLaunch p) {
                 have_tree = true;
             }
             const uint32_t dim = T.dim;
-            const uint32_t groups = dim * dim * dim / 32;
+            const uint32_t words = dim * dim * dim / 32;  // mask words per node
+            const uint32_t groups = words / KI;           // items per node
             const unsigned long long local = item - t_lo;
             const uint32_t node = (uint32_t)(local / groups), grp = (uint32_t)(local % groups);
             uint32_t* rec = T.nodes + T.ofs_l + (size_t)node * T.node_size;
@@ -309,27 +363,38 @@ interval_level_kernel(LevelLaunch p) {
             const uint32_t n = (uint32_t)__ldcg(&T.tapes[tape_idx]);
             const float cs = T.cs;
 
-            const uint32_t cell = grp * 32 + lane;
-            const uint32_t cz = cell % dim, cy = (cell / dim) % dim, cx = cell / (dim * dim);
-            const uint32_t gx = ncx * dim + cx, gy = ncy * dim + cy, gz = ncz * dim + cz;
-            // voxelizer/main.comp:113-116, :124-126
-            const float lox = __fadd_rn(T.lx, __fmul_rn((float)gx, cs));
-            const float loy = __fadd_rn(T.ly, __fmul_rn((float)gy, cs));
-            const float loz = __fadd_rn(T.lz, __fmul_rn((float)gz, cs));
-            sts_f2(lane_base + 0 * 256, make_float2(lox, __fadd_rn(lox, cs)));
-            sts_f2(lane_base + 1 * 256, make_float2(loy, __fadd_rn(loy, cs)));
-            sts_f2(lane_base + 2 * 256, make_float2(loz, __fadd_rn(loz, cs)));
-            sts_f2(lane_base + 3 * 256, make_float2(T.tt, T.tt));
+            uint32_t cell[KI], gx[KI], gy[KI], gz[KI];
+            IVK<KI> bx, by, bz, bt;
+#pragma unroll
+            for (int h = 0; h < KI; h++) {
+                cell[h] = grp * 32 * KI + h * 32 + lane;
+                const uint32_t cz = cell[h] % dim, cy = (cell[h] / dim) % dim, cx = cell[h] / (dim * dim);
+                gx[h] = ncx * dim + cx;
+                gy[h] = ncy * dim + cy;
+                gz[h] = ncz * dim + cz;
+                // voxelizer/main.comp:113-116, :124-126
+                const float lox = __fadd_rn(T.lx, __fmul_rn((float)gx[h], cs));
+                const float loy = __fadd_rn(T.ly, __fmul_rn((float)gy[h], cs));
+                const float loz = __fadd_rn(T.lz, __fmul_rn((float)gz[h], cs));
+                bx.v[h] = make_float2(lox, __fadd_rn(lox, cs));
+                by.v[h] = make_float2(loy, __fadd_rn(loy, cs));
+                bz.v[h] = make_float2(loz, __fadd_rn(loz, cs));
+                bt.v[h] = make_float2(T.tt, T.tt);
+            }
+            sts_iv<KI>(lane_base + 0 * 32 * ROWB, bx);
+            sts_iv<KI>(lane_base + 1 * 32 * ROWB, by);
+            sts_iv<KI>(lane_base + 2 * 32 * ROWB, bz);
+            sts_iv<KI>(lane_base + 3 * 32 * ROWB, bt);
 
             // ---- forward interval pass (interval.comp:121-160) ----
             uint32_t mm = 0;
-            float2 r = make_float2(0.0f, 0.0f);
+            IVK<KI> r;
             uint64_t pre[STAGE / 32];
             prefetch_chunk(pre, tape, 0, n, lane);
             for (uint32_t base = 0; base < n; base += STAGE) {
                 const uint32_t m = min(STAGE, n - base);
                 __syncwarp();
-                stage_chunk<false>(stage, pre, 8, lane, m);
+                stage_chunk<false>(stage, pre, ROWB, lane, m);
                 prefetch_chunk(pre, tape, base + STAGE, n, lane);
                 __syncwarp();
                 // The decode word of j+1 is read one instruction early.
@@ -340,89 +405,157 @@ interval_level_kernel(LevelLaunch p) {
                     dn = lds_u4(sbase + (j + 1) * 16);
                     if (d.x == OP_CONST) {
                         const float c = __uint_as_float(d.y);
-                        r = make_float2(c, c);
+#pragma unroll
+                        for (int h = 0; h < KI; h++) r.v[h] = make_float2(c, c);
                     } else {
-                        r = iv_exec<ROUND>(d, lane_base, lane, mmb, mm, p.mm_cap);
+                        r = iv_exec<ROUND, KI>(d, lane_base, lane, mmb, mm, p.mm_cap);
                     }
-                    sts_f2(lane_base + d.w, r);
+                    sts_iv<KI>(lane_base + d.w, r);
                 }
             }
             __syncwarp();
-            stat_work += 32ull * n;
+            stat_work += 32ull * KI * n;
 
             // ---- classification (voxelizer/main.comp:88-108) ----
-            const float2 d = lds_f2(lane_base);
-            const bool empty = d.x > 0.0f;
-            const bool leaf = !empty && d.y < 0.0f;
-            const bool amb = !empty && !leaf;
-            const uint32_t leaf_w = __ballot_sync(0xFFFFFFFFu, leaf);
-            const uint32_t amb_w = __ballot_sync(0xFFFFFFFFu, amb);
+            const IVK<KI> res = lds_iv<KI>(lane_base);
+            uint32_t leaf_w[KI], amb_w[KI], ok_w[KI];
+            bool ok[KI];
+            unsigned long long my_child[KI];
+            uint32_t n_amb = 0;
+#pragma unroll
+            for (int h = 0; h < KI; h++) {
+                const bool empty = res.v[h].x > 0.0f;
+                const bool leaf = !empty && res.v[h].y < 0.0f;
+                const bool amb = !empty && !leaf;
+                leaf_w[h] = __ballot_sync(0xFFFFFFFFu, leaf);
+                amb_w[h] = __ballot_sync(0xFFFFFFFFu, amb);
+                n_amb += __popc(amb_w[h]);
+            }
 
             // ---- child allocation (main.comp:138-148), warp-aggregated ----
-            const uint32_t n_amb = __popc(amb_w);
             unsigned long long child_base = 0;
             if (n_amb) {
                 if (lane == 0) child_base = atomicAdd(&T.H->node_count[L + 1], n_amb);
                 child_base = __shfl_sync(0xFFFFFFFFu, child_base, 0);
             }
-            const unsigned long long my_child = child_base + __popc(amb_w & lanemask_lt());
-            const bool ok = amb && my_child < T.child_cap;
-            const uint32_t ok_w = __ballot_sync(0xFFFFFFFFu, ok);
-            if (ok_w != amb_w && lane == 0) atomicOr(&T.H->overflow, 1u);
+            bool any_ok = false, lost = false;
+#pragma unroll
+            for (int h = 0; h < KI; h++) {
+                my_child[h] = child_base + __popc(amb_w[h] & lanemask_lt());
+                child_base += __popc(amb_w[h]);
+                const bool amb = (amb_w[h] >> lane) & 1u;
+                ok[h] = amb && my_child[h] < T.child_cap;
+                ok_w[h] = __ballot_sync(0xFFFFFFFFu, ok[h]);
+                any_ok |= ok_w[h] != 0u;
+                lost |= ok_w[h] != amb_w[h];
+            }
+            if (lost && lane == 0) atomicOr(&T.H->overflow, 1u);
 
-            uint32_t child_tape = tape_idx;
-            uint32_t child_len = n;
-            if (ok_w && T.shorten) {
+            uint32_t child_tape[KI], child_len[KI];
+#pragma unroll
+            for (int h = 0; h < KI; h++) {
+                child_tape[h] = tape_idx;
+                child_len[h] = n;
+            }
+            if (any_ok && T.shorten) {
                 // ---- backward liveness (shorten.comp:148-186) on transposed bitsets:
-                // live[s] bit l = slot s is live for lane l. The kept-mask of an
-                // instruction is live[out]; then live[out] = 0 and the inputs its
-                // choice uses become live for the lanes that kept it.
-                for (uint32_t s = lane; s < p.n_slots; s += 32) live[s] = 0u;
+                // live[s][h] bit l = slot s is live for cell grp*32*KI + h*32 + l.
+                // The kept-mask of an instruction is live[out]; then live[out] = 0
+                // and the inputs its choice uses become live for the cells that
+                // kept it.
+                for (uint32_t s = lane; s < p.n_slots * KI; s += 32) live[s] = 0u;
                 __syncwarp();
-                if (lane == 0) live[0] = ok_w;
+                if (lane == 0) {
+#pragma unroll
+                    for (int h = 0; h < KI; h++) live[h] = ok_w[h];
+                }
                 __syncwarp();
-                uint32_t kept = 0;
+                uint32_t kept[KI];
+#pragma unroll
+                for (int h = 0; h < KI; h++) kept[h] = 0;
                 int mmi = (int)mm - 1;
                 for (int hi = (int)n; hi > 0; hi -= 32) {
                     const int lo = max(0, hi - 32);
                     const int m = hi - lo;
                     // lane j holds instruction lo + j; walked from the top down
                     const uint64_t mine = (int)lane < m ? __ldcg(&tape[lo + lane]) : 0ull;
-                    uint32_t my_keep = 0;
+                    uint32_t my_keep[KI];
+#pragma unroll
+                    for (int h = 0; h < KI; h++) my_keep[h] = 0;
                     for (int j = m - 1; j >= 0; j--) {
                         const uint64_t w = __shfl_sync(0xFFFFFFFFu, mine, j);
                         const uint32_t op = w_op(w), o = w_out(w);
-                        const uint32_t k = live[o];
-                        if (k) {
-                            uint32_t first_m, second_m;
-                            if (op == OP_CONST) { first_m = 0u; second_m = 0u; }
-                            else if (op == OP_ADD || op == OP_SUB || op == OP_MUL || op == OP_DIV) {
-                                first_m = ~0u; second_m = ~0u;
+                        uint32_t k[KI];
+                        if constexpr (KI == 1) {
+                            k[0] = live[o];
+                        } else {
+                            const uint2 kk = *reinterpret_cast<const uint2*>(&live[o * 2]);
+                            k[0] = kk.x;
+                            k[1] = kk.y;
+                        }
+                        bool any = false;
+#pragma unroll
+                        for (int h = 0; h < KI; h++) any |= k[h] != 0u;
+                        if (any) {
+                            uint32_t first_m[KI], second_m[KI];
+                            if (op == OP_CONST) {
+#pragma unroll
+                                for (int h = 0; h < KI; h++) first_m[h] = second_m[h] = 0u;
+                            } else if (op == OP_ADD || op == OP_SUB || op == OP_MUL || op == OP_DIV) {
+#pragma unroll
+                                for (int h = 0; h < KI; h++) first_m[h] = second_m[h] = ~0u;
                             } else if (is_mm(op)) {
-                                const uint2 cb = mmb[mmi];
-                                first_m = cb.x; second_m = cb.y;
-                            } else { first_m = ~0u; second_m = 0u; }
-                            __syncwarp();
-                            if (lane == 0) {
-                                live[o] = 0u;
-                                const uint32_t fa = k & first_m, sb = k & second_m;
-                                if (fa) live[w_a(w)] |= fa;
-                                if (sb) live[w_b(w)] |= sb;
+#pragma unroll
+                                for (int h = 0; h < KI; h++) {
+                                    const uint2 cb = mmb[mmi * KI + h];
+                                    first_m[h] = cb.x;
+                                    second_m[h] = cb.y;
+                                }
+                            } else {
+#pragma unroll
+                                for (int h = 0; h < KI; h++) {
+                                    first_m[h] = ~0u;
+                                    second_m[h] = 0u;
+                                }
                             }
                             __syncwarp();
-                            kept += (k >> lane) & 1u;
+                            if (lane == 0) {
+                                const uint32_t ia = w_a(w), ib = w_b(w);
+#pragma unroll
+                                for (int h = 0; h < KI; h++) {
+                                    live[o * KI + h] = 0u;
+                                    const uint32_t fa = k[h] & first_m[h], sb = k[h] & second_m[h];
+                                    if (fa) live[ia * KI + h] |= fa;
+                                    if (sb) live[ib * KI + h] |= sb;
+                                }
+                            }
+                            __syncwarp();
+#pragma unroll
+                            for (int h = 0; h < KI; h++) kept[h] += (k[h] >> lane) & 1u;
                         }
-                        if ((int)lane == j) my_keep = k;
+                        if ((int)lane == j) {
+#pragma unroll
+                            for (int h = 0; h < KI; h++) my_keep[h] = k[h];
+                        }
                         if (is_mm(op)) mmi--;
                     }
-                    if ((int)lane < m) keep[lo + lane] = my_keep;
+                    if ((int)lane < m) {
+                        if constexpr (KI == 1) keep[lo + lane] = my_keep[0];
+                        else reinterpret_cast<uint2*>(keep)[lo + lane] = make_uint2(my_keep[0], my_keep[1]);
+                    }
                 }
                 __syncwarp();
 
                 // ---- claim output tapes (shorten.comp:136-142), one atomic per warp ----
-                const bool do_short = ok && kept < n;  // "not shorter -> reuse" (:188-191)
-                const uint32_t words = do_short ? (1 + kept + TAPE_ALIGN_WORDS - 1) / TAPE_ALIGN_WORDS * TAPE_ALIGN_WORDS : 0;
-                uint32_t incl = words;
+                bool do_short[KI];
+                uint32_t tw[KI], lane_words = 0;
+#pragma unroll
+                for (int h = 0; h < KI; h++) {
+                    do_short[h] = ok[h] && kept[h] < n;  // "not shorter -> reuse" (:188-191)
+                    tw[h] = do_short[h] ? (1 + kept[h] + TAPE_ALIGN_WORDS - 1) / TAPE_ALIGN_WORDS * TAPE_ALIGN_WORDS : 0;
+                    lane_words += tw[h];
+                }
+                uint32_t incl = lane_words;
                 for (int off = 1; off < 32; off <<= 1) {
                     const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, off);
                     if ((int)lane >= off) incl += v;
@@ -433,73 +566,104 @@ interval_level_kernel(LevelLaunch p) {
                     if (lane == 0) tbase = atomicAdd(&T.H->tape_top, (unsigned long long)total_words);
                     tbase = __shfl_sync(0xFFFFFFFFu, tbase, 0);
                 }
-                const unsigned long long my_tape = tbase + (incl - words);
-                const bool tape_ok = do_short && my_tape + words <= T.tape_cap;
-                if (do_short && !tape_ok) atomicOr(&T.H->overflow, 2u);
-                const uint32_t short_w = __ballot_sync(0xFFFFFFFFu, tape_ok);
+                unsigned long long my_tape[KI];
+                bool tape_ok[KI];
+                uint32_t short_w[KI], any_short = 0;
+                unsigned long long at = tbase + (incl - lane_words);
+#pragma unroll
+                for (int h = 0; h < KI; h++) {
+                    my_tape[h] = at;
+                    at += tw[h];
+                    tape_ok[h] = do_short[h] && my_tape[h] + tw[h] <= T.tape_cap;
+                    if (do_short[h] && !tape_ok[h]) atomicOr(&T.H->overflow, 2u);
+                    short_w[h] = __ballot_sync(0xFFFFFFFFu, tape_ok[h]);
+                    any_short |= short_w[h];
+                }
 
                 // ---- copy of the shortened tapes (shorten.comp:193-221) ----
-                // Chunk-outer: lane j holds instruction base + j, its keep mask
+                // Chunk-outer: lane j holds instruction base + j, its keep masks
                 // and (for MIN/MAX) its choice masks; each output tape then takes
                 // one ballot + one coalesced store per chunk.
-                if (short_w) {
-                    if (tape_ok) T.tapes[my_tape] = (uint64_t)kept;
-                    uint32_t run = 0;  // lane L: instructions written so far to its own tape
+                if (any_short) {
+                    uint32_t run[KI];  // lane L: instructions written so far to its own tapes
+#pragma unroll
+                    for (int h = 0; h < KI; h++) {
+                        if (tape_ok[h]) T.tapes[my_tape[h]] = (uint64_t)kept[h];
+                        run[h] = 0;
+                    }
                     uint32_t mm_run = 0;
                     for (uint32_t b = 0; b < n; b += 32) {
                         const uint32_t idx = b + lane;
                         const bool valid = idx < n;
                         const uint64_t w = valid ? __ldcg(&tape[idx]) : 0ull;
-                        const uint32_t kmask = valid ? keep[idx] : 0u;
+                        uint32_t kmask[KI];
+                        if constexpr (KI == 1) {
+                            kmask[0] = valid ? keep[idx] : 0u;
+                        } else {
+                            const uint2 kk = valid ? reinterpret_cast<const uint2*>(keep)[idx] : make_uint2(0u, 0u);
+                            kmask[0] = kk.x;
+                            kmask[1] = kk.y;
+                        }
                         const bool ism = valid && is_mm(w_op(w));
                         const uint32_t mball = __ballot_sync(0xFFFFFFFFu, ism);
-                        uint2 cb = make_uint2(0u, 0u);
-                        if (ism) cb = mmb[mm_run + __popc(mball & lanemask_lt())];
-                        uint32_t pending = short_w;
-                        while (pending) {
-                            const int sel = __ffs(pending) - 1;
-                            pending &= pending - 1;
-                            const bool kb = (kmask >> sel) & 1u;
-                            uint64_t wo = w;
-                            if (kb && ism) {
-                                const uint32_t c = ((cb.x >> sel) & 1u) | (((cb.y >> sel) & 1u) << 1);
-                                if (c == MM_FIRST) {
-                                    wo = (w & ~0xFFull) | OP_COPY;
-                                } else if (c == MM_SECOND) {  // COPY of B; the B field is kept
-                                    wo = (w & ~0xFFull & ~(0xFFFFull << 32)) | OP_COPY | ((uint64_t)w_b(w) << 32);
+                        uint2 cb[KI];
+#pragma unroll
+                        for (int h = 0; h < KI; h++) {
+                            cb[h] = make_uint2(0u, 0u);
+                            if (ism) cb[h] = mmb[(mm_run + __popc(mball & lanemask_lt())) * KI + h];
+                        }
+#pragma unroll
+                        for (int h = 0; h < KI; h++) {
+                            uint32_t pending = short_w[h];
+                            while (pending) {
+                                const int sel = __ffs(pending) - 1;
+                                pending &= pending - 1;
+                                const bool kb = (kmask[h] >> sel) & 1u;
+                                uint64_t wo = w;
+                                if (kb && ism) {
+                                    const uint32_t c = ((cb[h].x >> sel) & 1u) | (((cb[h].y >> sel) & 1u) << 1);
+                                    if (c == MM_FIRST) {
+                                        wo = (w & ~0xFFull) | OP_COPY;
+                                    } else if (c == MM_SECOND) {  // COPY of B; the B field is kept
+                                        wo = (w & ~0xFFull & ~(0xFFFFull << 32)) | OP_COPY | ((uint64_t)w_b(w) << 32);
+                                    }
                                 }
+                                const uint32_t kball = __ballot_sync(0xFFFFFFFFu, kb);
+                                const unsigned long long dst = __shfl_sync(0xFFFFFFFFu, my_tape[h], sel);
+                                const uint32_t rr = __shfl_sync(0xFFFFFFFFu, run[h], sel);
+                                if (kb) T.tapes[dst + 1 + rr + __popc(kball & lanemask_lt())] = wo;
+                                if ((int)lane == sel) run[h] += __popc(kball);
                             }
-                            const uint32_t kball = __ballot_sync(0xFFFFFFFFu, kb);
-                            const unsigned long long dst = __shfl_sync(0xFFFFFFFFu, my_tape, sel);
-                            const uint32_t r = __shfl_sync(0xFFFFFFFFu, run, sel);
-                            if (kb) T.tapes[dst + 1 + r + __popc(kball & lanemask_lt())] = wo;
-                            if ((int)lane == sel) run += __popc(kball);
                         }
                         mm_run += __popc(mball);
                     }
                 }
-                if (tape_ok) {
-                    child_tape = (uint32_t)my_tape;
-                    child_len = kept;
+#pragma unroll
+                for (int h = 0; h < KI; h++) {
+                    if (tape_ok[h]) {
+                        child_tape[h] = (uint32_t)my_tape[h];
+                        child_len[h] = kept[h];
+                    }
                 }
             }
 
             // ---- node records: masks, child list, children ----
-            if (ok) {
-                uint32_t* crec = T.nodes + T.ofs_next + (size_t)my_child * T.node_size_next;
-                crec[0] = child_tape;
-                crec[1] = gx;
-                crec[2] = gy;
-                crec[3] = gz;
-            }
-            rec[4 + 2 * groups + cell] = ok ? (uint32_t)my_child : 0xFFFFFFFFu;
-            if (lane == 0) {
-                rec[4 + grp] = leaf_w;
-                rec[4 + groups + grp] = ok_w;
-            }
-            if (ok) {
-                stat_sum += child_len;
-                stat_max = max(stat_max, child_len);
+#pragma unroll
+            for (int h = 0; h < KI; h++) {
+                if (ok[h]) {
+                    uint32_t* crec = T.nodes + T.ofs_next + (size_t)my_child[h] * T.node_size_next;
+                    crec[0] = child_tape[h];
+                    crec[1] = gx[h];
+                    crec[2] = gy[h];
+                    crec[3] = gz[h];
+                    stat_sum += child_len[h];
+                    stat_max = max(stat_max, child_len[h]);
+                }
+                rec[4 + 2 * words + cell[h]] = ok[h] ? (uint32_t)my_child[h] : 0xFFFFFFFFu;
+                if (lane == 0) {
+                    rec[4 + grp * KI + h] = leaf_w[h];
+                    rec[4 + words + grp * KI + h] = ok_w[h];
+                }
             }
         }
     }
@@ -707,19 +871,20 @@ point_level_kernel(LevelLaunch p) {
 // Lays the batch's items for `level` end to end: prefix[i] = items of trees
 // before i that this launch serves (interval passes: trees for which `level`
 // is not the last; point passes: trees for which it is, with a last-level node
-// size that takes `point_k` cells per lane). Interval passes also fix where
-// each tree's next level starts (node_ofs[level + 1]). One block.
-__device__ __forceinline__ unsigned long long level_items(TreeHeader* H, uint32_t L, int point, int point_k,
+// size that takes `k` cells per lane). An item is k mask words of a node (k
+// cells per lane). Interval passes also fix where each tree's next level
+// starts (node_ofs[level + 1]). One block.
+__device__ __forceinline__ unsigned long long level_items(TreeHeader* H, uint32_t L, int point, int k,
                                                           bool write_ofs) {
     if (L >= H->levels) return 0;
     const bool last = L == H->levels - 1;
     if ((point != 0) != last) return 0;
     const uint32_t dim = H->dims[L];
     const uint32_t words = dim * dim * dim / 32;
-    if (point && H->point_k != (uint32_t)point_k) return 0;
+    if (point && H->point_k != (uint32_t)k) return 0;
     const uint32_t count = level_count(H, L, H->node_cap, H->node_size[L]);
     if (!point && write_ofs) H->node_ofs[L + 1] = H->node_ofs[L] + (unsigned long long)count * H->node_size[L];
-    return (unsigned long long)count * (point ? words / (uint32_t)point_k : words);
+    return (unsigned long long)count * (words / (uint32_t)k);  // k: cells per lane of the pass
 }
 
 __global__ void __launch_bounds__(1024)
@@ -895,24 +1060,41 @@ static cudaError_t plan_point(uint32_t n_slots, LevelPlan* plan, int warps_hint)
     return occupancy(dev::point_level_kernel<1, K>, 32, pt, &plan->point_blocks);
 }
 
+template <int KI>
+static cudaError_t plan_interval(bool four, int rounding, uint32_t iv, LevelPlan* plan) {
+    if (four)
+        return rounding ? occupancy(dev::interval_level_kernel<1, 4, KI>, 128, 4 * iv, &plan->blocks)
+                        : occupancy(dev::interval_level_kernel<0, 4, KI>, 128, 4 * iv, &plan->blocks);
+    return rounding ? occupancy(dev::interval_level_kernel<1, 1, KI>, 32, iv, &plan->blocks)
+                    : occupancy(dev::interval_level_kernel<0, 1, KI>, 32, iv, &plan->blocks);
+}
+
 cudaError_t plan_levels(uint32_t n_slots, uint32_t mm_cap, int point_k, int rounding, LevelPlan* plan,
-                        int interval_warps, int point_warps) {
+                        int interval_warps, int point_warps, int interval_ki) {
     (void)mm_cap;  // the choice masks live in global scratch
-    const uint32_t iv = (n_slots * 256 + (dev::STAGE + 1) * 16 + n_slots * 4 + 15) / 16 * 16;
+    // Two cells per lane halve the dispatch work per cell but double a warp's
+    // slot rows: by default only while 16 warps still fit in an SM's shared
+    // memory (up to ~23 slots). Measured: the 23-slot 2048^3 scene's level-1
+    // pass 8.8 ms with two vs 9.5 ms with one; the 28-slot batch (13 warps
+    // with two) 106 vs 90 ms.
+    const auto iv_bytes = [&](uint32_t k) {
+        return (n_slots * 256 * k + (dev::STAGE + 1) * 16 + n_slots * 4 * k + 15) / 16 * 16;
+    };
+    const int ki = interval_ki == 1 || interval_ki == 2 ? interval_ki : (16 * iv_bytes(2) <= 227 * 1024 ? 2 : 1);
+    plan->interval_ki = ki;
+    const uint32_t iv = iv_bytes((uint32_t)ki);
     plan->smem_per_warp = iv;
     // Four warps (four tapes) per block when they fit in shared memory, else
     // one; a hint of 1 or 4 overrides the choice where shared memory allows.
     const bool four = 4ull * iv <= (interval_warps == 4 ? 227u : 200u) * 1024 && interval_warps != 1;
     plan->warps_per_block = four ? 4 : 1;
     if (!four && iv > 227 * 1024) return cudaErrorInvalidValue;
-    cudaError_t e;
-    if (four) {
-        e = rounding ? occupancy(dev::interval_level_kernel<1, 4>, 128, 4 * iv, &plan->blocks)
-                     : occupancy(dev::interval_level_kernel<0, 4>, 128, 4 * iv, &plan->blocks);
-    } else {
-        e = rounding ? occupancy(dev::interval_level_kernel<1, 1>, 32, iv, &plan->blocks)
-                     : occupancy(dev::interval_level_kernel<0, 1>, 32, iv, &plan->blocks);
-    }
+    // Both cell widths may run with this plan's shared memory (a level-0 pass
+    // takes one cell per lane): raise both kernels' limits, then size the grid
+    // for the planned width.
+    cudaError_t e = ki == 2 ? plan_interval<1>(four, rounding, iv, plan) : plan_interval<2>(four, rounding, iv, plan);
+    if (e == cudaSuccess)
+        e = ki == 2 ? plan_interval<2>(four, rounding, iv, plan) : plan_interval<1>(four, rounding, iv, plan);
     if (e != cudaSuccess) return e;
     plan->point_k = point_k;
     return point_k == 4 ? plan_point<4>(n_slots, plan, point_warps) : plan_point<2>(n_slots, plan, point_warps);
@@ -940,7 +1122,7 @@ cudaError_t launch_level_scan(const LevelLaunch& a, bool point, int point_k, cud
 }
 
 cudaError_t launch_level(const LevelLaunch& a, const LevelPlan& plan, int rounding, bool point,
-                         cudaStream_t stream) {
+                         cudaStream_t stream, int interval_ki) {
     if (point) {
         LevelLaunch b = a;
         b.smem_per_warp = plan.point_smem_per_warp;
@@ -959,13 +1141,26 @@ cudaError_t launch_level(const LevelLaunch& a, const LevelPlan& plan, int roundi
     b.smem_per_warp = plan.smem_per_warp;
     const int w = plan.warps_per_block;
     const size_t smem = (size_t)w * plan.smem_per_warp;
-    if (w == 4) {
-        if (rounding) dev::interval_level_kernel<1, 4><<<plan.blocks, 128, smem, stream>>>(b);
-        else dev::interval_level_kernel<0, 4><<<plan.blocks, 128, smem, stream>>>(b);
+    const int tpb = 32 * w;
+#define FREP_IV_LAUNCH(R, W, KI) dev::interval_level_kernel<R, W, KI><<<plan.blocks, tpb, smem, stream>>>(b)
+    if ((interval_ki ? interval_ki : plan.interval_ki) == 2) {
+        if (w == 4) {
+            if (rounding) FREP_IV_LAUNCH(1, 4, 2);
+            else FREP_IV_LAUNCH(0, 4, 2);
+        } else {
+            if (rounding) FREP_IV_LAUNCH(1, 1, 2);
+            else FREP_IV_LAUNCH(0, 1, 2);
+        }
     } else {
-        if (rounding) dev::interval_level_kernel<1, 1><<<plan.blocks, 32, smem, stream>>>(b);
-        else dev::interval_level_kernel<0, 1><<<plan.blocks, 32, smem, stream>>>(b);
+        if (w == 4) {
+            if (rounding) FREP_IV_LAUNCH(1, 4, 1);
+            else FREP_IV_LAUNCH(0, 4, 1);
+        } else {
+            if (rounding) FREP_IV_LAUNCH(1, 1, 1);
+            else FREP_IV_LAUNCH(0, 1, 1);
+        }
     }
+#undef FREP_IV_LAUNCH
     return cudaGetLastError();
 }
 
