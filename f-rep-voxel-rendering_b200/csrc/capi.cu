@@ -48,14 +48,18 @@ const char* frep_version(void) { return "frep-b200 0.1 (sm_100a)"; }
 
 // ---- tapes -------------------------------------------------------------------
 
-frep_status frep_tape_compile(const frep_dag* dag, frep_tape** out) {
+frep_status frep_tape_compile(const frep_dag* dag, frep_tape** out) { return frep_tape_compile_opts(dag, nullptr, out); }
+
+frep_status frep_tape_compile_opts(const frep_dag* dag, const frep_tape_opts* opts, frep_tape** out) {
     if (!dag || !out || !dag->ops || !dag->in0 || !dag->in1 || !dag->consts)
         return fail(FREP_ERR_INVALID_ARG, "frep_tape_compile: null argument");
+    const uint32_t reload = !opts || opts->const_reload_distance == 0 ? 8u
+                            : opts->const_reload_distance == 0xFFFFFFFFu ? 0u : opts->const_reload_distance;
     std::vector<frep::DagNode> nodes(dag->n_nodes);
     for (uint32_t i = 0; i < dag->n_nodes; i++)
         nodes[i] = {dag->ops[i], dag->in0[i], dag->in1[i], dag->consts[i]};
     auto* t = new frep_tape();
-    std::string err = frep::compile_tape(nodes.data(), dag->n_nodes, dag->root, &t->ct);
+    std::string err = frep::compile_tape(nodes.data(), dag->n_nodes, dag->root, &t->ct, reload);
     if (!err.empty()) {
         delete t;
         return fail(FREP_ERR_COMPILE, "frep_tape_compile: %s", err.c_str());

@@ -70,7 +70,11 @@ struct CompiledTape {
 
 // Returns an empty string on success, else a message. The DAG must be
 // topologically ordered (inputs before users) with root < n.
-std::string compile_tape(const DagNode* nodes, uint32_t n, uint32_t root, CompiledTape* out);
+// const_reload: for tapes beyond the reference's 8-bit encoding, a use that
+// lies more than this many instructions after its constant's last load gets a
+// CONST of its own (slots reallocated); 0 = never.
+std::string compile_tape(const DagNode* nodes, uint32_t n, uint32_t root, CompiledTape* out,
+                         uint32_t const_reload = 8);
 
 // Imports a tape in the wide encoding (as frep_tape_get_instrs returns it):
 // validates the opcodes and derives the slot count, MIN/MAX count and whether

@@ -45,13 +45,16 @@ class Tape:
     """A compiled tape (csg::Tape). ``Tape(expr)`` runs the library's compiler
     (simplify, topological sort, constant pool, slot allocation)."""
 
-    def __init__(self, expr: csg.Expr | None = None, *, _handle=None):
+    def __init__(self, expr: csg.Expr | None = None, *, _handle=None, const_reload: int = 0):
+        """const_reload: frep_tape_opts.const_reload_distance (0 = default,
+        0xFFFFFFFF = keep the reference's slot allocation everywhere)."""
         self._h = C.c_void_p()
         if _handle is not None:
             self._h = _handle
         elif expr is not None:
             d, keep = _dag_struct(expr)
-            L.check(L.lib().frep_tape_compile(C.byref(d), C.byref(self._h)))
+            opts = L.TapeOpts(const_reload)
+            L.check(L.lib().frep_tape_compile_opts(C.byref(d), C.byref(opts), C.byref(self._h)))
         else:
             raise ValueError("Tape needs an expression")
         info = L.TapeInfo()

@@ -30,6 +30,10 @@ class Dag(C.Structure):
                 ("in1", C.POINTER(C.c_uint32)), ("consts", C.POINTER(C.c_float)), ("root", C.c_uint32)]
 
 
+class TapeOpts(C.Structure):
+    _fields_ = [("const_reload_distance", C.c_uint32), ("reserved", C.c_uint32 * 3)]
+
+
 class TapeInfo(C.Structure):
     _fields_ = [("n_instr", C.c_uint32), ("n_slots", C.c_uint32), ("n_consts", C.c_uint32),
                 ("n_minmax", C.c_uint32), ("fits_reference", C.c_uint32), ("uses_time", C.c_uint32)]
@@ -107,6 +111,7 @@ _SIGS = {
     "frep_last_error": (C.c_char_p, []),
     "frep_version": (C.c_char_p, []),
     "frep_tape_compile": (C.c_int, [C.POINTER(Dag), C.POINTER(_P)]),
+    "frep_tape_compile_opts": (C.c_int, [C.POINTER(Dag), C.POINTER(TapeOpts), C.POINTER(_P)]),
     "frep_tape_from_reference": (C.c_int, [_P, C.c_uint32, _P, C.c_uint32, C.POINTER(_P)]),
     "frep_tape_get_info": (C.c_int, [_P, C.POINTER(TapeInfo)]),
     "frep_tape_get_instrs": (C.c_int, [_P, _P, C.c_uint32]),

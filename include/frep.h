@@ -82,8 +82,22 @@ typedef struct frep_tape_info {
 
 /* Replaces csg::Tape::Tape(Expr) (vulkan/src/csg/tape.cpp:14-228): simplify,
  * topologically sort, pool constants, allocate slots. Same instruction stream
- * as the reference; wide encoding so that large scenes compile. */
+ * as the reference for every tape its 8-bit encoding can hold; wide encoding
+ * so that large scenes compile. */
 frep_status frep_tape_compile(const frep_dag* dag, frep_tape** out);
+
+/* Compiler options. const_reload_distance applies to tapes beyond the 8-bit
+ * encoding only (whose instruction stream is this library's own): a use of a
+ * pooled constant more than this many instructions after its last load gets
+ * a CONST of its own and slots are allocated again, so that shared constants
+ * do not hold slots across the tape (the 256-primitive scene: 23 -> 14
+ * slots for 15 % more instructions; each slot costs every resident warp a
+ * shared-memory row on the device). 0 = default (8), 0xFFFFFFFF = never. */
+typedef struct frep_tape_opts {
+    uint32_t const_reload_distance;
+    uint32_t reserved[3];
+} frep_tape_opts;
+frep_status frep_tape_compile_opts(const frep_dag* dag, const frep_tape_opts* opts, frep_tape** out);
 
 /* Accepts a tape in the reference's own upload format
  * (vulkan/src/engine/voxelizer.cpp:385-398: op | out<<8 | inA<<16 | inB<<24)

@@ -143,3 +143,35 @@ def test_wide_import_rejects_bad_tapes():
     if len(a) > 1 and ((int(a[-2]) >> 16) & 0xFFFF) != 0:
         with pytest.raises(frep.FrepError):
             frep.Tape.from_wide(not_slot0)
+
+
+@pytest.mark.parametrize("n,seed", [(64, 3), (256, 2), (700, 9)])
+def test_constant_reload_keeps_values_and_cuts_slots(n, seed):
+    """Beyond the 8-bit encoding, reloading far-away constants changes only
+    CONSTs and slot numbers: the other instructions keep their order and
+    opcodes, every point value is bit-identical, and fewer slots are used."""
+    expr = scenes.random_csg(n, seed=seed).shape
+    plain = frep.Tape(expr, const_reload=0xFFFFFFFF)
+    packed = frep.Tape(expr)
+    assert not packed.fits_reference
+    wp, wk = plain.wide(), packed.wide()
+    ops_p, ops_k = wp & np.uint64(0xFF), wk & np.uint64(0xFF)
+    np.testing.assert_array_equal(ops_p[ops_p != 0], ops_k[ops_k != 0])
+    assert (ops_k == 0).sum() > (ops_p == 0).sum()
+    assert packed.n_slots < plain.n_slots
+    assert packed.n_minmax == plain.n_minmax and packed.uses_time == plain.uses_time
+    pts = np.random.default_rng(seed).uniform(-1.3, 1.3, (4000, 4)).astype(np.float32)
+    np.testing.assert_array_equal(plain.eval_points(pts), packed.eval_points(pts))
+    # the oracle's interval view agrees too
+    for lo, hi in (([-0.4, -0.3, -0.2], [0.1, 0.2, 0.3]), ([0.2, 0.1, -0.9], [0.25, 0.15, -0.85])):
+        iv_p, ch_p = oracle.eval_interval(wp, plain.n_slots, lo, hi, 0.0, 1)
+        iv_k, ch_k = oracle.eval_interval(wk, packed.n_slots, lo, hi, 0.0, 1)
+        np.testing.assert_array_equal(iv_p, iv_k)
+        np.testing.assert_array_equal(ch_p, ch_k)
+
+
+def test_small_tapes_keep_the_reference_stream():
+    expr = scenes.spheres_union(16).shape
+    a, b = frep.Tape(expr), frep.Tape(expr, const_reload=0xFFFFFFFF)
+    assert a.fits_reference
+    np.testing.assert_array_equal(a.wide(), b.wide())
