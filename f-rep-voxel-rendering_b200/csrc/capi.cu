@@ -280,6 +280,7 @@ frep_status tree_create_impl(frep_ctx* ctx, const frep_grid* grid, const frep_vo
     h.tape_cap = t->tape_cap;
     h.levels = grid->levels;
     h.shorten = t->opts.shorten;
+    h.share_tapes = t->opts.separate_tapes ? 0u : 1u;
     for (uint32_t l = 0; l < grid->levels; l++) {
         h.dims[l] = grid->dims[l];
         h.node_size[l] = t->node_size[l];

@@ -30,6 +30,7 @@ struct TreeHeader {
     unsigned long long tape_cap;               // u64 words
     uint32_t levels;
     uint32_t shorten;
+    uint32_t share_tapes;                      // identical child tapes of a group stored once
     uint32_t dims[MAX_LEVELS];
     uint32_t node_size[MAX_LEVELS];            // u32 words
     float cell_size[MAX_LEVELS];

@@ -139,7 +139,7 @@ struct LevelTree {
     uint32_t* nodes;
     uint64_t* tapes;
     unsigned long long tape_cap, ofs_l, ofs_next, child_cap;
-    uint32_t dim, node_size, node_size_next, shorten;
+    uint32_t dim, node_size, node_size_next, shorten, share;
     float cs, lx, ly, lz, tt;
 };
 
@@ -153,6 +153,7 @@ __device__ __forceinline__ LevelTree load_tree(TreeHeader* H, uint32_t L, bool p
     t.node_size = H->node_size[L];
     t.ofs_l = H->node_ofs[L];
     t.shorten = H->shorten;
+    t.share = H->share_tapes;
     t.cs = H->cell_size[L];
     t.lx = H->low[0];
     t.ly = H->low[1];
@@ -471,8 +472,15 @@ interval_level_kernel(LevelLaunch p) {
                 }
                 __syncwarp();
                 uint32_t kept[KI];
+                // sig: a cheap summary of this cell's output tape (the kept
+                // instruction positions and the MIN/MAX rewrites), to group
+                // cells whose tapes may be identical (verified exactly below)
+                uint32_t sig[KI];
 #pragma unroll
-                for (int h = 0; h < KI; h++) kept[h] = 0;
+                for (int h = 0; h < KI; h++) {
+                    kept[h] = 0;
+                    sig[h] = 0;
+                }
                 int mmi = (int)mm - 1;
                 for (int hi = (int)n; hi > 0; hi -= 32) {
                     const int lo = max(0, hi - 32);
@@ -531,7 +539,12 @@ interval_level_kernel(LevelLaunch p) {
                             }
                             __syncwarp();
 #pragma unroll
-                            for (int h = 0; h < KI; h++) kept[h] += (k[h] >> lane) & 1u;
+                            for (int h = 0; h < KI; h++) {
+                                const uint32_t kb = (k[h] >> lane) & 1u;
+                                kept[h] += kb;
+                                const uint32_t code = kb + ((first_m[h] >> lane) & kb) + ((second_m[h] >> lane) & kb) * 2u;
+                                sig[h] += code * (uint32_t)(lo + j + 1) * 0x9E3779B1u;
+                            }
                         }
                         if ((int)lane == j) {
 #pragma unroll
@@ -546,13 +559,81 @@ interval_level_kernel(LevelLaunch p) {
                 }
                 __syncwarp();
 
-                // ---- claim output tapes (shorten.comp:136-142), one atomic per warp ----
+                // ---- one tape per distinct output (this library's addition) ----
+                // Cells of a 32-cell group whose shortened tapes are identical
+                // share one copy: neighbouring cells usually keep the same
+                // primitives, and the pool then holds ~3x fewer tape words. A
+                // cell's leader is the lowest lane with the same signature and
+                // length; the grouping is then verified exactly (keep bits and
+                // MIN/MAX rewrites column by column), so a signature collision
+                // only costs a copy. Contents per cell are unchanged.
                 bool do_short[KI];
-                uint32_t tw[KI], lane_words = 0;
+                uint32_t leader[KI], lead_w[KI], group[KI];
 #pragma unroll
                 for (int h = 0; h < KI; h++) {
                     do_short[h] = ok[h] && kept[h] < n;  // "not shorter -> reuse" (:188-191)
-                    tw[h] = do_short[h] ? (1 + kept[h] + TAPE_ALIGN_WORDS - 1) / TAPE_ALIGN_WORDS * TAPE_ALIGN_WORDS : 0;
+                    const unsigned long long key = do_short[h] && T.share
+                                                       ? ((unsigned long long)sig[h] << 32 | kept[h]) * 2ull + 1ull
+                                                       : 2ull * (lane + 1);
+                    group[h] = __match_any_sync(0xFFFFFFFFu, key);
+                    leader[h] = __ffs(group[h]) - 1;
+                }
+                {
+                    // leaders whose group has followers
+                    uint32_t lwf[KI], any_fol = 0;
+#pragma unroll
+                    for (int h = 0; h < KI; h++) {
+                        lwf[h] = __ballot_sync(0xFFFFFFFFu, do_short[h] && leader[h] == lane && __popc(group[h]) > 1);
+                        any_fol |= lwf[h];
+                    }
+                    if (any_fol) {
+                        uint32_t bad[KI];
+#pragma unroll
+                        for (int h = 0; h < KI; h++) bad[h] = 0;
+                        uint32_t mm_v = 0;
+                        for (uint32_t b = 0; b < n; b += 32) {
+                            const uint32_t idx = b + lane;
+                            const bool valid = idx < n;
+                            const uint64_t w = valid ? __ldcg(&tape[idx]) : 0ull;
+                            const bool ism = valid && is_mm(w_op(w));
+                            const uint32_t mball = __ballot_sync(0xFFFFFFFFu, ism);
+#pragma unroll
+                            for (int h = 0; h < KI; h++) {
+                                const uint32_t km = valid ? keep[(size_t)idx * KI + h] : 0u;
+                                uint2 cb = make_uint2(0u, 0u);
+                                if (ism) cb = mmb[(mm_v + __popc(mball & lanemask_lt())) * KI + h];
+                                // lane `lane` holds instruction idx: within each group,
+                                // every member's keep bit (and, where kept, its MIN/MAX
+                                // choice bits) must equal the leader's
+                                uint32_t pend = lwf[h], d = 0;
+                                while (pend) {
+                                    const int ld = __ffs(pend) - 1;
+                                    pend &= pend - 1;
+                                    const uint32_t M = __shfl_sync(0xFFFFFFFFu, group[h], ld);
+                                    uint32_t diff = (km & M) ^ (((km >> ld) & 1u) ? M : 0u);
+                                    if (ism)
+                                        diff |= ((cb.x & M) ^ (((cb.x >> ld) & 1u) ? M : 0u) |
+                                                 (cb.y & M) ^ (((cb.y >> ld) & 1u) ? M : 0u)) & km;
+                                    d |= diff;
+                                }
+                                bad[h] |= __reduce_or_sync(0xFFFFFFFFu, d);
+                            }
+                            mm_v += __popc(mball);
+                        }
+#pragma unroll
+                        for (int h = 0; h < KI; h++)
+                            if ((bad[h] >> lane) & 1u) leader[h] = lane;
+                    }
+                }
+
+                // ---- claim output tapes (shorten.comp:136-142), one atomic per warp ----
+                uint32_t tw[KI], lane_words = 0;
+#pragma unroll
+                for (int h = 0; h < KI; h++) {
+                    lead_w[h] = __ballot_sync(0xFFFFFFFFu, do_short[h] && leader[h] == lane);
+                    tw[h] = ((lead_w[h] >> lane) & 1u)
+                                ? (1 + kept[h] + TAPE_ALIGN_WORDS - 1) / TAPE_ALIGN_WORDS * TAPE_ALIGN_WORDS
+                                : 0;
                     lane_words += tw[h];
                 }
                 uint32_t incl = lane_words;
@@ -574,10 +655,17 @@ interval_level_kernel(LevelLaunch p) {
                 for (int h = 0; h < KI; h++) {
                     my_tape[h] = at;
                     at += tw[h];
-                    tape_ok[h] = do_short[h] && my_tape[h] + tw[h] <= T.tape_cap;
-                    if (do_short[h] && !tape_ok[h]) atomicOr(&T.H->overflow, 2u);
-                    short_w[h] = __ballot_sync(0xFFFFFFFFu, tape_ok[h]);
+                    const bool lead = (lead_w[h] >> lane) & 1u;
+                    tape_ok[h] = lead && my_tape[h] + tw[h] <= T.tape_cap;
+                    if (lead && !tape_ok[h]) atomicOr(&T.H->overflow, 2u);
+                    short_w[h] = __ballot_sync(0xFFFFFFFFu, tape_ok[h]);  // leaders whose tape is written
                     any_short |= short_w[h];
+                    // followers take their leader's tape
+                    const unsigned long long lt = __shfl_sync(0xFFFFFFFFu, my_tape[h], (int)leader[h]);
+                    if (do_short[h] && !lead) {
+                        my_tape[h] = lt;
+                        tape_ok[h] = (short_w[h] >> leader[h]) & 1u;
+                    }
                 }
 
                 // ---- copy of the shortened tapes (shorten.comp:193-221) ----
@@ -588,7 +676,7 @@ interval_level_kernel(LevelLaunch p) {
                     uint32_t run[KI];  // lane L: instructions written so far to its own tapes
 #pragma unroll
                     for (int h = 0; h < KI; h++) {
-                        if (tape_ok[h]) T.tapes[my_tape[h]] = (uint64_t)kept[h];
+                        if ((short_w[h] >> lane) & 1u) T.tapes[my_tape[h]] = (uint64_t)kept[h];
                         run[h] = 0;
                     }
                     uint32_t mm_run = 0;

@@ -96,7 +96,8 @@ class Tape:
         return cls(_handle=h)
 
     def __del__(self):
-        if getattr(self, "_h", None) and self._h.value:
+        # at interpreter exit the module globals may already be gone
+        if L is not None and C is not None and L._lib is not None and getattr(self, "_h", None) and self._h.value:
             L.lib().frep_tape_destroy(self._h)
             self._h = C.c_void_p()
 
@@ -157,7 +158,8 @@ class Context:
         self._h = C.c_void_p()
 
     def __del__(self):
-        self.close()
+        if L is not None and C is not None:
+            self.close()
 
 
 @dataclass
@@ -183,7 +185,7 @@ class VoxelStorage:
 
     def __init__(self, grid_dims=(16, 4), low_vertex=(-1.5, -1.5, -1.5), world_size=3.0,
                  rounding: int = ROUND_OUTWARD, shorten: bool = True, node_words: int = 0,
-                 tape_words: int = 0, point_cells_per_lane: int = 0):
+                 tape_words: int = 0, point_cells_per_lane: int = 0, separate_tapes: bool = False):
         self.grid_dims = list(grid_dims)
         self.low_vertex = tuple(float(v) for v in low_vertex)
         self.world_size = float(world_size)
@@ -192,6 +194,7 @@ class VoxelStorage:
         self.node_words = node_words
         self.tape_words = tape_words
         self.point_cells_per_lane = point_cells_per_lane
+        self.separate_tapes = separate_tapes
         self.tape: Tape | None = None
         self.ctx: Context | None = None
         self._tree = C.c_void_p()
@@ -219,7 +222,7 @@ class VoxelStorage:
         self.ctx = ctx
         self.tape = shape if isinstance(shape, Tape) else Tape(shape)
         opts = L.VoxelizeOpts(self.rounding, 1 if self.shorten else 0, self.node_words, self.tape_words,
-                              self.point_cells_per_lane, 0)
+                              self.point_cells_per_lane, 1 if self.separate_tapes else 0)
         g = self.grid_struct()
         L.check(L.lib().frep_tree_create(ctx._h, C.byref(g), C.byref(opts), C.byref(self._tree)))
         self.interior_node_count = [0] * self.grid_levels
@@ -230,12 +233,13 @@ class VoxelStorage:
         return self._tree
 
     def cleanup(self):
-        if self._tree.value:
+        if self._tree.value and L._lib is not None:
             L.lib().frep_tree_destroy(self._tree)
             self._tree = C.c_void_p()
 
     def __del__(self):
-        self.cleanup()
+        if L is not None and C is not None:
+            self.cleanup()
 
     def sync(self, raise_on_overflow: bool = True) -> L.TreeInfo:
         info = L.TreeInfo()
@@ -440,7 +444,8 @@ class Batch:
         self._h = C.c_void_p()
 
     def __del__(self):
-        self.close()
+        if L is not None and C is not None:
+            self.close()
 
     def set_tapes(self):
         self._tapes = (C.c_void_p * len(self.storages))(*[s.tape.handle.value for s in self.storages])
@@ -537,7 +542,8 @@ class Server:
         self._keep.clear()
 
     def __del__(self):
-        self.close()
+        if L is not None and C is not None:
+            self.close()
 
     def add_scene(self, tape: Tape, grid_dims, low_vertex, world_size, node_words: int = 0, tape_words: int = 0,
                   point_cells_per_lane: int = 0, rounding: int = ROUND_OUTWARD) -> int:

@@ -52,7 +52,7 @@ class BatchInfo(C.Structure):
 
 class VoxelizeOpts(C.Structure):
     _fields_ = [("rounding", C.c_uint32), ("shorten", C.c_uint32), ("node_words", C.c_uint64),
-                ("tape_words", C.c_uint64), ("point_cells_per_lane", C.c_uint32), ("reserved", C.c_uint32)]
+                ("tape_words", C.c_uint64), ("point_cells_per_lane", C.c_uint32), ("separate_tapes", C.c_uint32)]
 
 
 class TreeInfo(C.Structure):

@@ -167,7 +167,9 @@ typedef struct frep_voxelize_opts {
     uint64_t tape_words;      /* tape pool capacity in u64 words (0 = automatic)     */
     uint32_t point_cells_per_lane; /* last-level pass: cells per lane, 2 or 4 (0 =
                                     * automatic: 4 when dim^3/32 is a multiple of 4) */
-    uint32_t reserved;        /* 0                                                   */
+    uint32_t separate_tapes;  /* 0: cells of a 32-cell group whose shortened tapes
+                               * are identical share one copy (~3x less tape pool);
+                               * 1: one copy per cell, as the reference stores them */
 } frep_voxelize_opts;
 
 typedef struct frep_tree frep_tree;

@@ -146,3 +146,29 @@ def test_stress_gyroid_small(ctx, rounding, t):
     assert compare_hits(d_hits, o_hits, exp, orc) == []
     np.testing.assert_array_equal(d_rgba, o_rgba)
     assert sum(exp.node_count) > 100
+
+
+@pytest.mark.parametrize("rounding", [0, 1])
+def test_identical_child_tapes_are_stored_once(ctx, rounding):
+    """Cells of a 32-cell group with identical shortened tapes share one copy:
+    same canonical tree as the oracle (which stores every copy), a smaller
+    pool, and leaf nodes that point at the same tape."""
+    sc = scenes.random_csg(120, seed=31, grid_dims=[16, 8, 4], width=64, height=48)
+    vs = device_tree(ctx, sc, rounding=rounding)
+    exp = vs.export()
+    orc = oracle_tree(sc, vs.tape, rounding=rounding)
+    assert compare_trees(exp, orc) == []
+    used = vs.sync().tape_words_used
+    assert used < 0.6 * len(orc.tapes), (used, len(orc.tapes))
+    last = exp.levels - 1
+    base, size = exp.node_offset[last], exp.node_size[last]
+    idx = exp.nodes[base: base + exp.node_count[last] * size: size]
+    assert len(np.unique(idx)) < 0.5 * len(idx)
+    # one copy per cell, as the reference (and the oracle) store them
+    vs2 = frep.VoxelStorage(sc.grid_dims, sc.low_vertex, sc.world_size, rounding=rounding, separate_tapes=True)
+    vs2.init(ctx, sc.shape)
+    frep.Voxelizer(ctx, vs2).voxelize(0.0)
+    exp2 = vs2.export()
+    assert compare_trees(exp2, orc) == []
+    idx2 = exp2.nodes[base: base + exp2.node_count[last] * size: size]
+    assert vs2.sync().tape_words_used > used and len(np.unique(idx2)) > len(np.unique(idx))
