@@ -52,8 +52,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=("batch", "large", "stress"), default="batch")
+    ap.add_argument("--workload", choices=("batch", "large", "stress", "animated"), default="batch")
     ap.add_argument("--frames", type=int, default=30, help="stress: animation frames (T = frame / frames)")
+    ap.add_argument("--no-reuse", action="store_true",
+                    help="animated: re-voxelize every frame in full (no reuse of the previous frame's tree)")
     ap.add_argument("--scenes", type=int, default=512, help="batch: number of scenes")
     ap.add_argument("--plain-steps", type=int, default=2, help="batch: timed passes of the plain launch loop")
     ap.add_argument("--no-tune", action="store_true", help="batch: default branching, no autotuning")
@@ -82,6 +84,9 @@ def parse():
     elif args.workload == "stress":
         args.workload_name = (f"stress_twisted_gyroid_64spheres_{fine}cube_{args.width}x{args.height}_shadow_"
                               f"{args.frames}frames")
+    elif args.workload == "animated":
+        args.workload_name = (f"animated_csg_256prim_4orbiting_{fine}cube_{args.width}x{args.height}_shadow_"
+                              f"60fps_{'full' if args.no_reuse else 'reuse'}")
     else:
         args.workload_name = f"random_csg_256prim_{fine}cube_{args.width}x{args.height}_shadow"
     return args
@@ -186,13 +191,19 @@ def make_scene(args, grid_dims=None):
     dims = grid_dims or args.grid_dims
     if args.workload == "stress":
         return scenes.stress_gyroid(grid_dims=dims, width=args.width, height=args.height)
+    if args.workload == "animated":
+        return scenes.animated_csg(256, 4, seed=2, grid_dims=dims, width=args.width, height=args.height)
     return scenes.random_csg(256, seed=2, grid_dims=dims, width=args.width, height=args.height, shadows=True)
 
 
 def frame_times(args):
-    """Tape time of each step: the stress animation sweeps T over [0, 1)."""
+    """Tape time of each step: the stress animation sweeps T over [0, 1); the
+    animated scene advances T by 1/60 per frame (4 s per revolution of its
+    spheres; the list is long enough never to wrap within a run)."""
     if args.workload == "stress":
         return [f / args.frames for f in range(args.frames)]
+    if args.workload == "animated":
+        return [0.3 + f / 60.0 for f in range(100000)]
     return [0.0]
 
 
@@ -269,6 +280,14 @@ def run_ours(args, world, rank, local):
                            node_words=node_words, tape_words=tape_words)
     vs.init(ctx, scene.shape)
     vox = frep.Voxelizer(ctx, vs)
+    # the animated scene alternates two trees, each frame reusing the other
+    anim = args.workload == "animated"
+    reuse = anim and not args.no_reuse
+    storages = [vs]
+    if anim:
+        storages.append(frep.VoxelStorage(scene.grid_dims, scene.low_vertex, scene.world_size,
+                                          rounding=frep.ROUND_OUTWARD, node_words=node_words,
+                                          tape_words=tape_words).init(ctx, vs.tape))
     rt = frep.Raytracer(ctx, vs)
     rt.lights = frep.Lights(shadow_mask=scene.shadow_mask)
     W, H = scene.width, scene.height
@@ -279,17 +298,31 @@ def run_ours(args, world, rank, local):
 
     frame = [0]
 
-    def step():
-        t = tt[frame[0] % len(tt)]
+    def voxelize_frame():
+        """Voxelizes the next frame; returns its tape time and storage."""
+        f = frame[0]
         frame[0] += 1
-        vox.voxelize(t, stream)
+        t = tt[f % len(tt)]
+        cur = storages[f % len(storages)]
+        prev = storages[(f - 1) % 2] if reuse and f > 0 else None
+        frep.Voxelizer(ctx, cur).voxelize(t, stream, reuse=prev)
+        rt.voxels = cur
+        return t, cur
+
+    def step():
+        t, _ = voxelize_frame()
         rt.trace(scene.camera, t, W, H, out=(rgba, None), stream=stream)
 
     for _ in range(args.warmup):
         step()
-    info = vs.sync()
-    frame[0] = 0
-    launches_per_step = 1 + 2 * vs.grid_levels + 1  # init + (work scan + level pass) per level + render
+    for st in storages:
+        info = st.sync()
+    if not anim:  # (the animation runs on instead: every timed frame follows another frame)
+        frame[0] = 0
+    L = vs.grid_levels
+    launches_per_step = 1 + 2 * L + 1  # init + (work scan + level pass) per level + render
+    if reuse:
+        launches_per_step += 1 + (L - 1) + L  # match passes (root, each child level) + copy passes
 
     # ---- device-resident timing (value) -------------------------------------
     torch.cuda.synchronize()
@@ -308,24 +341,30 @@ def run_ours(args, world, rank, local):
     value = world * args.steps / (t_ms / 1e3)
 
     # ---- per-kernel timing of the dominant kernel (level passes) -----------
-    vs.set_profiling(True)
+    for st in storages:
+        st.set_profiling(True)
     level_ms = [0.0] * vs.grid_levels
     render_ms = 0.0
     reps = max(3, min(args.steps, 10))
     for _ in range(reps):
         flush.fill_(1)
-        vox.voxelize(tt[0], stream)
+        if not anim:
+            frame[0] = 0  # (the profiled voxelization is at tape time tt[0])
+        t, cur = voxelize_frame()
         rs, re_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         rs.record(stream)
-        rt.trace(scene.camera, tt[0], W, H, out=(rgba, None), stream=stream)
+        rt.trace(scene.camera, t, W, H, out=(rgba, None), stream=stream)
         re_.record(stream)
-        lt = vs.level_timings()
+        lt = cur.level_timings()
         torch.cuda.synchronize()
         level_ms = [a + b / reps for a, b in zip(level_ms, lt)]
         render_ms += rs.elapsed_time(re_) / reps
-    vs.set_profiling(False)
-    fp32_ops = vs.fp32_ops()   # of the profiled voxelization (tape time tt[0])
-    cell_instr = vs.work()
+    for st in storages:
+        st.set_profiling(False)
+    fp32_ops = cur.fp32_ops()   # of the last profiled voxelization (evaluated nodes only)
+    cell_instr = cur.work()
+    if not anim:
+        frame[0] = 0
 
     # ---- end to end through the public API with host buffers ---------------
     torch.cuda.synchronize()
@@ -333,9 +372,8 @@ def run_ours(args, world, rank, local):
     e2e_evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     for i, (s, e) in enumerate(e2e_evs):
         flush.fill_(1)
-        t = tt[i % len(tt)]
         s.record(stream)
-        vox.voxelize(t, stream)   # host tape -> device (pinned staging + H2D)
+        t, _ = voxelize_frame()   # host tape -> device (pinned staging + H2D)
         rt.trace(scene.camera, t, W, H, out=(rgba, None), stream=stream)
         host_img.copy_(rgba, non_blocking=True)  # result -> host
         e.record(stream)
@@ -373,6 +411,8 @@ def run_ours(args, world, rank, local):
                    "parallelism": f"replicas x{world}"},
         "roofline": roofline,
         "level_ms": level_ms, "render_ms": render_ms,
+        **({"reuse": {"previous_frame_tree": reuse,
+                      "cell_instr_per_level": cell_instr}} if anim else {}),
         "e2e": {"value": e2e_value, "unit": "scenes/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "clocks": clocks.summary(),
         "gpu_launches": launches_per_step * args.steps,
@@ -386,7 +426,8 @@ def run_ours(args, world, rank, local):
                                           f"{W}x{H} render {t_ren:.2f} s), oracle C++ port, {threads} threads"}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    vs.cleanup()
+    for st in storages:
+        st.cleanup()
     ctx.close()
 
 # ---- many-scene batch ----------------------------------------------------------------

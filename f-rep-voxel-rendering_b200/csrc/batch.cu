@@ -294,6 +294,7 @@ void mark_voxelized(frep_batch* b, const frep_tape* const* tapes, cudaStream_t s
     for (uint32_t i = 0; i < b->trees.size(); i++) {
         frep_tree* t = b->trees[i];
         t->voxelized = true;
+        t->reuse_last = false;
         t->stream = s;
         t->n_slots = std::max<uint32_t>(tapes[i]->ct.n_slots, 4);
         t->mm_cap = tapes[i]->ct.n_minmax;

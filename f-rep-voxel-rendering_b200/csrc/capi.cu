@@ -343,6 +343,7 @@ void frep_tree_destroy(frep_tree* t) {
         cudaFree(t->tapes);
     }
     cudaFree(t->keep);
+    cudaFree(t->reuse_src);
     if (t->staging) cudaFreeHost(t->staging);
     if (t->upload_done) cudaEventDestroy(t->upload_done);
     for (auto& e : t->ev)
@@ -376,10 +377,18 @@ frep_status ensure_plan(frep_tree* tree, const frep_tape* tape, const char* who)
 
 // Enqueues init + every level pass of one tree whose root tape is already at
 // word 0 of its pool. `plan` may narrow the grid (the static-scratch path).
+// With `prev`, nodes whose time-free tape equals prev's at the same place are
+// copied from it (reuse.cu): a match pass fixes every node's source before its
+// level pass, and a copy pass follows it.
 frep_status enqueue_tree_levels(frep_tree* tree, const frep_tape* tape, float tape_time, uint32_t* keep,
-                                frep::WarpScratch ws, const frep::LevelPlan& plan, cudaStream_t stream) {
+                                frep::WarpScratch ws, const frep::LevelPlan& plan, cudaStream_t stream,
+                                const frep_tree* prev = nullptr) {
     cudaError_t e = frep::launch_tree_init(tree->d_self, 1, nullptr, tape_time, stream);
     if (e != cudaSuccess) return cuda_fail(e, "tree_init_kernel");
+    if (prev) {
+        e = frep::launch_reuse_match(tree->hdr, prev->hdr, tree->reuse_src, 0, stream);
+        if (e != cudaSuccess) return cuda_fail(e, "reuse_match_kernel");
+    }
     const frep_grid& g = tree->grid;
     if (tree->profile) FREP_CUDA(cudaEventRecord(tree->ev[0], stream));
     frep::LevelLaunch a{};
@@ -392,6 +401,7 @@ frep_status enqueue_tree_levels(frep_tree* tree, const frep_tape* tape, float ta
     a.mm_ofs = ws.mm_ofs;
     a.n_slots = std::max<uint32_t>(tape->ct.n_slots, 4);
     a.mm_cap = std::max<uint32_t>(tape->ct.n_minmax, 1);
+    a.reuse_src = prev ? tree->reuse_src : nullptr;
     for (uint32_t l = 0; l < g.levels; l++) {
         const bool point = l == g.levels - 1;
         a.level = l;
@@ -402,9 +412,18 @@ frep_status enqueue_tree_levels(frep_tree* tree, const frep_tape* tape, float ta
         if (e != cudaSuccess) return cuda_fail(e, "level_scan_kernel");
         e = frep::launch_level(a, plan, (int)tree->opts.rounding, point, stream, ki);
         if (e != cudaSuccess) return cuda_fail(e, "level kernel");
+        if (prev) {
+            if (!point) {  // before the copies add children of their own
+                e = frep::launch_reuse_match(tree->hdr, prev->hdr, tree->reuse_src, l + 1, stream);
+                if (e != cudaSuccess) return cuda_fail(e, "reuse_match_kernel");
+            }
+            e = frep::launch_reuse_copy(tree->hdr, prev->hdr, tree->reuse_src, l, stream);
+            if (e != cudaSuccess) return cuda_fail(e, "reuse_copy_kernel");
+        }
         if (tree->profile) FREP_CUDA(cudaEventRecord(tree->ev[l + 1], stream));
     }
     tree->voxelized = true;
+    tree->reuse_last = prev != nullptr;
     return FREP_OK;
 }
 
@@ -412,10 +431,33 @@ frep_status enqueue_tree_levels(frep_tree* tree, const frep_tape* tape, float ta
 
 extern "C" {
 
-frep_status frep_voxelize(frep_ctx* ctx, frep_tree* tree, const frep_tape* tape, float tape_time,
-                          void* stream_ptr) {
+}  // extern "C"
+
+namespace {
+
+// Pools and grid that make a tree's subtrees interchangeable with prev's.
+frep_status check_reuse(const frep_tree* tree, const frep_tree* prev) {
+    if (prev == tree) return fail(FREP_ERR_INVALID_ARG, "frep_voxelize_reuse: prev is the tree being voxelized");
+    if (prev->ctx != tree->ctx) return fail(FREP_ERR_INVALID_ARG, "frep_voxelize_reuse: prev belongs to another context");
+    if (!prev->voxelized) return fail(FREP_ERR_INVALID_ARG, "frep_voxelize_reuse: prev has not been voxelized");
+    const frep_grid &a = tree->grid, &b = prev->grid;
+    bool same = a.levels == b.levels && a.world_size == b.world_size && tree->point_k == prev->point_k;
+    for (int k = 0; k < 3; k++) same = same && a.low_vertex[k] == b.low_vertex[k];
+    for (uint32_t l = 0; same && l < a.levels; l++) same = a.dims[l] == b.dims[l];
+    if (!same) return fail(FREP_ERR_INVALID_ARG, "frep_voxelize_reuse: prev has another grid");
+    if (tree->opts.rounding != prev->opts.rounding || tree->opts.shorten != prev->opts.shorten)
+        return fail(FREP_ERR_INVALID_ARG, "frep_voxelize_reuse: prev was built with other rounding / shortening");
+    return FREP_OK;
+}
+
+frep_status voxelize_impl(frep_ctx* ctx, frep_tree* tree, const frep_tree* prev, const frep_tape* tape,
+                          float tape_time, void* stream_ptr) {
     if (!ctx || !tree || !tape) return fail(FREP_ERR_INVALID_ARG, "frep_voxelize: null argument");
     if (tree->ctx != ctx) return fail(FREP_ERR_INVALID_ARG, "frep_voxelize: tree belongs to another context");
+    if (prev) {
+        frep_status rs = check_reuse(tree, prev);
+        if (rs != FREP_OK) return rs;
+    }
     cudaStream_t stream = (cudaStream_t)stream_ptr;
     FREP_CUDA(cudaSetDevice(ctx->device));
     const uint32_t n = (uint32_t)tape->ct.instrs.size();
@@ -445,6 +487,16 @@ frep_status frep_voxelize(frep_ctx* ctx, frep_tree* tree, const frep_tape* tape,
         tree->bytes += keep_words * 4;
         ctx->used += keep_words * 4;
     }
+    if (prev && !tree->reuse_src) {  // one entry per possible node (nodes are >= 8 words)
+        const uint64_t words = tree->node_cap / 8 + 1;
+        if (ctx->used + words * 4 > ctx->budget)
+            return fail(FREP_ERR_OOM, "frep_voxelize_reuse: side array of %llu bytes exceeds the budget",
+                        (unsigned long long)words * 4);
+        FREP_CUDA(cudaMalloc(&tree->reuse_src, words * 4));
+        tree->reuse_words = words;
+        tree->bytes += words * 4;
+        ctx->used += words * 4;
+    }
     // Root tape upload through pinned staging (reused once the previous copy is done).
     if (root_words > tree->staging_words) {
         if (tree->staging) {
@@ -466,7 +518,22 @@ frep_status frep_voxelize(frep_ctx* ctx, frep_tree* tree, const frep_tape* tape,
     tree->root_words = (uint32_t)root_words;
     tree->stream = stream;
 
-    return enqueue_tree_levels(tree, tape, tape_time, tree->keep, ws, tree->plan, stream);
+    return enqueue_tree_levels(tree, tape, tape_time, tree->keep, ws, tree->plan, stream, prev);
+}
+
+}  // namespace
+
+extern "C" {
+
+frep_status frep_voxelize(frep_ctx* ctx, frep_tree* tree, const frep_tape* tape, float tape_time,
+                          void* stream_ptr) {
+    return voxelize_impl(ctx, tree, nullptr, tape, tape_time, stream_ptr);
+}
+
+frep_status frep_voxelize_reuse(frep_ctx* ctx, frep_tree* tree, const frep_tree* prev, const frep_tape* tape,
+                                float tape_time, void* stream_ptr) {
+    if (!prev) return fail(FREP_ERR_INVALID_ARG, "frep_voxelize_reuse: null prev");
+    return voxelize_impl(ctx, tree, prev, tape, tape_time, stream_ptr);
 }
 
 frep_status frep_tree_sync(frep_tree* tree, frep_tree_info* info) {
@@ -539,7 +606,8 @@ frep_status frep_tree_fp32_ops(frep_tree* tree, uint64_t* ops) {
     for (uint32_t l = 0; l < g.levels; l++) {
         cudaError_t e = frep::launch_count_ops(tree->hdr, tree->nodes, tree->tapes, tree->node_cap, l,
                                                tree->node_size[l], g.dims[l] * g.dims[l] * g.dims[l],
-                                               l == g.levels - 1, tree->stream);
+                                               l == g.levels - 1, tree->reuse_last ? tree->reuse_src : nullptr,
+                                               tree->stream);
         if (e != cudaSuccess) return cuda_fail(e, "count_ops_kernel");
     }
     FREP_CUDA(cudaStreamSynchronize(tree->stream));

@@ -47,7 +47,26 @@ struct TreeHeader {
     unsigned long long fp32_ops[MAX_LEVELS];   // op-weighted FP32 work per level (count_ops_kernel)
     uint32_t overflow;                         // bit 0 node pool, bit 1 tape pool
     uint32_t status;                           // reserved for bounded-wait failures
+    uint32_t reuse_eval[MAX_LEVELS];           // reuse: nodes [0, n) of a level may need
+                                               //   evaluation; the rest are copies
 };
+
+__device__ __forceinline__ uint32_t level_count(const TreeHeader* H, uint32_t level,
+                                                unsigned long long node_cap, uint32_t node_size) {
+    // A pool overflow in the previous level may have counted children that
+    // were never written; only the ones that fit exist.
+    const unsigned long long ofs = H->node_ofs[level];
+    const unsigned long long cap = node_cap > ofs ? (node_cap - ofs) / node_size : 0;
+    return (uint32_t)min((unsigned long long)H->node_count[level], cap);
+}
+
+// Entry of a node in a tree's reuse side array (one u32 per node: the
+// previous tree's node it is copied from, or ~0). Nodes are at least 8 words
+// (dims are multiples of 4), so word offset / 8 is unique per node.
+__host__ __device__ inline unsigned long long reuse_slot(unsigned long long level_ofs, uint32_t node,
+                                                         uint32_t node_size) {
+    return (level_ofs + (unsigned long long)node * node_size) >> 3;
+}
 
 __host__ __device__ inline uint32_t node_words(uint32_t dim, bool last) {
     const uint32_t c3 = dim * dim * dim;       // node.comp:4-15
@@ -67,6 +86,9 @@ __device__ __forceinline__ uint32_t w_a(uint64_t w) { return (uint32_t)(w >> 32)
 __device__ __forceinline__ uint32_t w_b(uint64_t w) { return (uint32_t)(w >> 48); }
 __device__ __forceinline__ float w_const(uint64_t w) { return __uint_as_float((uint32_t)(w >> 32)); }
 __device__ __forceinline__ bool is_mm(uint32_t op) { return op == OP_MIN || op == OP_MAX; }
+__host__ __device__ constexpr bool is_binary(uint32_t op) {
+    return op == OP_ADD || op == OP_SUB || op == OP_MUL || op == OP_DIV || op == OP_MIN || op == OP_MAX;
+}
 
 // glm's min/max selection rules (the oracle uses the same selects).
 __device__ __forceinline__ float min_sel(float a, float b) { return (b < a) ? b : a; }

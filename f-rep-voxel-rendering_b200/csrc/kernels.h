@@ -24,6 +24,9 @@ struct LevelLaunch {
     uint32_t n_slots;                  // slot-file rows per lane (max over the batch)
     uint32_t mm_cap;                   // MIN/MAX choice entries per warp (max over the batch)
     uint32_t smem_per_warp;            // bytes (set by launch_level from the plan)
+    const uint32_t* reuse_src;         // one-tree launches that copy subtrees from a previous
+                                       //   tree: nodes whose entry is not ~0 are skipped
+                                       //   (reuse_slot); null = evaluate every node
 };
 
 // Per-warp global scratch of the interval pass, in u32 words: one keep mask per
@@ -82,11 +85,22 @@ cudaError_t launch_level_scan(const LevelLaunch& a, bool point, int point_k, cud
 cudaError_t launch_level(const LevelLaunch& a, const LevelPlan& plan, int rounding, bool point,
                          cudaStream_t stream, int interval_ki = 0);
 
+// Reuse of a previous tree (reuse.cu), one tree per launch; src is the tree's
+// side array (one u32 per node, indexed by reuse_slot).
+// match: entries of the nodes of `level` present now (previous node id or ~0).
+// copy: the nodes of `level` with an entry are copied from `prev`, with their
+// children (entries set to the previous children).
+cudaError_t launch_reuse_match(dev::TreeHeader* hdr, const dev::TreeHeader* prev, uint32_t* src, uint32_t level,
+                               cudaStream_t stream);
+cudaError_t launch_reuse_copy(dev::TreeHeader* hdr, const dev::TreeHeader* prev, uint32_t* src, uint32_t level,
+                              cudaStream_t stream);
+
 // Op-weighted work of every node of `level` (interval or point weights),
 // added to the header's fp32_ops[level].
+// Nodes with a `skip` entry other than ~0 (copied, not evaluated) are left out.
 cudaError_t launch_count_ops(dev::TreeHeader* hdr, const uint32_t* nodes, const uint64_t* tapes,
                              unsigned long long node_cap, uint32_t level, uint32_t node_size,
-                             uint32_t cells, bool point, cudaStream_t stream);
+                             uint32_t cells, bool point, const uint32_t* skip, cudaStream_t stream);
 
 struct RenderArgs {
     const dev::TreeHeader* hdr;

@@ -70,10 +70,6 @@ __device__ __forceinline__ void sts_f4(uint32_t a, float4 v) {
 // register holding that result instead of loading the slot row.
 constexpr uint32_t F_FWD_A = 1u << 4, F_FWD_B = 1u << 5;
 
-__host__ __device__ constexpr bool is_binary(uint32_t op) {
-    return op == OP_ADD || op == OP_SUB || op == OP_MUL || op == OP_DIV || op == OP_MIN || op == OP_MAX;
-}
-
 __device__ __forceinline__ uint4 decode(uint64_t w, uint32_t prev_out, uint32_t row_bytes) {
     const uint32_t op = w_op(w);
     const uint32_t stride = 32u * row_bytes;
@@ -108,15 +104,6 @@ __device__ __forceinline__ uint32_t fetch_items(unsigned long long* cursor, unsi
 __device__ __forceinline__ uint32_t chunk_for(unsigned long long total, uint32_t grid_warps) {
     unsigned long long c = total / ((unsigned long long)grid_warps * 8ull);
     return (uint32_t)max(1ull, min(c, 32ull));
-}
-
-__device__ __forceinline__ uint32_t level_count(const TreeHeader* H, uint32_t level,
-                                                unsigned long long node_cap, uint32_t node_size) {
-    // A pool overflow in the previous level may have counted children that
-    // were never written; only the ones that fit exist.
-    const unsigned long long ofs = H->node_ofs[level];
-    const unsigned long long cap = node_cap > ofs ? (node_cap - ofs) / node_size : 0;
-    return (uint32_t)min((unsigned long long)H->node_count[level], cap);
 }
 
 // Largest tree index i with prefix[i] <= item (prefix[0] = 0 <= item < prefix[n]).
@@ -357,6 +344,8 @@ interval_level_kernel(LevelLaunch p) {
             const uint32_t groups = words / KI;           // items per node
             const unsigned long long local = item - t_lo;
             const uint32_t node = (uint32_t)(local / groups), grp = (uint32_t)(local % groups);
+            if (p.reuse_src && __ldcg(&p.reuse_src[reuse_slot(T.ofs_l, node, T.node_size)]) != 0xFFFFFFFFu)
+                continue;  // copied from the previous tree by reuse_copy_kernel
             uint32_t* rec = T.nodes + T.ofs_l + (size_t)node * T.node_size;
             const uint32_t tape_idx = rec[0];
             const uint32_t ncx = rec[1], ncy = rec[2], ncz = rec[3];
@@ -883,6 +872,8 @@ point_level_kernel(LevelLaunch p) {
             const float cs = T.cs;
             const unsigned long long local = item - t_lo;
             const uint32_t node = (uint32_t)(local / groups), grp = (uint32_t)(local % groups);
+            if (p.reuse_src && __ldcg(&p.reuse_src[reuse_slot(T.ofs_l, node, T.node_size)]) != 0xFFFFFFFFu)
+                continue;  // copied from the previous tree by reuse_copy_kernel
             uint32_t* rec = T.nodes + T.ofs_l + (size_t)node * T.node_size;
             const uint32_t tape_idx = rec[0];
             const uint64_t* tape = T.tapes + tape_idx + 1;
@@ -963,7 +954,7 @@ point_level_kernel(LevelLaunch p) {
 // cells per lane). Interval passes also fix where each tree's next level
 // starts (node_ofs[level + 1]). One block.
 __device__ __forceinline__ unsigned long long level_items(TreeHeader* H, uint32_t L, int point, int k,
-                                                          bool write_ofs) {
+                                                          bool write_ofs, bool reuse) {
     if (L >= H->levels) return 0;
     const bool last = L == H->levels - 1;
     if ((point != 0) != last) return 0;
@@ -972,18 +963,20 @@ __device__ __forceinline__ unsigned long long level_items(TreeHeader* H, uint32_
     if (point && H->point_k != (uint32_t)k) return 0;
     const uint32_t count = level_count(H, L, H->node_cap, H->node_size[L]);
     if (!point && write_ofs) H->node_ofs[L + 1] = H->node_ofs[L] + (unsigned long long)count * H->node_size[L];
-    return (unsigned long long)count * (words / (uint32_t)k);  // k: cells per lane of the pass
+    // with reuse, the nodes past reuse_eval[L] were added by copies: no items
+    const uint32_t evaluated = reuse ? min(count, H->reuse_eval[L]) : count;
+    return (unsigned long long)evaluated * (words / (uint32_t)k);  // k: cells per lane of the pass
 }
 
 __global__ void __launch_bounds__(1024)
 level_scan_kernel(TreeHeader* const* trees, uint32_t n, uint32_t L, int point, int point_k,
-                  unsigned long long* prefix, unsigned long long* cursor) {
+                  unsigned long long* prefix, unsigned long long* cursor, int reuse) {
     __shared__ unsigned long long part[1024];
     const uint32_t t = threadIdx.x, T = blockDim.x;
     const uint32_t per = (n + T - 1) / T;
     const uint32_t b = min(n, t * per), e = min(n, b + per);
     unsigned long long sum = 0;
-    for (uint32_t i = b; i < e; i++) sum += level_items(trees[i], L, point, point_k, true);
+    for (uint32_t i = b; i < e; i++) sum += level_items(trees[i], L, point, point_k, true, reuse != 0);
     part[t] = sum;
     __syncthreads();
     for (uint32_t off = 1; off < T; off <<= 1) {  // inclusive scan
@@ -995,7 +988,7 @@ level_scan_kernel(TreeHeader* const* trees, uint32_t n, uint32_t L, int point, i
     unsigned long long run = part[t] - sum;
     for (uint32_t i = b; i < e; i++) {
         prefix[i] = run;
-        run += level_items(trees[i], L, point, point_k, false);
+        run += level_items(trees[i], L, point, point_k, false, reuse != 0);
     }
     if (t == T - 1) prefix[n] = part[t];
     if (t == 0) *cursor = 0ull;
@@ -1086,7 +1079,7 @@ __global__ void gather_usage_kernel(TreeHeader* const* trees, uint32_t n, unsign
 // with the interval weights (interior levels) or the point weights (last level).
 __global__ void count_ops_kernel(TreeHeader* H, const uint32_t* nodes, const uint64_t* tapes,
                                  unsigned long long node_cap, uint32_t level, uint32_t node_size,
-                                 uint32_t cells, int point) {
+                                 uint32_t cells, int point, const uint32_t* skip) {
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t count = level_count(H, level, node_cap, node_size);
     const unsigned long long ofs = H->node_ofs[level];
@@ -1094,6 +1087,7 @@ __global__ void count_ops_kernel(TreeHeader* H, const uint32_t* nodes, const uin
     unsigned long long sum = 0;
     for (uint32_t node = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); node < count;
          node += gridDim.x * (blockDim.x / 32)) {
+        if (skip && skip[reuse_slot(ofs, node, node_size)] != 0xFFFFFFFFu) continue;
         const uint32_t tidx = nodes[ofs + (size_t)node * node_size];
         const uint32_t n = (uint32_t)tapes[tidx];
         uint32_t s = 0;
@@ -1205,7 +1199,7 @@ cudaError_t launch_tree_init_staged(dev::TreeHeader* const* trees, uint32_t n, c
 
 cudaError_t launch_level_scan(const LevelLaunch& a, bool point, int point_k, cudaStream_t stream) {
     dev::level_scan_kernel<<<1, 1024, 0, stream>>>(a.trees, a.n_trees, a.level, point ? 1 : 0, point_k, a.prefix,
-                                                   a.cursor);
+                                                   a.cursor, a.reuse_src ? 1 : 0);
     return cudaGetLastError();
 }
 
@@ -1261,9 +1255,9 @@ cudaError_t launch_gather_usage(dev::TreeHeader* const* trees, uint32_t n, unsig
 
 cudaError_t launch_count_ops(dev::TreeHeader* hdr, const uint32_t* nodes, const uint64_t* tapes,
                              unsigned long long node_cap, uint32_t level, uint32_t node_size,
-                             uint32_t cells, bool point, cudaStream_t stream) {
+                             uint32_t cells, bool point, const uint32_t* skip, cudaStream_t stream) {
     dev::count_ops_kernel<<<1184, 256, 0, stream>>>(hdr, nodes, tapes, node_cap, level, node_size, cells,
-                                                    point ? 1 : 0);
+                                                    point ? 1 : 0, skip);
     return cudaGetLastError();
 }
 

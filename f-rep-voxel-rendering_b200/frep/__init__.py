@@ -299,10 +299,17 @@ class Voxelizer:
         self.ctx = ctx
         self.voxels = voxels
 
-    def voxelize(self, tape_time: float = 0.0, stream=None) -> None:
-        """Enqueues every level pass on `stream`; no host round trip per level."""
-        L.check(L.lib().frep_voxelize(self.ctx._h, self.voxels.tree, self.voxels.tape.handle,
-                                      float(tape_time), _stream_ptr(stream)))
+    def voxelize(self, tape_time: float = 0.0, stream=None, reuse: "VoxelStorage | None" = None) -> None:
+        """Enqueues every level pass on `stream`; no host round trip per level.
+        reuse: a VoxelStorage of the same grid voxelized earlier (the previous
+        frame); subtrees whose tape does not read the time and matches it are
+        copied from it instead of evaluated (frep_voxelize_reuse)."""
+        if reuse is None:
+            L.check(L.lib().frep_voxelize(self.ctx._h, self.voxels.tree, self.voxels.tape.handle,
+                                          float(tape_time), _stream_ptr(stream)))
+        else:
+            L.check(L.lib().frep_voxelize_reuse(self.ctx._h, self.voxels.tree, reuse.tree, self.voxels.tape.handle,
+                                                float(tape_time), _stream_ptr(stream)))
 
     def print_stats(self) -> None:
         info = self.voxels.sync()
@@ -313,6 +320,36 @@ class Voxelizer:
             cnt = max(info.node_count[i], 1)
             print(f"\t{i}: nodes={info.node_count[i]}  avg tape={info.tape_size_sum[i] / cnt:.1f}"
                   f"  max tape={info.tape_size_max[i]}")
+
+
+class AnimatedVoxelizer:
+    """Re-voxelizes a time-dependent shape every frame (the reference's
+    real-time mode, application.cpp:68-79) into two alternating trees, each
+    frame reusing the time-independent subtrees of the previous one.
+    `voxelize(t)` returns the VoxelStorage holding frame t; a Raytracer follows
+    it through `raytracer.voxels = ...`."""
+
+    def __init__(self, ctx: Context, make_storage, shape):
+        """make_storage: a callable returning a new (un-initialised) VoxelStorage."""
+        self.ctx = ctx
+        tape = shape if isinstance(shape, Tape) else Tape(shape)
+        self.storages = [make_storage().init(ctx, tape), make_storage().init(ctx, tape)]
+        self.frame = 0
+
+    @property
+    def current(self) -> VoxelStorage:
+        return self.storages[(self.frame - 1) % 2]
+
+    def voxelize(self, tape_time: float, stream=None) -> VoxelStorage:
+        vs = self.storages[self.frame % 2]
+        prev = self.storages[(self.frame - 1) % 2] if self.frame > 0 else None
+        Voxelizer(self.ctx, vs).voxelize(tape_time, stream=stream, reuse=prev)
+        self.frame += 1
+        return vs
+
+    def cleanup(self) -> None:
+        for s in self.storages:
+            s.cleanup()
 
 
 @dataclass

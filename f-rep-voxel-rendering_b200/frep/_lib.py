@@ -124,6 +124,7 @@ _SIGS = {
     "frep_tree_create": (C.c_int, [_P, C.POINTER(Grid), C.POINTER(VoxelizeOpts), C.POINTER(_P)]),
     "frep_tree_destroy": (None, [_P]),
     "frep_voxelize": (C.c_int, [_P, _P, _P, C.c_float, _P]),
+    "frep_voxelize_reuse": (C.c_int, [_P, _P, _P, _P, C.c_float, _P]),
     "frep_voxelize_static_scratch": (C.c_int, [_P, _P, _P, C.c_float, _P]),
     "frep_tree_sync": (C.c_int, [_P, C.POINTER(TreeInfo)]),
     "frep_tree_work": (C.c_int, [_P, _P]),

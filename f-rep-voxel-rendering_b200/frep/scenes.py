@@ -11,6 +11,8 @@ slab boxes as in vulkan/src/csg/lib.cpp:117-148):
                         smooth-min (the large single-scene config)
 * ``gyroid_stress``   — twisted gyroid lattice clipped to a box and smooth-
                         unioned with spheres (the stress config)
+* ``animated_csg``    — random_csg plus spheres orbiting with T (a static part
+                        and a moving part, for re-voxelization with reuse)
 
 Every scene also carries its grid and camera so that a workload is one object.
 """
@@ -134,6 +136,29 @@ def random_csg(n: int = 256, seed: int = 2, grid_dims=(16, 16, 8), width: int = 
                  fov_deg=60.0)
     return Scene("random_csg", shape, list(grid_dims), (-1.25, -1.25, -1.25), 2.5, cam, width, height,
                  shadow_mask=1 if shadows else 0, meta={"n": n, "seed": seed})
+
+
+def animated_csg(n: int = 256, n_moving: int = 4, seed: int = 2, grid_dims=(16, 16, 8), width: int = 1920,
+                 height: int = 1080, shadows: bool = True) -> Scene:
+    """A scene with a static part and a moving part: random_csg(n, seed) (the
+    static part) min-unioned with n_moving spheres (radii U[0.08, 0.15]) that
+    orbit the z axis, sphere i on a circle of radius U[0.4, 1.0] at height
+    U[-0.6, 0.6], at angle 2 pi T + phase_i (one revolution per unit of T).
+    At a given T only the cells near a sphere keep it in their shortened tape;
+    every other cell's tape is the static part's, independent of T."""
+    base = random_csg(n, seed, grid_dims, width, height, shadows)
+    rng = np.random.default_rng(seed + 7919)
+    shape = base.shape
+    for _ in range(n_moving):
+        r, z0 = float(rng.uniform(0.4, 1.0)), float(rng.uniform(-0.6, 0.6))
+        phase, rad = float(rng.uniform(0.0, 2.0 * np.pi)), float(rng.uniform(0.08, 0.15))
+        ang = f32(2.0 * np.pi) * T() + f32(phase)
+        ball = Sqrt(Square(X() - f32(r) * Cos(ang)) + Square(Y() - f32(r) * Sin(ang)) + Square(Z() - z0)) - rad
+        shape = Min(shape, ball)
+    base.name = "animated_csg"
+    base.shape = shape
+    base.meta = {"n": n, "n_moving": n_moving, "seed": seed}
+    return base
 
 
 # ---- the reference's demo shapes (vulkan/src/shapes.cpp:5-117) ---------------------

@@ -187,6 +187,28 @@ void frep_tree_destroy(frep_tree* tree);
 frep_status frep_voxelize(frep_ctx* ctx, frep_tree* tree, const frep_tape* tape, float tape_time,
                           void* stream);
 
+/* Animated scenes: the same voxelization as frep_voxelize (the same nodes,
+ * masks and tape contents), built faster by copying from `prev` (the previous
+ * frame's tree) every subtree whose node tape never reads the time input and
+ * is identical to prev's node tape at the same level and coordinates; only the
+ * time-dependent part is evaluated again. Replaces the reference's full
+ * re-voxelization per frame (Application::Draw, application.cpp:68-79).
+ *   - prev: another tree of the same context, same grid, rounding and
+ *     shortening, voxelized before (any tape and time; a subtree is copied only
+ *     when its tape matches exactly). Its voxelization must be ordered before
+ *     this call's work (the same stream, or synchronized), and prev must not be
+ *     voxelized again until this call's work is done. A prev whose pools
+ *     overflowed is not used (everything is evaluated).
+ *   - Typical use: two trees A and B alternate, frame k voxelizes into one
+ *     with the other as prev.
+ *   - The first call allocates a side array of node_words / 8 + 1 u32 for the
+ *     tree (one entry per node: where it was copied from).
+ *   - frep_tree_work and frep_tree_fp32_ops count only the evaluated nodes.
+ * FREP_ERR_INVALID_ARG: prev null, equal to tree, not voxelized, or with
+ * another grid / options. */
+frep_status frep_voxelize_reuse(frep_ctx* ctx, frep_tree* tree, const frep_tree* prev, const frep_tape* tape,
+                                float tape_time, void* stream);
+
 /* Same voxelization as frep_voxelize, for callers that cannot allocate device
  * memory when they voxelize (a fixed budget reserved up front, a frame loop
  * that must not hit cudaMalloc's implicit synchronisation, or an application
