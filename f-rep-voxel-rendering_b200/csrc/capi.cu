@@ -386,7 +386,7 @@ frep_status enqueue_tree_levels(frep_tree* tree, const frep_tape* tape, float ta
     cudaError_t e = frep::launch_tree_init(tree->d_self, 1, nullptr, tape_time, stream);
     if (e != cudaSuccess) return cuda_fail(e, "tree_init_kernel");
     if (prev) {
-        e = frep::launch_reuse_match(tree->hdr, prev->hdr, tree->reuse_src, 0, stream);
+        e = frep::launch_reuse_match(tree->hdr, prev->hdr, tree->reuse_src, tree->reuse_list, 0, stream);
         if (e != cudaSuccess) return cuda_fail(e, "reuse_match_kernel");
     }
     const frep_grid& g = tree->grid;
@@ -401,7 +401,7 @@ frep_status enqueue_tree_levels(frep_tree* tree, const frep_tape* tape, float ta
     a.mm_ofs = ws.mm_ofs;
     a.n_slots = std::max<uint32_t>(tape->ct.n_slots, 4);
     a.mm_cap = std::max<uint32_t>(tape->ct.n_minmax, 1);
-    a.reuse_src = prev ? tree->reuse_src : nullptr;
+    a.eval_list = prev ? tree->reuse_list : nullptr;
     for (uint32_t l = 0; l < g.levels; l++) {
         const bool point = l == g.levels - 1;
         a.level = l;
@@ -414,7 +414,8 @@ frep_status enqueue_tree_levels(frep_tree* tree, const frep_tape* tape, float ta
         if (e != cudaSuccess) return cuda_fail(e, "level kernel");
         if (prev) {
             if (!point) {  // before the copies add children of their own
-                e = frep::launch_reuse_match(tree->hdr, prev->hdr, tree->reuse_src, l + 1, stream);
+                e = frep::launch_reuse_match(tree->hdr, prev->hdr, tree->reuse_src, tree->reuse_list, l + 1,
+                                             stream);
                 if (e != cudaSuccess) return cuda_fail(e, "reuse_match_kernel");
             }
             e = frep::launch_reuse_copy(tree->hdr, prev->hdr, tree->reuse_src, l, stream);
@@ -487,15 +488,16 @@ frep_status voxelize_impl(frep_ctx* ctx, frep_tree* tree, const frep_tree* prev,
         tree->bytes += keep_words * 4;
         ctx->used += keep_words * 4;
     }
-    if (prev && !tree->reuse_src) {  // one entry per possible node (nodes are >= 8 words)
+    if (prev && !tree->reuse_src) {  // one entry per possible node (nodes are >= 8 words), twice
         const uint64_t words = tree->node_cap / 8 + 1;
-        if (ctx->used + words * 4 > ctx->budget)
-            return fail(FREP_ERR_OOM, "frep_voxelize_reuse: side array of %llu bytes exceeds the budget",
-                        (unsigned long long)words * 4);
-        FREP_CUDA(cudaMalloc(&tree->reuse_src, words * 4));
+        if (ctx->used + words * 8 > ctx->budget)
+            return fail(FREP_ERR_OOM, "frep_voxelize_reuse: side arrays of %llu bytes exceed the budget",
+                        (unsigned long long)words * 8);
+        FREP_CUDA(cudaMalloc(&tree->reuse_src, words * 8));
+        tree->reuse_list = tree->reuse_src + words;
         tree->reuse_words = words;
-        tree->bytes += words * 4;
-        ctx->used += words * 4;
+        tree->bytes += words * 8;
+        ctx->used += words * 8;
     }
     // Root tape upload through pinned staging (reused once the previous copy is done).
     if (root_words > tree->staging_words) {

@@ -94,10 +94,12 @@ struct frep_tree {
     cudaStream_t stream = nullptr;
     bool voxelized = false;
     bool profile = false;
-    // reuse of a previous tree (frep_voxelize_reuse): one u32 per node
-    // (reuse_slot), allocated on first use; reuse_last: the last voxelization
-    // copied the nodes whose entry is set
+    // reuse of a previous tree (frep_voxelize_reuse), allocated on first use:
+    // reuse_src one u32 per node (reuse_slot), reuse_list the nodes of a level
+    // to evaluate (reuse_words entries each); reuse_last: the last
+    // voxelization copied the nodes whose entry is set
     uint32_t* reuse_src = nullptr;
+    uint32_t* reuse_list = nullptr;
     uint64_t reuse_words = 0;
     bool reuse_last = false;
     cudaEvent_t ev[FREP_MAX_LEVELS + 1] = {};

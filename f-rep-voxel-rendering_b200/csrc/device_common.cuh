@@ -47,8 +47,8 @@ struct TreeHeader {
     unsigned long long fp32_ops[MAX_LEVELS];   // op-weighted FP32 work per level (count_ops_kernel)
     uint32_t overflow;                         // bit 0 node pool, bit 1 tape pool
     uint32_t status;                           // reserved for bounded-wait failures
-    uint32_t reuse_eval[MAX_LEVELS];           // reuse: nodes [0, n) of a level may need
-                                               //   evaluation; the rest are copies
+    uint32_t reuse_eval[MAX_LEVELS];           // reuse: nodes of each level listed for
+                                               //   evaluation (the others are copies)
 };
 
 __device__ __forceinline__ uint32_t level_count(const TreeHeader* H, uint32_t level,

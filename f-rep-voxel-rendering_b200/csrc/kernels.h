@@ -24,9 +24,9 @@ struct LevelLaunch {
     uint32_t n_slots;                  // slot-file rows per lane (max over the batch)
     uint32_t mm_cap;                   // MIN/MAX choice entries per warp (max over the batch)
     uint32_t smem_per_warp;            // bytes (set by launch_level from the plan)
-    const uint32_t* reuse_src;         // one-tree launches that copy subtrees from a previous
-                                       //   tree: nodes whose entry is not ~0 are skipped
-                                       //   (reuse_slot); null = evaluate every node
+    const uint32_t* eval_list;         // one-tree launches that copy subtrees from a previous
+                                       //   tree: the nodes to evaluate (reuse_eval[level] of
+                                       //   them, listed by reuse_match_kernel); null = all
 };
 
 // Per-warp global scratch of the interval pass, in u32 words: one keep mask per
@@ -87,11 +87,12 @@ cudaError_t launch_level(const LevelLaunch& a, const LevelPlan& plan, int roundi
 
 // Reuse of a previous tree (reuse.cu), one tree per launch; src is the tree's
 // side array (one u32 per node, indexed by reuse_slot).
-// match: entries of the nodes of `level` present now (previous node id or ~0).
+// match: entries of the nodes of `level` present now (previous node id or ~0);
+// the nodes left to evaluate are appended to `list` (count: reuse_eval[level]).
 // copy: the nodes of `level` with an entry are copied from `prev`, with their
 // children (entries set to the previous children).
-cudaError_t launch_reuse_match(dev::TreeHeader* hdr, const dev::TreeHeader* prev, uint32_t* src, uint32_t level,
-                               cudaStream_t stream);
+cudaError_t launch_reuse_match(dev::TreeHeader* hdr, const dev::TreeHeader* prev, uint32_t* src, uint32_t* list,
+                               uint32_t level, cudaStream_t stream);
 cudaError_t launch_reuse_copy(dev::TreeHeader* hdr, const dev::TreeHeader* prev, uint32_t* src, uint32_t level,
                               cudaStream_t stream);
 

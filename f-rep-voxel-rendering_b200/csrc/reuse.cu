@@ -16,7 +16,8 @@
 //                       the previous tree's node at the same coordinates (a
 //                       descent from its root) and compare tapes; the side
 //                       array entry becomes that node's id, or ~0;
-//   level pass          evaluates the nodes whose entry is ~0;
+//                       nodes left to evaluate are listed for the level pass;
+//   level pass          evaluates the listed nodes (entry ~0);
 //   reuse_copy_kernel   the nodes whose entry is set: masks from the previous
 //                       node; each interior cell gets a new child whose tape is
 //                       copied (tapes shared within a 32-cell group stay
@@ -95,13 +96,12 @@ __device__ bool same_time_free_tape(const uint64_t* A, uint32_t a, const uint64_
 // Side-array entries of every node of level L present now (children of
 // evaluated parents; the root for L = 0).
 __global__ void __launch_bounds__(128) reuse_match_kernel(TreeHeader* H, const TreeHeader* P, uint32_t* src,
-                                                          uint32_t L) {
+                                                          uint32_t* list, uint32_t L) {
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t count = level_count(H, L, H->node_cap, H->node_size[L]);
     const unsigned long long ofs = H->node_ofs[L];
     const uint32_t size = H->node_size[L];
     const bool prev_ok = P->overflow == 0u && P->levels == H->levels;
-    if (blockIdx.x == 0 && threadIdx.x == 0) H->reuse_eval[L] = count;  // later nodes are copies
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
     for (uint32_t node = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); node < count; node += warps) {
         const uint32_t* rec = H->nodes + ofs + (size_t)node * size;
@@ -116,7 +116,10 @@ __global__ void __launch_bounds__(128) reuse_match_kernel(TreeHeader* H, const T
                     from = pn;
             }
         }
-        if (lane == 0) src[reuse_slot(ofs, node, size)] = from;
+        if (lane == 0) {
+            src[reuse_slot(ofs, node, size)] = from;
+            if (from == NONE) list[atomicAdd(&H->reuse_eval[L], 1u)] = node;  // to evaluate
+        }
     }
 }
 
@@ -258,9 +261,9 @@ static uint32_t reuse_blocks() {
     return (uint32_t)(sms > 0 ? sms : 1) * 8u;
 }
 
-cudaError_t launch_reuse_match(dev::TreeHeader* hdr, const dev::TreeHeader* prev, uint32_t* src, uint32_t level,
-                               cudaStream_t stream) {
-    dev::reuse_match_kernel<<<reuse_blocks(), 128, 0, stream>>>(hdr, prev, src, level);
+cudaError_t launch_reuse_match(dev::TreeHeader* hdr, const dev::TreeHeader* prev, uint32_t* src, uint32_t* list,
+                               uint32_t level, cudaStream_t stream) {
+    dev::reuse_match_kernel<<<reuse_blocks(), 128, 0, stream>>>(hdr, prev, src, list, level);
     return cudaGetLastError();
 }
 

@@ -269,6 +269,102 @@ __device__ __forceinline__ IVK<KI> iv_exec(const uint4 d, uint32_t lane_base, ui
     return r;
 }
 
+// Backward liveness walk of one item's cells over a tape of at most 64 slots
+// (shorten.comp:148-186): lane l keeps, for each of its KI cells, the set of
+// live slots as a 64-bit mask. From the last instruction down, an instruction
+// is kept where its output slot is live; the output then dies and the inputs
+// its choice uses (both for arithmetic, the chosen ones for MIN/MAX, none for
+// CONST) become live. Writes the kept masks of the tape (one ballot per
+// instruction and cell group) to keep[], and counts kept instructions and the
+// grouping signature per cell.
+//
+// U, the union of every cell's live set, is kept exact alongside: an
+// instruction whose output is not in U is dead for all the warp's cells and
+// changes nothing, so each step jumps (one ballot) straight to the next
+// instruction of the chunk whose output is in U. Long tapes of which each cell
+// keeps a few percent (the root level) skip most instructions.
+template <int KI>
+__device__ __forceinline__ void walk_regs(const uint64_t* tape, uint32_t n, int mm, const uint2* mmb,
+                                          uint32_t* keep, const uint32_t (&ok_w)[KI], uint32_t lane,
+                                          uint32_t (&kept)[KI], uint32_t (&sig)[KI]) {
+    uint64_t lv[KI];
+    uint32_t any_ok = 0;
+#pragma unroll
+    for (int h = 0; h < KI; h++) {
+        lv[h] = (ok_w[h] >> lane) & 1u;  // slot 0 (the result) is live
+        any_ok |= ok_w[h];
+    }
+    uint64_t U = any_ok ? 1ull : 0ull;
+    int mm_top = mm;  // MIN/MAX instructions before the current chunk's end
+    for (int hi = (int)n; hi > 0; hi -= 32) {
+        const int lo = max(0, hi - 32);
+        const int m = hi - lo;
+        // lane j holds instruction lo + j (packed: out | a << 6 | b << 12 | op
+        // << 18) and, for a MIN/MAX, its choices
+        const uint64_t mine = (int)lane < m ? __ldcg(&tape[lo + lane]) : 0ull;
+        const uint32_t pk = (w_out(mine) & 63u) | (w_a(mine) & 63u) << 6 | (w_b(mine) & 63u) << 12 |
+                            w_op(mine) << 18;
+        const bool ism = (int)lane < m && is_mm(w_op(mine));
+        const uint32_t mball = __ballot_sync(0xFFFFFFFFu, ism);
+        const int mbase = mm_top - __popc(mball);
+        uint2 cb[KI];
+#pragma unroll
+        for (int h = 0; h < KI; h++)
+            cb[h] = ism ? mmb[(mbase + __popc(mball & lanemask_lt())) * KI + h] : make_uint2(0u, 0u);
+        uint32_t my_keep[KI];
+#pragma unroll
+        for (int h = 0; h < KI; h++) my_keep[h] = 0;
+        int j = m - 1;
+        while (j >= 0) {
+            const uint32_t cand = __ballot_sync(0xFFFFFFFFu, (int)lane <= j && ((U >> (pk & 63u)) & 1ull));
+            if (!cand) break;
+            j = 31 - __clz(cand);
+            const uint32_t q = __shfl_sync(0xFFFFFFFFu, pk, j);
+            const uint32_t o = q & 63u, a = (q >> 6) & 63u, b = (q >> 12) & 63u, op = q >> 18;
+            const bool arith = op == OP_ADD || op == OP_SUB || op == OP_MUL || op == OP_DIV;
+            const bool mmop = is_mm(op);
+            uint32_t fany = 0, sany = 0;
+#pragma unroll
+            for (int h = 0; h < KI; h++) {
+                const uint32_t k = (uint32_t)(lv[h] >> o) & 1u;
+                const uint32_t kb = __ballot_sync(0xFFFFFFFFu, k);
+                uint32_t f, sc;
+                if (mmop) {
+                    f = (__shfl_sync(0xFFFFFFFFu, cb[h].x, j) >> lane) & 1u;
+                    sc = (__shfl_sync(0xFFFFFFFFu, cb[h].y, j) >> lane) & 1u;
+                } else {
+                    f = op != OP_CONST;
+                    sc = arith;
+                }
+                f &= k;
+                sc &= k;
+                lv[h] &= ~(1ull << o);
+                if (f) lv[h] |= 1ull << a;
+                if (sc) lv[h] |= 1ull << b;
+                kept[h] += k;
+                sig[h] += (k + f + 2u * sc) * (uint32_t)(lo + j + 1) * 0x9E3779B1u;
+                if ((int)lane == j) my_keep[h] = kb;
+                if (mmop) {
+                    fany |= __ballot_sync(0xFFFFFFFFu, f);
+                    sany |= __ballot_sync(0xFFFFFFFFu, sc);
+                } else {  // the output is live in some cell: so are the inputs it reads
+                    fany |= op != OP_CONST;
+                    sany |= arith;
+                }
+            }
+            U &= ~(1ull << o);
+            if (fany) U |= 1ull << a;
+            if (sany) U |= 1ull << b;
+            j--;
+        }
+        if ((int)lane < m) {
+            if constexpr (KI == 1) keep[lo + lane] = my_keep[0];
+            else reinterpret_cast<uint2*>(keep)[lo + lane] = make_uint2(my_keep[0], my_keep[1]);
+        }
+        mm_top = mbase;
+    }
+}
+
 // ---- interval level pass -------------------------------------------------------
 //
 // A work item is KI whole mask words of a node (32 * KI cells); lane l
@@ -343,9 +439,9 @@ interval_level_kernel(LevelLaunch p) {
             const uint32_t words = dim * dim * dim / 32;  // mask words per node
             const uint32_t groups = words / KI;           // items per node
             const unsigned long long local = item - t_lo;
-            const uint32_t node = (uint32_t)(local / groups), grp = (uint32_t)(local % groups);
-            if (p.reuse_src && __ldcg(&p.reuse_src[reuse_slot(T.ofs_l, node, T.node_size)]) != 0xFFFFFFFFu)
-                continue;  // copied from the previous tree by reuse_copy_kernel
+            const uint32_t grp = (uint32_t)(local % groups);
+            uint32_t node = (uint32_t)(local / groups);
+            if (p.eval_list) node = __ldcg(&p.eval_list[node]);  // the others are copies
             uint32_t* rec = T.nodes + T.ofs_l + (size_t)node * T.node_size;
             const uint32_t tape_idx = rec[0];
             const uint32_t ncx = rec[1], ncy = rec[2], ncz = rec[3];
@@ -448,18 +544,7 @@ interval_level_kernel(LevelLaunch p) {
                 child_len[h] = n;
             }
             if (any_ok && T.shorten) {
-                // ---- backward liveness (shorten.comp:148-186) on transposed bitsets:
-                // live[s][h] bit l = slot s is live for cell grp*32*KI + h*32 + l.
-                // The kept-mask of an instruction is live[out]; then live[out] = 0
-                // and the inputs its choice uses become live for the cells that
-                // kept it.
-                for (uint32_t s = lane; s < p.n_slots * KI; s += 32) live[s] = 0u;
-                __syncwarp();
-                if (lane == 0) {
-#pragma unroll
-                    for (int h = 0; h < KI; h++) live[h] = ok_w[h];
-                }
-                __syncwarp();
+                // ---- backward liveness (shorten.comp:148-186) ----
                 uint32_t kept[KI];
                 // sig: a cheap summary of this cell's output tape (the kept
                 // instruction positions and the MIN/MAX rewrites), to group
@@ -470,80 +555,98 @@ interval_level_kernel(LevelLaunch p) {
                     kept[h] = 0;
                     sig[h] = 0;
                 }
-                int mmi = (int)mm - 1;
-                for (int hi = (int)n; hi > 0; hi -= 32) {
-                    const int lo = max(0, hi - 32);
-                    const int m = hi - lo;
-                    // lane j holds instruction lo + j; walked from the top down
-                    const uint64_t mine = (int)lane < m ? __ldcg(&tape[lo + lane]) : 0ull;
-                    uint32_t my_keep[KI];
+                if (p.n_slots <= 64) {
+                    // per-cell slot bitsets in registers, like the reference's
+                    // per-thread bitset: no shared memory on the walk's path
+                    walk_regs<KI>(tape, n, (int)mm, mmb, keep, ok_w, lane, kept, sig);
+                } else {
+                    // wider slot files: transposed bitsets, live[s][h] bit l =
+                    // slot s is live for cell grp*32*KI + h*32 + l. The
+                    // kept-mask of an instruction is live[out]; then live[out] =
+                    // 0 and the inputs its choice uses become live for the cells
+                    // that kept it.
+                    for (uint32_t s = lane; s < p.n_slots * KI; s += 32) live[s] = 0u;
+                    __syncwarp();
+                    if (lane == 0) {
 #pragma unroll
-                    for (int h = 0; h < KI; h++) my_keep[h] = 0;
-                    for (int j = m - 1; j >= 0; j--) {
-                        const uint64_t w = __shfl_sync(0xFFFFFFFFu, mine, j);
-                        const uint32_t op = w_op(w), o = w_out(w);
-                        uint32_t k[KI];
-                        if constexpr (KI == 1) {
-                            k[0] = live[o];
-                        } else {
-                            const uint2 kk = *reinterpret_cast<const uint2*>(&live[o * 2]);
-                            k[0] = kk.x;
-                            k[1] = kk.y;
-                        }
-                        bool any = false;
-#pragma unroll
-                        for (int h = 0; h < KI; h++) any |= k[h] != 0u;
-                        if (any) {
-                            uint32_t first_m[KI], second_m[KI];
-                            if (op == OP_CONST) {
-#pragma unroll
-                                for (int h = 0; h < KI; h++) first_m[h] = second_m[h] = 0u;
-                            } else if (op == OP_ADD || op == OP_SUB || op == OP_MUL || op == OP_DIV) {
-#pragma unroll
-                                for (int h = 0; h < KI; h++) first_m[h] = second_m[h] = ~0u;
-                            } else if (is_mm(op)) {
-#pragma unroll
-                                for (int h = 0; h < KI; h++) {
-                                    const uint2 cb = mmb[mmi * KI + h];
-                                    first_m[h] = cb.x;
-                                    second_m[h] = cb.y;
-                                }
-                            } else {
-#pragma unroll
-                                for (int h = 0; h < KI; h++) {
-                                    first_m[h] = ~0u;
-                                    second_m[h] = 0u;
-                                }
-                            }
-                            __syncwarp();
-                            if (lane == 0) {
-                                const uint32_t ia = w_a(w), ib = w_b(w);
-#pragma unroll
-                                for (int h = 0; h < KI; h++) {
-                                    live[o * KI + h] = 0u;
-                                    const uint32_t fa = k[h] & first_m[h], sb = k[h] & second_m[h];
-                                    if (fa) live[ia * KI + h] |= fa;
-                                    if (sb) live[ib * KI + h] |= sb;
-                                }
-                            }
-                            __syncwarp();
-#pragma unroll
-                            for (int h = 0; h < KI; h++) {
-                                const uint32_t kb = (k[h] >> lane) & 1u;
-                                kept[h] += kb;
-                                const uint32_t code = kb + ((first_m[h] >> lane) & kb) + ((second_m[h] >> lane) & kb) * 2u;
-                                sig[h] += code * (uint32_t)(lo + j + 1) * 0x9E3779B1u;
-                            }
-                        }
-                        if ((int)lane == j) {
-#pragma unroll
-                            for (int h = 0; h < KI; h++) my_keep[h] = k[h];
-                        }
-                        if (is_mm(op)) mmi--;
+                        for (int h = 0; h < KI; h++) live[h] = ok_w[h];
                     }
-                    if ((int)lane < m) {
-                        if constexpr (KI == 1) keep[lo + lane] = my_keep[0];
-                        else reinterpret_cast<uint2*>(keep)[lo + lane] = make_uint2(my_keep[0], my_keep[1]);
+                    __syncwarp();
+                    int mmi = (int)mm - 1;
+                    for (int hi = (int)n; hi > 0; hi -= 32) {
+                        const int lo = max(0, hi - 32);
+                        const int m = hi - lo;
+                        // lane j holds instruction lo + j; walked from the top down
+                        const uint64_t mine = (int)lane < m ? __ldcg(&tape[lo + lane]) : 0ull;
+                        uint32_t my_keep[KI];
+#pragma unroll
+                        for (int h = 0; h < KI; h++) my_keep[h] = 0;
+                        for (int j = m - 1; j >= 0; j--) {
+                            const uint64_t w = __shfl_sync(0xFFFFFFFFu, mine, j);
+                            const uint32_t op = w_op(w), o = w_out(w);
+                            uint32_t k[KI];
+                            if constexpr (KI == 1) {
+                                k[0] = live[o];
+                            } else {
+                                const uint2 kk = *reinterpret_cast<const uint2*>(&live[o * 2]);
+                                k[0] = kk.x;
+                                k[1] = kk.y;
+                            }
+                            bool any = false;
+#pragma unroll
+                            for (int h = 0; h < KI; h++) any |= k[h] != 0u;
+                            if (any) {
+                                uint32_t first_m[KI], second_m[KI];
+                                if (op == OP_CONST) {
+#pragma unroll
+                                    for (int h = 0; h < KI; h++) first_m[h] = second_m[h] = 0u;
+                                } else if (op == OP_ADD || op == OP_SUB || op == OP_MUL || op == OP_DIV) {
+#pragma unroll
+                                    for (int h = 0; h < KI; h++) first_m[h] = second_m[h] = ~0u;
+                                } else if (is_mm(op)) {
+#pragma unroll
+                                    for (int h = 0; h < KI; h++) {
+                                        const uint2 cb = mmb[mmi * KI + h];
+                                        first_m[h] = cb.x;
+                                        second_m[h] = cb.y;
+                                    }
+                                } else {
+#pragma unroll
+                                    for (int h = 0; h < KI; h++) {
+                                        first_m[h] = ~0u;
+                                        second_m[h] = 0u;
+                                    }
+                                }
+                                __syncwarp();
+                                if (lane == 0) {
+                                    const uint32_t ia = w_a(w), ib = w_b(w);
+#pragma unroll
+                                    for (int h = 0; h < KI; h++) {
+                                        live[o * KI + h] = 0u;
+                                        const uint32_t fa = k[h] & first_m[h], sb = k[h] & second_m[h];
+                                        if (fa) live[ia * KI + h] |= fa;
+                                        if (sb) live[ib * KI + h] |= sb;
+                                    }
+                                }
+                                __syncwarp();
+#pragma unroll
+                                for (int h = 0; h < KI; h++) {
+                                    const uint32_t kb = (k[h] >> lane) & 1u;
+                                    kept[h] += kb;
+                                    const uint32_t code = kb + ((first_m[h] >> lane) & kb) + ((second_m[h] >> lane) & kb) * 2u;
+                                    sig[h] += code * (uint32_t)(lo + j + 1) * 0x9E3779B1u;
+                                }
+                            }
+                            if ((int)lane == j) {
+#pragma unroll
+                                for (int h = 0; h < KI; h++) my_keep[h] = k[h];
+                            }
+                            if (is_mm(op)) mmi--;
+                        }
+                        if ((int)lane < m) {
+                            if constexpr (KI == 1) keep[lo + lane] = my_keep[0];
+                            else reinterpret_cast<uint2*>(keep)[lo + lane] = make_uint2(my_keep[0], my_keep[1]);
+                        }
                     }
                 }
                 __syncwarp();
@@ -593,8 +696,11 @@ interval_level_kernel(LevelLaunch p) {
                                 if (ism) cb = mmb[(mm_v + __popc(mball & lanemask_lt())) * KI + h];
                                 // lane `lane` holds instruction idx: within each group,
                                 // every member's keep bit (and, where kept, its MIN/MAX
-                                // choice bits) must equal the leader's
-                                uint32_t pend = lwf[h], d = 0;
+                                // choice bits) must equal the leader's; groups that keep
+                                // nothing of this chunk agree on it
+                                const uint32_t anyk = __reduce_or_sync(0xFFFFFFFFu, km);
+                                uint32_t pend = __ballot_sync(0xFFFFFFFFu, ((lwf[h] >> lane) & 1u) && (group[h] & anyk)),
+                                         d = 0;
                                 while (pend) {
                                     const int ld = __ffs(pend) - 1;
                                     pend &= pend - 1;
@@ -691,7 +797,8 @@ interval_level_kernel(LevelLaunch p) {
                         }
 #pragma unroll
                         for (int h = 0; h < KI; h++) {
-                            uint32_t pending = short_w[h];
+                            // only the tapes that keep some instruction of this chunk
+                            uint32_t pending = short_w[h] & __reduce_or_sync(0xFFFFFFFFu, kmask[h]);
                             while (pending) {
                                 const int sel = __ffs(pending) - 1;
                                 pending &= pending - 1;
@@ -871,9 +978,9 @@ point_level_kernel(LevelLaunch p) {
             const uint32_t groups = words / K;                // items per node
             const float cs = T.cs;
             const unsigned long long local = item - t_lo;
-            const uint32_t node = (uint32_t)(local / groups), grp = (uint32_t)(local % groups);
-            if (p.reuse_src && __ldcg(&p.reuse_src[reuse_slot(T.ofs_l, node, T.node_size)]) != 0xFFFFFFFFu)
-                continue;  // copied from the previous tree by reuse_copy_kernel
+            const uint32_t grp = (uint32_t)(local % groups);
+            uint32_t node = (uint32_t)(local / groups);
+            if (p.eval_list) node = __ldcg(&p.eval_list[node]);  // the others are copies
             uint32_t* rec = T.nodes + T.ofs_l + (size_t)node * T.node_size;
             const uint32_t tape_idx = rec[0];
             const uint64_t* tape = T.tapes + tape_idx + 1;
@@ -963,7 +1070,7 @@ __device__ __forceinline__ unsigned long long level_items(TreeHeader* H, uint32_
     if (point && H->point_k != (uint32_t)k) return 0;
     const uint32_t count = level_count(H, L, H->node_cap, H->node_size[L]);
     if (!point && write_ofs) H->node_ofs[L + 1] = H->node_ofs[L] + (unsigned long long)count * H->node_size[L];
-    // with reuse, the nodes past reuse_eval[L] were added by copies: no items
+    // with reuse, only the listed nodes are evaluated
     const uint32_t evaluated = reuse ? min(count, H->reuse_eval[L]) : count;
     return (unsigned long long)evaluated * (words / (uint32_t)k);  // k: cells per lane of the pass
 }
@@ -1009,6 +1116,7 @@ __global__ void tree_init_kernel(TreeHeader* const* trees, uint32_t n, const flo
             H->tape_size_max[t] = t == 0 ? root_n : 0;
             H->cell_instr[t] = 0;
             H->fp32_ops[t] = 0;
+            H->reuse_eval[t] = 0;
         }
         if (t == 0) {
             H->tape_top = (1 + (unsigned long long)root_n + TAPE_ALIGN_WORDS - 1) / TAPE_ALIGN_WORDS * TAPE_ALIGN_WORDS;
@@ -1044,6 +1152,7 @@ __global__ void tree_init_staged_kernel(TreeHeader* const* trees, uint32_t n, co
             H->tape_size_max[t] = t == 0 ? root_n : 0;
             H->cell_instr[t] = 0;
             H->fp32_ops[t] = 0;
+            H->reuse_eval[t] = 0;
         }
         if (t == 0) {
             H->tape_top = e - b;
@@ -1199,7 +1308,7 @@ cudaError_t launch_tree_init_staged(dev::TreeHeader* const* trees, uint32_t n, c
 
 cudaError_t launch_level_scan(const LevelLaunch& a, bool point, int point_k, cudaStream_t stream) {
     dev::level_scan_kernel<<<1, 1024, 0, stream>>>(a.trees, a.n_trees, a.level, point ? 1 : 0, point_k, a.prefix,
-                                                   a.cursor, a.reuse_src ? 1 : 0);
+                                                   a.cursor, a.eval_list ? 1 : 0);
     return cudaGetLastError();
 }
 

@@ -201,8 +201,9 @@ frep_status frep_voxelize(frep_ctx* ctx, frep_tree* tree, const frep_tape* tape,
  *     overflowed is not used (everything is evaluated).
  *   - Typical use: two trees A and B alternate, frame k voxelizes into one
  *     with the other as prev.
- *   - The first call allocates a side array of node_words / 8 + 1 u32 for the
- *     tree (one entry per node: where it was copied from).
+ *   - The first call allocates two side arrays of node_words / 8 + 1 u32 for
+ *     the tree (per node, where it was copied from; per level, the nodes to
+ *     evaluate).
  *   - frep_tree_work and frep_tree_fp32_ops count only the evaluated nodes.
  * FREP_ERR_INVALID_ARG: prev null, equal to tree, not voxelized, or with
  * another grid / options. */
