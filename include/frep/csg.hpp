@@ -331,6 +331,12 @@ public:
     void Voxelize(void* stream, float tapeTime) {
         check(frep_voxelize(ctx_, voxels_->tree(), voxels_->tape.handle(), tapeTime, stream));
     }
+    // The same tree, copying from `prev` (the previous frame's storage, same
+    // grid) every subtree that does not depend on the time
+    // (frep_voxelize_reuse).
+    void Voxelize(void* stream, float tapeTime, const VoxelStorage& prev) {
+        check(frep_voxelize_reuse(ctx_, voxels_->tree(), prev.tree(), voxels_->tape.handle(), tapeTime, stream));
+    }
 
 private:
     frep_ctx* ctx_ = nullptr;
