@@ -69,6 +69,8 @@ def parse():
                     help="large / stress: tree branching per level (default 16,16,8 / 16,16,4,4)")
     ap.add_argument("--res", default=None, help="render resolution WxH (batch 512x512, large 1920x1080)")
     ap.add_argument("--pool-mb", type=int, default=3072, help="large: node + tape pool size of the tree, MB")
+    ap.add_argument("--no-compact", action="store_true",
+                    help="large: skip the compact-tree measurements (compaction time, bytes, render time)")
     args = ap.parse_args()
     if args.grid is None:
         args.grid = "16,16,4,4" if args.workload == "stress" else "16,16,8"
@@ -384,6 +386,11 @@ def run_ours(args, world, rank, local):
     h2d = 8 * info.root_tape_words
     d2h = W * H * 4
 
+    # ---- compact trees (large scene): compaction time, bytes, render time ---
+    compact_stats = None
+    if args.workload == "large" and not args.no_compact:
+        compact_stats = measure_compact(args, ctx, vs, scene, rt.lights, tt[0], rgba, flush, stream, render_ms)
+
     # ---- roofline of the dominant kernel -------------------------------------
     peaks = measured_peaks()
     dom = max(range(vs.grid_levels), key=lambda l: level_ms[l])
@@ -413,6 +420,7 @@ def run_ours(args, world, rank, local):
         "level_ms": level_ms, "render_ms": render_ms,
         **({"reuse": {"previous_frame_tree": reuse,
                       "cell_instr_per_level": cell_instr}} if anim else {}),
+        **({"compact": compact_stats} if compact_stats else {}),
         "e2e": {"value": e2e_value, "unit": "scenes/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "clocks": clocks.summary(),
         "gpu_launches": launches_per_step * args.steps,
@@ -429,6 +437,50 @@ def run_ours(args, world, rank, local):
     for st in storages:
         st.cleanup()
     ctx.close()
+
+def measure_compact(args, ctx, vs, scene, lights, t, rgba, flush, stream, render_ms_full):
+    """Compacts the last voxelized tree both ways (frep_tree_compact) and
+    renders each: device time of the compaction (CUDA events around the
+    blocking call), bytes held, render time of one frame, blob size."""
+    import torch
+    import frep
+
+    frep.Voxelizer(ctx, vs).voxelize(t, stream)
+    info = vs.sync()
+    out = {"source_bytes": info.node_words_used * 4 + info.tape_words_used * 8,
+           "source_node_bytes": info.node_words_used * 4, "source_tape_bytes": info.tape_words_used * 8,
+           "render_ms_source": render_ms_full}
+    W, H = scene.width, scene.height
+    for name, prune in (("layout", False), ("prune", True)):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ms = []
+        for _ in range(3):
+            flush.fill_(1)
+            a.record(stream)
+            ct = frep.CompactTree.from_storage(ctx, vs, prune=prune, stream=stream)
+            b.record(stream)
+            torch.cuda.synchronize()
+            ms.append(a.elapsed_time(b))
+            if len(ms) < 3:
+                ct.close()
+        ct.lights = lights
+        rms = []
+        for _ in range(max(3, min(args.steps, 10))):
+            flush.fill_(1)
+            a.record(stream)
+            ct.trace(scene.camera, t, W, H, out=(rgba, None), stream=stream)
+            b.record(stream)
+            torch.cuda.synchronize()
+            rms.append(a.elapsed_time(b))
+        ci = ct.info()
+        size = len(ct.export())
+        out[name] = {"compact_ms": sorted(ms)[1], "device_bytes": ci.device_bytes,
+                     "node_bytes": ci.node_words * 4, "tape_bytes": ci.tape_words * 8,
+                     "nodes_per_level": list(ci.node_count[:ci.levels]), "blob_bytes": size,
+                     "render_ms": sum(rms) / len(rms)}
+        ct.close()
+    return out
+
 
 # ---- many-scene batch ----------------------------------------------------------------
 

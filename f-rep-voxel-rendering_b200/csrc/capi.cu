@@ -674,13 +674,9 @@ frep_status fill_render_args(const frep_tree* tree, const frep_camera* cam, cons
                              float tape_time, const frep_image* out, RenderArgs* args) {
     if (!tree || !cam || !lights || !out) return fail(FREP_ERR_INVALID_ARG, "frep_render: null argument");
     if (!tree->voxelized) return fail(FREP_ERR_INVALID_ARG, "frep_render: the tree has not been voxelized");
-    if (cam->width == 0 || cam->height == 0 || cam->projection > 1)
-        return fail(FREP_ERR_INVALID_ARG, "frep_render: bad camera");
-    if (lights->count > FREP_MAX_LIGHTS) return fail(FREP_ERR_INVALID_ARG, "frep_render: too many lights");
-    if (((uintptr_t)out->rgba8 & 3) || ((uintptr_t)out->hits & 3))
-        return fail(FREP_ERR_INVALID_ARG, "frep_render: output buffers must be 4-byte aligned");
+    frep_status st = fill_view_args(cam, lights, tape_time, out, args);
+    if (st != FREP_OK) return st;
     RenderArgs& a = *args;
-    a = RenderArgs{};
     a.hdr = tree->hdr;
     a.nodes = tree->nodes;
     a.tapes = tree->tapes;
@@ -692,6 +688,20 @@ frep_status fill_render_args(const frep_tree* tree, const frep_camera* cam, cons
     }
     for (int k = 0; k < 3; k++) a.low[k] = tree->grid.low_vertex[k];
     a.world_size = tree->grid.world_size;
+    a.n_slots = tree->n_slots;
+    return FREP_OK;
+}
+
+frep_status fill_view_args(const frep_camera* cam, const frep_lights* lights, float tape_time,
+                           const frep_image* out, RenderArgs* args) {
+    if (!cam || !lights || !out) return fail(FREP_ERR_INVALID_ARG, "frep_render: null argument");
+    if (cam->width == 0 || cam->height == 0 || cam->projection > 1)
+        return fail(FREP_ERR_INVALID_ARG, "frep_render: bad camera");
+    if (lights->count > FREP_MAX_LIGHTS) return fail(FREP_ERR_INVALID_ARG, "frep_render: too many lights");
+    if (((uintptr_t)out->rgba8 & 3) || ((uintptr_t)out->hits & 3))
+        return fail(FREP_ERR_INVALID_ARG, "frep_render: output buffers must be 4-byte aligned");
+    RenderArgs& a = *args;
+    a = RenderArgs{};
     a.tape_time = tape_time;
     // Camera::Init, Right(), Up() (camera.cpp:8-27); raytracer.cpp:177-181.
     const H3 fwd = normalize3({cam->forward[0], cam->forward[1], cam->forward[2]});
@@ -723,7 +733,6 @@ frep_status fill_render_args(const frep_tree* tree, const frep_camera* cam, cons
         a.background[c] = lights->background[c];
     }
     a.shadow_mask = lights->shadow_mask;
-    a.n_slots = tree->n_slots;
     a.rgba8 = out->rgba8;
     a.hits = out->hits;
     return FREP_OK;

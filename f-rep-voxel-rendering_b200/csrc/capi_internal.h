@@ -35,6 +35,9 @@ frep_status tree_create_impl(frep_ctx* ctx, const frep_grid* grid, const frep_vo
 // Camera basis, lights and tree description for one frame (frep_render).
 frep_status fill_render_args(const frep_tree* tree, const frep_camera* cam, const frep_lights* lights,
                              float tape_time, const frep_image* out, RenderArgs* args);
+// The frame part alone (camera basis, lights, outputs): resets *args first.
+frep_status fill_view_args(const frep_camera* cam, const frep_lights* lights, float tape_time,
+                           const frep_image* out, RenderArgs* args);
 }  // namespace detail
 }  // namespace frep
 

@@ -127,6 +127,9 @@ struct RenderArgs {
     uint32_t n_slots;
     uint8_t* rgba8;
     void* hits;                      // frep_hit*
+    uint32_t compact;                // 1: nodes are in the compact layout (compact.cu), whose
+    unsigned long long node_ofs[8];  //   level offsets (u32 words) are given here; 0: the
+                                     //   reference's layout, offsets from hdr
 };
 
 cudaError_t launch_render(const RenderArgs& a, cudaStream_t stream);

@@ -30,6 +30,38 @@ struct Tree {
     }
 };
 
+// Where a node record keeps its masks and children. CMP = false: the
+// reference's layout (node.comp:4-72), [tape, coords, leaf, interior,
+// childList[dim^3]]; CMP = true: the compact layout, [tape, leaf[W],
+// interior[W], prefix[W], base] (last level [tape, leaf[W]]), W = dim^3 / 32,
+// whose interior children are numbered consecutively from `base` in cell
+// order, prefix[w] = interior cells before word w.
+template <bool CMP>
+struct Layout;
+template <>
+struct Layout<false> {
+    static __device__ __forceinline__ bool leaf(const uint32_t* r, uint32_t c3, uint32_t idx) {
+        return (__ldg(&r[4 + (idx >> 5)]) >> (idx & 31)) & 1u;
+    }
+    // The child node of an interior cell, or ~0 when the cell is not interior.
+    static __device__ __forceinline__ uint32_t child(const uint32_t* r, uint32_t c3, uint32_t idx) {
+        if (!((__ldg(&r[4 + c3 / 32 + (idx >> 5)]) >> (idx & 31)) & 1u)) return ~0u;
+        return __ldg(&r[4 + c3 / 16 + idx]);
+    }
+};
+template <>
+struct Layout<true> {
+    static __device__ __forceinline__ bool leaf(const uint32_t* r, uint32_t c3, uint32_t idx) {
+        return (__ldg(&r[1 + (idx >> 5)]) >> (idx & 31)) & 1u;
+    }
+    static __device__ __forceinline__ uint32_t child(const uint32_t* r, uint32_t c3, uint32_t idx) {
+        const uint32_t W = c3 >> 5;
+        const uint32_t iw = __ldg(&r[1 + W + (idx >> 5)]);
+        if (!((iw >> (idx & 31)) & 1u)) return ~0u;
+        return __ldg(&r[1 + 3 * W]) + __ldg(&r[1 + 2 * W + (idx >> 5)]) + __popc(iw & ((1u << (idx & 31)) - 1u));
+    }
+};
+
 // raygrid_intersect (main.comp:24-43).
 __device__ bool grid_intersect(const RenderArgs& A, float3 o, float3 inv, float& te, float& tl) {
     const float gs = A.world_size;
@@ -49,6 +81,7 @@ __device__ bool grid_intersect(const RenderArgs& A, float3 o, float3 inv, float&
 
 // dda (main.comp:46-111), kd-restart. Cell coordinates are clamped to
 // [0, dim) and the step count is bounded (both also in the oracle).
+template <bool CMP>
 __device__ bool dda(const Tree& T, float3 o, float3 d, RHit& hit) {
     const RenderArgs& A = *T.a;
     hit.steps = 0;
@@ -84,7 +117,7 @@ __device__ bool dda(const Tree& T, float3 o, float3 d, RHit& hit) {
             const uint32_t idx = (uint32_t)(cz + dim * cy + dim * dim * cx);
             const uint32_t* r = T.rec(lvl, node);
             const uint32_t c3 = (uint32_t)(dim * dim * dim);
-            if ((__ldg(&r[4 + (idx >> 5)]) >> (idx & 31)) & 1u) {
+            if (Layout<CMP>::leaf(r, c3, idx)) {
                 hit.t = t_curr;
                 hit.node = node;
                 hit.level = lvl;
@@ -92,8 +125,9 @@ __device__ bool dda(const Tree& T, float3 o, float3 d, RHit& hit) {
                 hit.steps = steps;
                 return true;
             }
-            if (lvl < last && ((__ldg(&r[4 + c3 / 32 + (idx >> 5)]) >> (idx & 31)) & 1u)) {
-                node = __ldg(&r[4 + c3 / 16 + idx]);
+            const uint32_t ch = lvl < last ? Layout<CMP>::child(r, c3, idx) : ~0u;
+            if (ch != ~0u) {
+                node = ch;
                 npx = __fadd_rn(npx, __fmul_rn((float)cx, cs));
                 npy = __fadd_rn(npy, __fmul_rn((float)cy, cs));
                 npz = __fadd_rn(npz, __fmul_rn((float)cz, cs));
@@ -205,12 +239,12 @@ struct HitRecord {  // == frep_hit
     uint32_t level, node, cell, steps;
 };
 
-template <int NS>
+template <int NS, bool CMP>
 __device__ __forceinline__ void render_pixel(const RenderArgs& A, uint32_t x, uint32_t y) {
     Tree T;
     T.nodes = A.nodes;
     T.a = &A;
-    for (uint32_t l = 0; l < A.levels; l++) T.ofs[l] = A.hdr->node_ofs[l];
+    for (uint32_t l = 0; l < A.levels; l++) T.ofs[l] = CMP ? A.node_ofs[l] : A.hdr->node_ofs[l];
 
     // Ray generation (main.comp:168-178).
     float ox = 0.0f, oy = 0.0f;
@@ -239,7 +273,7 @@ __device__ __forceinline__ void render_pixel(const RenderArgs& A, uint32_t x, ui
     }
 
     RHit h;
-    const bool did = dda(T, o, d, h);
+    const bool did = dda<CMP>(T, o, d, h);
     float col[4];
     float3 n = make_float3(0.0f, 0.0f, 0.0f);
     if (!did) {
@@ -261,7 +295,7 @@ __device__ __forceinline__ void render_pixel(const RenderArgs& A, uint32_t x, ui
                 const float3 so = make_float3(__fadd_rn(o.x, __fmul_rn(ts, d.x)), __fadd_rn(o.y, __fmul_rn(ts, d.y)),
                                               __fadd_rn(o.z, __fmul_rn(ts, d.z)));
                 RHit sh;
-                if (dda(T, so, make_float3(-L.x, -L.y, -L.z), sh)) continue;
+                if (dda<CMP>(T, so, make_float3(-L.x, -L.y, -L.z), sh)) continue;
             }
             const float dd = dot3(make_float3(-L.x, -L.y, -L.z), n);
             const float inten = fmaxf(dd, 0.0f);
@@ -288,12 +322,12 @@ __device__ __forceinline__ void render_pixel(const RenderArgs& A, uint32_t x, ui
     }
 }
 
-template <int NS>
+template <int NS, bool CMP = false>
 __global__ void __launch_bounds__(64) render_kernel(const RenderArgs A) {
     const uint32_t x = blockIdx.x * 8 + (threadIdx.x & 7);
     const uint32_t y = blockIdx.y * 8 + (threadIdx.x >> 3);
     if (x >= A.width || y >= A.height) return;
-    render_pixel<NS>(A, x, y);
+    render_pixel<NS, CMP>(A, x, y);
 }
 
 // Many frames in one launch: blockIdx.z selects the frame.
@@ -303,7 +337,7 @@ __global__ void __launch_bounds__(64) render_batch_kernel(const RenderArgs* args
     const uint32_t x = blockIdx.x * 8 + (threadIdx.x & 7);
     const uint32_t y = blockIdx.y * 8 + (threadIdx.x >> 3);
     if (x >= A.width || y >= A.height) return;
-    render_pixel<NS>(A, x, y);
+    render_pixel<NS, false>(A, x, y);
 }
 
 // Temporal resolve (renderer/triangle.frag:14-23): the pixel is the mean of
@@ -340,6 +374,16 @@ cudaError_t launch_resolve_layers(const uint8_t* layers, uint32_t n, uint32_t pi
 cudaError_t launch_render(const RenderArgs& a, cudaStream_t stream) {
     const dim3 grid((a.width + 7) / 8, (a.height + 7) / 8);
     const uint32_t ns = a.n_slots;
+    if (a.compact) {
+        if (ns <= 32) dev::render_kernel<32, true><<<grid, 64, 0, stream>>>(a);
+        else if (ns <= 64) dev::render_kernel<64, true><<<grid, 64, 0, stream>>>(a);
+        else if (ns <= 128) dev::render_kernel<128, true><<<grid, 64, 0, stream>>>(a);
+        else if (ns <= 256) dev::render_kernel<256, true><<<grid, 64, 0, stream>>>(a);
+        else if (ns <= 512) dev::render_kernel<512, true><<<grid, 64, 0, stream>>>(a);
+        else if (ns <= 1024) dev::render_kernel<1024, true><<<grid, 64, 0, stream>>>(a);
+        else return cudaErrorInvalidValue;
+        return cudaGetLastError();
+    }
     if (ns <= 32) dev::render_kernel<32><<<grid, 64, 0, stream>>>(a);
     else if (ns <= 64) dev::render_kernel<64><<<grid, 64, 0, stream>>>(a);
     else if (ns <= 128) dev::render_kernel<128><<<grid, 64, 0, stream>>>(a);

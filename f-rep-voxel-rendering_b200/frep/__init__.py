@@ -24,7 +24,7 @@ from . import _lib as L
 from ._lib import FrepError
 
 __all__ = ["csg", "Tape", "Context", "VoxelStorage", "Voxelizer", "Camera", "Lights", "Raytracer",
-           "FrepError", "ROUND_NEAREST", "ROUND_OUTWARD", "TreeExport"]
+           "FrepError", "ROUND_NEAREST", "ROUND_OUTWARD", "TreeExport", "CompactTree"]
 
 ROUND_NEAREST = 0
 ROUND_OUTWARD = 1
@@ -451,6 +451,71 @@ class Raytracer:
                                              float(tape_time), n_samples, layers.data_ptr(), rgba.data_ptr(),
                                              _stream_ptr(stream)))
         return rgba, layers
+
+
+class CompactTree:
+    """A compact tree (frep_compact): the voxelized tree with every level in
+    depth-first preorder and no per-node child lists, optionally pruned as
+    SceneBuilder::BuildNode does (scene_builder.cpp:91-156); renders like
+    Raytracer.trace and round-trips through a host blob (frep.compact)."""
+
+    def __init__(self, ctx: Context, handle: C.c_void_p):
+        self.ctx = ctx
+        self._h = handle
+        self.lights = Lights()
+
+    @classmethod
+    def from_storage(cls, ctx: Context, voxels: VoxelStorage, prune: bool = False, stream=None) -> "CompactTree":
+        h = C.c_void_p()
+        L.check(L.lib().frep_tree_compact(ctx._h, voxels.tree, 1 if prune else 0, _stream_ptr(stream), C.byref(h)))
+        return cls(ctx, h)
+
+    @classmethod
+    def from_blob(cls, ctx: Context, blob) -> "CompactTree":
+        arr = np.ascontiguousarray(np.frombuffer(bytes(blob), np.uint8) if not isinstance(blob, np.ndarray) else blob,
+                                   np.uint8)
+        h = C.c_void_p()
+        L.check(L.lib().frep_compact_import(ctx._h, _ptr(arr), arr.nbytes, C.byref(h)))
+        return cls(ctx, h)
+
+    def info(self) -> "L.CompactInfo":
+        i = L.CompactInfo()
+        L.check(L.lib().frep_compact_get_info(self._h, C.byref(i)))
+        return i
+
+    def export(self) -> np.ndarray:
+        """The blob (uint8 array)."""
+        size = C.c_uint64()
+        L.check(L.lib().frep_compact_export(self._h, None, 0, C.byref(size)))
+        out = np.zeros(size.value, np.uint8)
+        L.check(L.lib().frep_compact_export(self._h, _ptr(out), out.nbytes, C.byref(size)))
+        return out
+
+    def trace(self, camera: Camera, tape_time: float = 0.0, width: int = 256, height: int = 256,
+              hits: bool = False, out=None, stream=None):
+        import torch
+        dev = torch.device("cuda", self.ctx.device)
+        if out is None:
+            rgba = torch.empty((height, width, 4), dtype=torch.uint8, device=dev)
+            hit_buf = torch.empty((height, width, 8), dtype=torch.int32, device=dev) if hits else None
+        else:
+            rgba, hit_buf = out
+        img = L.Image(rgba.data_ptr() if rgba is not None else None,
+                      hit_buf.data_ptr() if hit_buf is not None else None)
+        cam = camera.struct(width, height)
+        lights = self.lights.struct()
+        L.check(L.lib().frep_render_compact(self.ctx._h, self._h, C.byref(cam), C.byref(lights), float(tape_time),
+                                            C.byref(img), _stream_ptr(stream)))
+        return rgba, hit_buf
+
+    def close(self):
+        if self._h is not None and self._h.value and L is not None and L._lib is not None:
+            L.lib().frep_compact_destroy(self._h)
+        self._h = C.c_void_p()
+
+    def __del__(self):
+        if L is not None and C is not None:
+            self.close()
 
 
 def resolve_layers(layers, stream=None):

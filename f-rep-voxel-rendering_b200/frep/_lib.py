@@ -99,6 +99,13 @@ class LightsStruct(C.Structure):
                 ("background", C.c_float * 4), ("shadow_mask", C.c_uint32)]
 
 
+class CompactInfo(C.Structure):
+    _fields_ = [("levels", C.c_uint32), ("dims", C.c_uint32 * MAX_LEVELS), ("mode", C.c_uint32),
+                ("n_slots", C.c_uint32), ("node_count", C.c_uint32 * MAX_LEVELS),
+                ("node_offset", C.c_uint64 * MAX_LEVELS), ("node_size", C.c_uint32 * MAX_LEVELS),
+                ("node_words", C.c_uint64), ("tape_words", C.c_uint64), ("device_bytes", C.c_uint64)]
+
+
 class Image(C.Structure):
     _fields_ = [("rgba8", C.c_void_p), ("hits", C.c_void_p)]
 
@@ -160,6 +167,14 @@ _SIGS = {
     "frep_batch_timings": (C.c_int, [_P, _P]),
     "frep_render": (C.c_int, [_P, _P, C.POINTER(CameraStruct), C.POINTER(LightsStruct), C.c_float,
                               C.POINTER(Image), _P]),
+    "frep_tree_compact": (C.c_int, [_P, _P, C.c_uint32, _P, C.POINTER(_P)]),
+    "frep_compact_get_info": (C.c_int, [_P, C.POINTER(CompactInfo)]),
+    "frep_compact_destroy": (None, [_P]),
+    "frep_render_compact": (C.c_int, [_P, _P, C.POINTER(CameraStruct), C.POINTER(LightsStruct), C.c_float,
+                                      C.POINTER(Image), _P]),
+    "frep_compact_export": (C.c_int, [_P, _P, C.c_uint64, C.POINTER(C.c_uint64)]),
+    "frep_compact_check": (C.c_int, [_P, C.c_uint64]),
+    "frep_compact_import": (C.c_int, [_P, _P, C.c_uint64, C.POINTER(_P)]),
 }
 
 

@@ -352,6 +352,100 @@ frep_status frep_render_temporal(frep_ctx* ctx, const frep_tree* tree, const fre
                                  uint8_t* rgba8, void* stream);
 
 /* ---------------------------------------------------------------------------
+ * Compact trees (render-ready, export / import)
+ *
+ * Replaces SceneBuilder's compaction and layout (vulkan/src/engine/
+ * scene_builder.cpp: BuildNode :91-156, LayoutNode :199-238; the layout notes
+ * of vulkan/README.md:22-54): the voxelizer's tree is not compactified
+ * (nodes can be empty or have only leaf cells), and every interior node
+ * carries a full dim^3 child list. A compact tree
+ *   - numbers the nodes of every level in depth-first preorder, children in
+ *     ascending cell order (LayoutNode), so the children of a node are
+ *     consecutive and are found from one base index and a popcount: a
+ *     non-last node is [tapeIdx, leafMask[W], interiorMask[W], prefix[W],
+ *     base] (W = dim^3/32; prefix[w] = interior cells in words before w; the
+ *     child of interior cell i is base + prefix[i/32] + the interior cells
+ *     before i in its word), a last-level node [tapeIdx, leafMask[W]];
+ *   - keeps one copy of every tape its nodes use (tapeIdx: u64 word index
+ *     into the compact tree's own tape pool, records as in frep_tree);
+ *   - with FREP_COMPACT_PRUNE, also applies BuildNode's rules bottom-up: a
+ *     child node with no leaf and no interior cell is dropped, one whose
+ *     cells are all leaves becomes a leaf cell of its parent. The solid
+ *     voxels are the same; rays that hit a collapsed node hit its parent's
+ *     cell instead (same depth t, normal from the parent's tape). The root is
+ *     always kept. FREP_COMPACT_LAYOUT keeps every node and mask: renders
+ *     give the same hits (cells, depths, normals) as the source tree.
+ * ------------------------------------------------------------------------- */
+
+enum { FREP_COMPACT_LAYOUT = 0, FREP_COMPACT_PRUNE = 1 };
+
+typedef struct frep_compact frep_compact;
+
+typedef struct frep_compact_info {
+    uint32_t levels;
+    uint32_t dims[FREP_MAX_LEVELS];
+    uint32_t mode;                              /* FREP_COMPACT_*                       */
+    uint32_t n_slots;                           /* slots of the longest tape (render)   */
+    uint32_t node_count[FREP_MAX_LEVELS];
+    uint64_t node_offset[FREP_MAX_LEVELS];      /* u32 words                            */
+    uint32_t node_size[FREP_MAX_LEVELS];        /* u32 words                            */
+    uint64_t node_words;                        /* u32 words of the node pool           */
+    uint64_t tape_words;                        /* u64 words of the tape pool           */
+    uint64_t device_bytes;                      /* held on the device                   */
+} frep_compact_info;
+
+/* Builds the compact form of a voxelized tree (which is left unchanged and
+ * may then be destroyed or voxelized again). Blocking: waits for the tree's
+ * voxelization, runs the compaction on `stream` and waits for it. Device
+ * memory: the result (charged to the context's budget) plus temporary
+ * scratch of about 16 bytes per source node and 1/4 byte per tape word.
+ * FREP_ERR_CAPACITY: the tree's pools overflowed; FREP_ERR_INVALID_ARG: not
+ * voxelized or a bad mode. */
+frep_status frep_tree_compact(frep_ctx* ctx, frep_tree* tree, uint32_t mode, void* stream, frep_compact** out);
+frep_status frep_compact_get_info(const frep_compact* compact, frep_compact_info* info);
+void frep_compact_destroy(frep_compact* compact);
+
+/* Raytracer::Trace over a compact tree: the same camera, lights, shading and
+ * outputs as frep_render; frep_hit.node is the node's preorder index. */
+frep_status frep_render_compact(frep_ctx* ctx, const frep_compact* compact, const frep_camera* camera,
+                                const frep_lights* lights, float tape_time, const frep_image* out, void* stream);
+
+/* Serialised compact tree ("blob"): a frep_compact_header, then the node pool
+ * (node_words u32), then the tape pool (tape_words u64); each section starts
+ * on an 8-byte boundary (the node section is zero-padded to one). Little
+ * endian, position independent: it can be written to a file and imported in
+ * another process or on another device. */
+typedef struct frep_compact_header {
+    char magic[8];                              /* "FREPCT01"                           */
+    uint32_t version;                           /* 1                                    */
+    uint32_t levels;
+    uint32_t dims[FREP_MAX_LEVELS];
+    float low_vertex[3];
+    float world_size;
+    uint32_t mode;
+    uint32_t n_slots;
+    uint32_t node_count[FREP_MAX_LEVELS];
+    uint64_t node_words;
+    uint64_t tape_words;
+} frep_compact_header;
+
+/* Writes the blob of `compact` to host memory. *size = its size in bytes;
+ * dst = NULL asks for the size only; a dst smaller than it (cap) is
+ * FREP_ERR_INVALID_ARG. Blocking. */
+frep_status frep_compact_export(const frep_compact* compact, void* dst, uint64_t cap, uint64_t* size);
+
+/* Checks a blob on the host (no device needed): header fields, section sizes,
+ * every node's masks, prefix counts and child ranges (each child referenced
+ * once, in preorder), every tape index and record, and every instruction's
+ * opcode and slots against n_slots. FREP_OK or FREP_ERR_INVALID_ARG with the
+ * first problem in frep_last_error(). */
+frep_status frep_compact_check(const void* blob, uint64_t size);
+
+/* Uploads a blob (checked first with frep_compact_check) into a new compact
+ * tree of `ctx`. Blocking. */
+frep_status frep_compact_import(frep_ctx* ctx, const void* blob, uint64_t size, frep_compact** out);
+
+/* ---------------------------------------------------------------------------
  * Batching: many scenes per launch
  * ------------------------------------------------------------------------- */
 

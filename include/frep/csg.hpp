@@ -343,6 +343,49 @@ private:
     VoxelStorage* voxels_ = nullptr;
 };
 
+// SceneBuilder (scene_builder.h:9-61): the reference builds a compactified
+// tree on the CPU and uploads it; here BuildScene compacts the voxelized tree
+// on the device (frep_tree_compact: empty children dropped and all-leaf
+// children turned into leaf cells when `prune`, every level in depth-first
+// preorder, no per-node child lists). Export / Import move it through host
+// memory (e.g. a file) as one position-independent blob.
+class SceneBuilder {
+public:
+    void Init(frep_ctx* ctx, VoxelStorage* voxels) {
+        ctx_ = ctx;
+        voxels_ = voxels;
+    }
+    void BuildScene(bool prune = true, void* stream = nullptr) {
+        frep_compact* c = nullptr;
+        check(frep_tree_compact(ctx_, voxels_->tree(), prune ? FREP_COMPACT_PRUNE : FREP_COMPACT_LAYOUT, stream, &c));
+        compact_.reset(c, frep_compact_destroy);
+    }
+    std::vector<uint8_t> Export() const {
+        uint64_t size = 0;
+        check(frep_compact_export(compact_.get(), nullptr, 0, &size));
+        std::vector<uint8_t> blob(size);
+        check(frep_compact_export(compact_.get(), blob.data(), blob.size(), &size));
+        return blob;
+    }
+    void Import(frep_ctx* ctx, const std::vector<uint8_t>& blob) {
+        frep_compact* c = nullptr;
+        check(frep_compact_import(ctx, blob.data(), blob.size(), &c));
+        ctx_ = ctx;
+        compact_.reset(c, frep_compact_destroy);
+    }
+    frep_compact_info Info() const {
+        frep_compact_info info{};
+        check(frep_compact_get_info(compact_.get(), &info));
+        return info;
+    }
+    frep_compact* compact() const { return compact_.get(); }
+
+private:
+    frep_ctx* ctx_ = nullptr;
+    VoxelStorage* voxels_ = nullptr;
+    std::shared_ptr<frep_compact> compact_;
+};
+
 // Camera (camera.h:6-41); the library normalises forward / initialUp.
 struct Camera {
     float position[3] = {0, 0, 40};
@@ -370,6 +413,20 @@ public:
     // Renders into a device rgba8 buffer of width*height*4 bytes.
     void Trace(void* stream, const Camera& cam, float tapeTime, uint32_t width, uint32_t height,
                uint8_t* device_rgba8, frep_hit* device_hits = nullptr) {
+        const frep_camera c = MakeCamera(cam, width, height);
+        frep_image img{device_rgba8, device_hits};
+        check(frep_render(ctx_, voxels_->tree(), &c, &lights_, tapeTime, &img, stream));
+    }
+    // The same frame from a compact tree (frep_render_compact).
+    void Trace(void* stream, const SceneBuilder& scene, const Camera& cam, float tapeTime, uint32_t width,
+               uint32_t height, uint8_t* device_rgba8, frep_hit* device_hits = nullptr) {
+        const frep_camera c = MakeCamera(cam, width, height);
+        frep_image img{device_rgba8, device_hits};
+        check(frep_render_compact(ctx_, scene.compact(), &c, &lights_, tapeTime, &img, stream));
+    }
+
+private:
+    static frep_camera MakeCamera(const Camera& cam, uint32_t width, uint32_t height) {
         frep_camera c{};
         for (int k = 0; k < 3; k++) {
             c.position[k] = cam.position[k];
@@ -381,11 +438,9 @@ public:
         c.projection = cam.orthographic ? FREP_ORTHOGRAPHIC : FREP_PERSPECTIVE;
         c.width = width;
         c.height = height;
-        frep_image img{device_rgba8, device_hits};
-        check(frep_render(ctx_, voxels_->tree(), &c, &lights_, tapeTime, &img, stream));
+        return c;
     }
 
-private:
     frep_ctx* ctx_ = nullptr;
     VoxelStorage* voxels_ = nullptr;
     frep_lights lights_{};

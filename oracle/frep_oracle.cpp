@@ -602,6 +602,138 @@ void oracle_tree_work(void* tree, uint64_t* cell_instr8) {
 
 }  // extern "C"
 
+// ---- compaction (vulkan/src/engine/scene_builder.cpp) --------------------------
+namespace {
+
+enum : uint8_t { ST_EMPTY = 0, ST_KEPT = 1, ST_FULL = 2 };
+
+struct Compactor {
+    const Tree& S;
+    int prune;
+    std::vector<std::vector<uint8_t>> status;  // per level, per source node (prune only)
+    Tree* D = nullptr;
+    std::vector<uint32_t> next;                 // LayoutNode's nextNodeIdx
+
+    const uint32_t* rec(uint32_t l, uint32_t node) const {
+        return &S.nodes[S.node_ofs[l] + (uint64_t)node * S.node_size[l]];
+    }
+
+    // A node's masks after its children are compacted. BuildNode
+    // (scene_builder.cpp:91-156): a child whose cells are all leaves becomes a
+    // leaf bit (:132-137, HasAllLeafChildren :79-89), an empty child (nullptr,
+    // :151-154) clears its bit, any other child stays an interior child.
+    void masks(uint32_t l, uint32_t node, std::vector<uint32_t>& leaf, std::vector<uint32_t>& inter) const {
+        const uint32_t dim = S.dims[l], c3 = dim * dim * dim, W = c3 / 32;
+        const bool last = l == S.levels - 1;
+        const uint32_t* r = rec(l, node);
+        leaf.assign(r + 4, r + 4 + W);
+        inter.assign(W, 0);
+        if (last) return;
+        for (uint32_t w = 0; w < W; w++) inter[w] = r[4 + W + w];
+        if (!prune) return;
+        const uint32_t* list = r + 4 + c3 / 16;
+        for (uint32_t w = 0; w < W; w++) {
+            for (uint32_t b = 0; b < 32; b++) {
+                if (!((inter[w] >> b) & 1u)) continue;
+                const uint8_t st = status[l + 1][list[w * 32 + b]];
+                if (st == ST_FULL) {
+                    leaf[w] |= 1u << b;
+                    inter[w] &= ~(1u << b);
+                } else if (st == ST_EMPTY) {
+                    inter[w] &= ~(1u << b);
+                }
+            }
+        }
+    }
+
+    void compute_status() {
+        status.assign(S.levels, {});
+        std::vector<uint32_t> leaf, inter;
+        for (int l = (int)S.levels - 1; l >= 0; l--) {
+            status[l].assign(S.node_count[l], ST_KEPT);
+            for (uint32_t i = 0; i < S.node_count[l]; i++) {
+                masks((uint32_t)l, i, leaf, inter);
+                bool any = false, full = true;
+                for (size_t w = 0; w < leaf.size(); w++) {
+                    any = any || leaf[w] || inter[w];
+                    full = full && leaf[w] == 0xFFFFFFFFu;
+                }
+                status[l][i] = !any ? ST_EMPTY : (full ? ST_FULL : ST_KEPT);
+            }
+        }
+    }
+
+    // CountInteriorNodes (scene_builder.cpp:158-168) over the compacted tree.
+    void count(uint32_t l, uint32_t node, std::vector<uint32_t>& counts) const {
+        counts[l]++;
+        if (l == S.levels - 1) return;
+        std::vector<uint32_t> leaf, inter;
+        masks(l, node, leaf, inter);
+        const uint32_t* list = rec(l, node) + 4 + S.dims[l] * S.dims[l] * S.dims[l] / 16;
+        for (uint32_t w = 0; w < inter.size(); w++)
+            for (uint32_t b = 0; b < 32; b++)
+                if ((inter[w] >> b) & 1u) count(l + 1, list[w * 32 + b], counts);
+    }
+
+    // LayoutNode (scene_builder.cpp:199-238): the node's index at its level is
+    // claimed before its children, which follow in cell order (x, y, z loops =
+    // ascending bit index), so every level is numbered in depth-first preorder.
+    uint32_t layout(uint32_t l, uint32_t node) {
+        const uint32_t idx = next[l]++;
+        const uint32_t dim = S.dims[l], c3 = dim * dim * dim, W = c3 / 32;
+        std::vector<uint32_t> leaf, inter;
+        masks(l, node, leaf, inter);
+        const uint32_t* r = rec(l, node);
+        uint32_t* d = &D->nodes[D->node_ofs[l] + (uint64_t)idx * D->node_size[l]];
+        d[0] = r[0];
+        d[1] = r[1];
+        d[2] = r[2];
+        d[3] = r[3];
+        std::memcpy(d + 4, leaf.data(), W * 4);
+        if (l == S.levels - 1) return idx;
+        std::memcpy(d + 4 + W, inter.data(), W * 4);
+        const uint32_t* list = r + 4 + c3 / 16;
+        uint32_t* dlist = d + 4 + c3 / 16;
+        for (uint32_t c = 0; c < c3; c++) dlist[c] = 0xFFFFFFFFu;
+        for (uint32_t w = 0; w < W; w++)
+            for (uint32_t b = 0; b < 32; b++)
+                if ((inter[w] >> b) & 1u) dlist[w * 32 + b] = layout(l + 1, list[w * 32 + b]);
+        return idx;
+    }
+};
+
+}  // namespace
+
+extern "C" void* oracle_compact(void* tree, int prune) {
+    const Tree& S = *(const Tree*)tree;
+    Compactor C{S, prune, {}, nullptr, {}};
+    if (prune) C.compute_status();
+    std::vector<uint32_t> counts(S.levels, 0);
+    C.count(0, 0, counts);  // the root is always kept (BuildScene asserts it exists, :24-25)
+    auto* D = new Tree();
+    D->levels = S.levels;
+    std::memcpy(D->dims, S.dims, sizeof(D->dims));
+    std::memcpy(D->low, S.low, sizeof(D->low));
+    D->world_size = S.world_size;
+    std::memcpy(D->cell_size, S.cell_size, sizeof(D->cell_size));
+    std::memcpy(D->node_size, S.node_size, sizeof(D->node_size));
+    D->n_slots = S.n_slots;
+    D->tape_time = S.tape_time;
+    std::memcpy(D->work, S.work, sizeof(D->work));
+    uint64_t ofs = 0;
+    for (uint32_t l = 0; l < S.levels; l++) {
+        D->node_count[l] = counts[l];
+        D->node_ofs[l] = ofs;
+        ofs += (uint64_t)counts[l] * S.node_size[l];
+    }
+    D->nodes.assign(ofs, 0);
+    D->tapes = S.tapes;
+    C.D = D;
+    C.next.assign(S.levels, 0);
+    C.layout(0, 0);
+    return D;
+}
+
 // ---- raytracer (raytracer/main.comp) -----------------------------------------
 namespace {
 

@@ -64,6 +64,14 @@ void oracle_tree_tapes(void* tree, uint64_t* dst);
 // Work counters: per level, cell-instructions evaluated (interval or point).
 void oracle_tree_work(void* tree, uint64_t* cell_instr8);
 
+// Compaction of a voxelized tree (vulkan/src/engine/scene_builder.cpp): a new
+// tree handle in the same node layout whose levels are numbered in depth-first
+// preorder (LayoutNode, :199-238: children in ascending cell order). prune != 0
+// also applies BuildNode's rules (:91-156) bottom-up: a child node with no leaf
+// or interior cell is dropped, one whose cells are all leaves becomes a leaf
+// cell of its parent. The root is always kept. Tapes are unchanged (same pool).
+void* oracle_compact(void* tree, int prune);
+
 // ---- rendering --------------------------------------------------------------
 // camera: [pos3, fwd3, up3, fov_deg, ortho_width, projection, width, height,
 // jitter, jitter_seed] as floats (width/height/projection/jitter as values).

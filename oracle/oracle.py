@@ -61,6 +61,8 @@ def oracle_lib() -> C.CDLL:
         lib.oracle_tree_nodes.argtypes = [_P, _P]
         lib.oracle_tree_tapes.argtypes = [_P, _P]
         lib.oracle_tree_work.argtypes = [_P, _P]
+        lib.oracle_compact.argtypes = [_P, C.c_int]
+        lib.oracle_compact.restype = _P
         lib.oracle_render.argtypes = [_P, _P, C.c_uint32, _P, _P, _P, _P, C.c_uint32, C.c_float, _P, _P,
                                       C.c_int]
         _oracle = lib
@@ -216,6 +218,9 @@ class OracleTree:
                                               world_size, tape_time, rounding, 1 if shorten else 0, threads)
         if not self.h:
             raise ValueError("oracle_voxelize rejected its arguments")
+        self._read()
+
+    def _read(self):
         info = np.zeros(27, np.uint64)
         oracle_lib().oracle_tree_info(self.h, _p(info))
         self.levels = int(info[0])
@@ -229,6 +234,16 @@ class OracleTree:
         w = np.zeros(8, np.uint64)
         oracle_lib().oracle_tree_work(self.h, _p(w))
         self.work = [int(v) for v in w[: self.levels]]
+
+    def compact(self, prune: bool) -> "OracleTree":
+        """The tree compacted as SceneBuilder does (oracle_compact): levels in
+        depth-first preorder; with prune, empty children dropped and all-leaf
+        children turned into leaf cells."""
+        t = OracleTree.__new__(OracleTree)
+        t.dims, t.low_vertex, t.world_size, t.n_slots = list(self.dims), self.low_vertex, self.world_size, self.n_slots
+        t.h = oracle_lib().oracle_compact(self.h, 1 if prune else 0)
+        t._read()
+        return t
 
     def render(self, camera_vec, lights, tape_time=0.0, threads=None):
         """camera_vec: 16 floats (see frep_oracle.h); lights: a frep.Lights."""

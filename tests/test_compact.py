@@ -1,0 +1,184 @@
+"""Compact trees on the host (no GPU): the oracle's restatement of
+SceneBuilder's compaction (vulkan/src/engine/scene_builder.cpp: BuildNode
+:91-156, LayoutNode :199-238) and the library's blob format (frep.compact:
+pack / expand, and frep_compact_check, which needs no device)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import frep
+import oracle
+from frep import compact, scenes
+from frep._lib import ERR_INVALID_ARG, FrepError
+
+
+def _oracle(sc, rounding=1):
+    tape = frep.Tape(sc.shape)
+    return oracle.OracleTree(tape.wide(), tape.n_slots, sc.grid_dims, sc.low_vertex, sc.world_size,
+                             rounding=rounding, threads=8)
+
+
+@pytest.fixture(scope="module")
+def spheres():
+    return _oracle(scenes.spheres_union(16, seed=1, width=96, height=96))
+
+
+@pytest.fixture(scope="module")
+def three_level():
+    return _oracle(scenes.random_csg(24, seed=5, grid_dims=[8, 4, 4], width=96, height=64))
+
+
+def _records(t, l):
+    return t.nodes[t.node_offset[l]: t.node_offset[l] + t.node_count[l] * t.node_size[l]].reshape(
+        t.node_count[l], t.node_size[l])
+
+
+def _solid(t) -> np.ndarray:
+    """Finest-grid occupancy: every leaf cell of every node, expanded."""
+    fine = int(np.prod(t.dims))
+    occ = np.zeros((fine, fine, fine), bool)
+    for l, dim in enumerate(t.dims):
+        span = int(np.prod(t.dims[l + 1:]))
+        for rec in _records(t, l):
+            cells = compact._cells(rec[4:4 + dim ** 3 // 32])
+            x0, y0, z0 = (int(v) * dim for v in rec[1:4])
+            for c in cells:
+                x, y, z = x0 + c // (dim * dim), y0 + (c // dim) % dim, z0 + c % dim
+                occ[x * span:(x + 1) * span, y * span:(y + 1) * span, z * span:(z + 1) * span] = True
+    return occ
+
+
+def _children_in_preorder(t) -> bool:
+    """Children of consecutive nodes are consecutive, each in cell order."""
+    for l in range(t.levels - 1):
+        c3 = t.dims[l] ** 3
+        ids = [rec[4 + c3 // 16 + compact._cells(rec[4 + c3 // 32:4 + c3 // 16])] for rec in _records(t, l)]
+        ids = np.concatenate(ids) if ids else np.zeros(0)
+        if not np.array_equal(ids, np.arange(t.node_count[l + 1])):
+            return False
+    return True
+
+
+@pytest.mark.parametrize("which", ["spheres", "three_level"])
+def test_layout_keeps_every_node_in_preorder(which, request):
+    src = request.getfixturevalue(which)
+    c = src.compact(prune=False)
+    assert c.node_count == src.node_count
+    a, pa = oracle.canonical_of_oracle(src)
+    b, pb = oracle.canonical_of_oracle(c)
+    assert pa == [] and pb == [] and a == b
+    assert _children_in_preorder(c)
+
+
+@pytest.mark.parametrize("which", ["spheres", "three_level"])
+def test_prune_applies_buildnode_rules(which, request):
+    src = request.getfixturevalue(which)
+    p = src.compact(prune=True)
+    assert _children_in_preorder(p)
+    assert oracle.canonical_of_oracle(p)[1] == []
+    np.testing.assert_array_equal(_solid(p), _solid(src))
+    # no node below the root is empty or has only leaf cells
+    for l in range(1, p.levels):
+        w = p.dims[l] ** 3 // 32
+        last = l == p.levels - 1
+        for rec in _records(p, l):
+            leaf = rec[4:4 + w]
+            inter = np.zeros(w, np.uint32) if last else rec[4 + w:4 + 2 * w]
+            assert (leaf | inter).any()
+            assert not (leaf == 0xFFFFFFFF).all()
+    assert sum(p.node_count) <= sum(src.node_count)
+
+
+def test_pruning_removes_nodes_somewhere(three_level):
+    p = three_level.compact(prune=True)
+    assert sum(p.node_count) < sum(three_level.node_count)
+
+
+def test_layout_renders_like_the_source(spheres):
+    sc = scenes.spheres_union(16, seed=1, width=96, height=96)
+    c = spheres.compact(prune=False)
+    cam = oracle.camera_vector(sc.camera, 96, 96)
+    lights = frep.Lights(shadow_mask=1)
+    ra, ha = spheres.render(cam, lights)
+    rb, hb = c.render(cam, lights)
+    np.testing.assert_array_equal(ra, rb)
+    ka = oracle.hit_cells(ha, spheres.dims, spheres.node_offset, spheres.node_size, spheres.nodes)
+    kb = oracle.hit_cells(hb, c.dims, c.node_offset, c.node_size, c.nodes)
+    np.testing.assert_array_equal(ka, kb)
+    np.testing.assert_array_equal(ha[..., :4], hb[..., :4])  # depth and normal bits
+
+
+@pytest.mark.parametrize("which", ["spheres", "three_level"])
+def test_pack_expand_round_trip(which, request):
+    src = request.getfixturevalue(which)
+    blob = compact.pack(src.levels, src.dims, src.node_count, src.node_offset, src.node_size, src.nodes,
+                        src.tapes, src.low_vertex, src.world_size, src.n_slots)
+    compact.check(blob)
+    e = compact.expand(blob)
+    want = src.compact(prune=False)
+    assert e.node_count == want.node_count
+    assert e.node_size == want.node_size
+    np.testing.assert_array_equal(e.nodes, want.nodes)
+    np.testing.assert_array_equal(e.tapes, want.tapes)
+    again = compact.pack(e.levels, e.dims, e.node_count, e.node_offset, e.node_size, e.nodes, e.tapes,
+                         e.low_vertex, e.world_size, e.n_slots)
+    np.testing.assert_array_equal(again, blob)
+
+
+def test_pruned_tree_packs_to_a_valid_blob(three_level):
+    p = three_level.compact(prune=True)
+    blob = compact.pack(p.levels, p.dims, p.node_count, p.node_offset, p.node_size, p.nodes, p.tapes,
+                        p.low_vertex, p.world_size, p.n_slots)
+    compact.check(blob)
+    np.testing.assert_array_equal(compact.expand(blob).nodes, p.nodes)
+
+
+def _expect_invalid(blob, what):
+    with pytest.raises(FrepError) as ei:
+        compact.check(blob)
+    assert ei.value.status == ERR_INVALID_ARG, what
+
+
+def test_check_rejects_damaged_blobs(three_level):
+    t = three_level
+    good = compact.pack(t.levels, t.dims, t.node_count, t.node_offset, t.node_size, t.nodes, t.tapes,
+                        t.low_vertex, t.world_size, t.n_slots)
+    compact.check(good)
+    b = compact.parse(good)
+    w0 = t.dims[0] ** 3 // 32
+    nat = 120  # node section offset
+
+    def patched(word_index, value, dtype=np.uint32, at=nat):
+        out = good.copy()
+        out[at + word_index * np.dtype(dtype).itemsize: at + (word_index + 1) * np.dtype(dtype).itemsize] = \
+            np.array([value], dtype).view(np.uint8)
+        return out
+
+    bad = good.copy()
+    bad[0] = ord("X")
+    _expect_invalid(bad, "magic")
+    _expect_invalid(good[:-8], "truncated")
+    _expect_invalid(np.concatenate([good, np.zeros(8, np.uint8)]), "trailing bytes")
+    _expect_invalid(good[:100], "shorter than the header")
+    # header fields (byte offsets of frep_compact_header)
+    _expect_invalid(patched(0, 2, at=8), "version")
+    _expect_invalid(patched(0, 9, at=12), "levels")
+    _expect_invalid(patched(0, 6, at=16), "dims[0] not a multiple of 4")
+    _expect_invalid(patched(0, 2000, at=68), "n_slots")
+    _expect_invalid(patched(0, 2, at=72), "two roots")
+    # root record: [tape, leaf[W], interior[W], prefix[W], base]
+    inter = b.nodes[1 + w0:1 + 2 * w0]
+    wi = int(np.nonzero(inter)[0][0])
+    _expect_invalid(patched(1 + 2 * w0 + wi + 1, int(b.nodes[1 + 2 * w0 + wi + 1]) + 1), "prefix")
+    _expect_invalid(patched(1 + 3 * w0, 1), "base")
+    _expect_invalid(patched(1 + wi, int(b.nodes[1 + wi]) | int(inter[wi])), "leaf and interior")
+    _expect_invalid(patched(0, len(b.tapes) + 16), "tape index")
+    # a tape instruction with an out-of-range slot
+    tat = 120 + (4 * len(b.nodes) + 7) // 8 * 8
+    n = int(b.tapes[0] & 0xFFFFFFFF)
+    assert n > 0
+    w = int(b.tapes[1]) & ~(0xFFFF << 16) | ((t.n_slots + 3) << 16)
+    _expect_invalid(patched(1, w, np.uint64, at=tat), "slot")
+    # a record that runs past the pool
+    _expect_invalid(patched(0, (1 << 31), np.uint64, at=tat), "record length")
