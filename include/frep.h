@@ -403,6 +403,8 @@ typedef struct frep_compact_info {
  * voxelized or a bad mode. */
 frep_status frep_tree_compact(frep_ctx* ctx, frep_tree* tree, uint32_t mode, void* stream, frep_compact** out);
 frep_status frep_compact_get_info(const frep_compact* compact, frep_compact_info* info);
+/* Waits for the device (renders of the tree may be in flight on any stream),
+ * then frees it. */
 void frep_compact_destroy(frep_compact* compact);
 
 /* Raytracer::Trace over a compact tree: the same camera, lights, shading and

@@ -182,3 +182,30 @@ def test_check_rejects_damaged_blobs(three_level):
     _expect_invalid(patched(1, w, np.uint64, at=tat), "slot")
     # a record that runs past the pool
     _expect_invalid(patched(0, (1 << 31), np.uint64, at=tat), "record length")
+
+
+@pytest.mark.parametrize("rounding", [0, 1])
+@pytest.mark.parametrize("which", ["spheres", "three_level"])
+def test_tree_occupancy_equals_scenebuilder_point_sampling(which, rounding):
+    """SceneBuilder::BuildNode (scene_builder.cpp:91-156) decides every
+    finest voxel by the point value at its low corner,
+    WorldPosition = lowVertex + pos * worldSize / fineGridDim
+    (voxel_storage.h:58-61), through csg::Tape::Eval at T = 0. The interval
+    tree (leaf cells at any level, expanded) must give the same solid set.
+    The reference's own Tape::Eval is used where the reference bridge is built;
+    elsewhere frep_tape_eval, which is pinned bit-exact to it."""
+    sc = (scenes.spheres_union(16, seed=1, width=96, height=96) if which == "spheres"
+          else scenes.random_csg(24, seed=5, grid_dims=[8, 4, 4], width=96, height=64))
+    t = _oracle(sc, rounding)
+    occ = _solid(t)
+    fine = occ.shape[0]
+    ii = np.indices(occ.shape).reshape(3, -1).T.astype(np.float32)
+    low = np.asarray(sc.low_vertex, np.float32)
+    pos = (low + (ii * np.float32(sc.world_size)) / np.float32(fine)).astype(np.float32)
+    xyzt = np.concatenate([pos, np.zeros((len(pos), 1), np.float32)], 1)
+    if oracle.ref_available():
+        values = oracle.RefTape(*sc.shape.flatten()).eval(xyzt)
+    else:
+        values = frep.Tape(sc.shape).eval_points(xyzt)
+    np.testing.assert_array_equal(occ, (values < 0).reshape(occ.shape))
+    assert occ.sum() > 1000
