@@ -185,6 +185,19 @@ static frep_status validate_grid(const frep_grid* g) {
 }  // extern "C"
 
 namespace frep {
+namespace dev {
+
+// Writes a tree's static header and its self pointer. The header travels as a
+// kernel parameter, so enqueueing it never waits: a cudaMemcpyAsync from
+// pageable host memory may wait for the stream's earlier work, which blocks
+// the serving scheduler (it creates trees while it holds its lock).
+__global__ void tree_header_write_kernel(const TreeHeader h, TreeHeader* dst, TreeHeader** self) {
+    *dst = h;
+    *self = dst;
+}
+
+}  // namespace dev
+
 namespace detail {
 
 uint64_t tree_external_bytes(uint64_t node_words, uint64_t tape_words) {
@@ -292,9 +305,9 @@ frep_status tree_create_impl(frep_ctx* ctx, const frep_grid* grid, const frep_vo
     t->d_prefix = t->d_small + 1;
     t->d_cursor = t->d_small + 3;
     cudaError_t ce;
-    if (ext) {  // pageable sources: the copies are staged before the calls return
-        ce = cudaMemcpyAsync(t->hdr, &h, sizeof(h), cudaMemcpyHostToDevice, stream);
-        if (ce == cudaSuccess) ce = cudaMemcpyAsync(t->d_self, &t->hdr, sizeof(void*), cudaMemcpyHostToDevice, stream);
+    if (ext) {  // ordered on the caller's stream, without a host wait
+        frep::dev::tree_header_write_kernel<<<1, 1, 0, stream>>>(h, t->hdr, t->d_self);
+        ce = cudaGetLastError();
     } else {
         ce = cudaMemcpy(t->hdr, &h, sizeof(h), cudaMemcpyHostToDevice);
         if (ce == cudaSuccess) ce = cudaMemcpy(t->d_self, &t->hdr, sizeof(void*), cudaMemcpyHostToDevice);

@@ -389,6 +389,18 @@ struct DevBufs {
     }
 };
 
+// Carves 256-byte-aligned pieces from one block (base null: sizes only).
+struct Carve {
+    uint8_t* base = nullptr;
+    uint64_t at = 0;
+    template <typename T>
+    T* take(uint64_t count) {
+        T* p = reinterpret_cast<T*>(base + at);
+        at += align_up(std::max<uint64_t>(count, 1) * sizeof(T), 256);
+        return p;
+    }
+};
+
 bool valid_dims(uint32_t levels, const uint32_t* dims) {
     if (levels == 0 || levels > FREP_MAX_LEVELS) return false;
     for (uint32_t l = 0; l < levels; l++)
@@ -454,17 +466,32 @@ frep_status frep_tree_compact(frep_ctx* ctx, frep_tree* tree, uint32_t mode, voi
     uint64_t* dtapes;
     uint8_t* status;
     CompactHeader* H;
+    // The result's two buffers (kept when already exact) and one block for
+    // everything else: few allocations, few synchronizing frees.
+    Carve cv;
+    for (int pass = 0; pass < 2; pass++) {
+        cv.at = 0;
+        order0 = cv.take<uint32_t>(max_count);
+        order1 = cv.take<uint32_t>(max_count);
+        cnt = cv.take<uint32_t>(max_count);
+        base = cv.take<uint32_t>(max_count);
+        status = cv.take<uint8_t>(mode ? sum_count : 1);
+        mark = cv.take<uint32_t>(slots);
+        newofs = cv.take<uint32_t>(slots);
+        partials = cv.take<uint32_t>(frep::dev::SCAN_BLOCKS);
+        H = cv.take<CompactHeader>(1);
+        if (pass == 0) {
+            uint8_t* block = nullptr;
+            cudaError_t be = tmp.alloc(&block, cv.at);
+            if (be != cudaSuccess) {
+                cudaGetLastError();
+                return fail(FREP_ERR_OOM, "frep_tree_compact: cudaMalloc failed (%s)", cudaGetErrorString(be));
+            }
+            cv.base = block;
+        }
+    }
     cudaError_t e = tmp.alloc(&dnodes, node_bound);
     if (e == cudaSuccess) e = tmp.alloc(&dtapes, tape_top);
-    if (e == cudaSuccess) e = tmp.alloc(&order0, max_count);
-    if (e == cudaSuccess) e = tmp.alloc(&order1, max_count);
-    if (e == cudaSuccess) e = tmp.alloc(&cnt, max_count);
-    if (e == cudaSuccess) e = tmp.alloc(&base, max_count);
-    if (e == cudaSuccess) e = tmp.alloc(&status, mode ? sum_count : 1);
-    if (e == cudaSuccess) e = tmp.alloc(&mark, slots);
-    if (e == cudaSuccess) e = tmp.alloc(&newofs, slots);
-    if (e == cudaSuccess) e = tmp.alloc(&partials, frep::dev::SCAN_BLOCKS);
-    if (e == cudaSuccess) e = tmp.alloc(&H, 1);
     if (e != cudaSuccess) {
         cudaGetLastError();
         return fail(FREP_ERR_OOM, "frep_tree_compact: cudaMalloc failed (%s)", cudaGetErrorString(e));

@@ -177,3 +177,32 @@ def test_compact_refuses_unfinished_trees(ctx):
     with pytest.raises(frep.FrepError) as e:
         frep.CompactTree.from_storage(ctx, vs2)
     assert e.value.status == frep._lib.ERR_CAPACITY
+
+
+def test_compact_of_batched_and_reused_trees(ctx):
+    """Trees voxelized by a batch (frep_batch_voxelize) and by reuse of a
+    previous frame (frep_voxelize_reuse) compact to the oracle's compaction of
+    the same tape, like trees voxelized alone."""
+    scs = [scenes.random_csg(12 + 10 * i, seed=60 + i, grid_dims=list(d), width=64, height=48)
+           for i, d in enumerate([(16, 4), (8, 8, 4), (16, 4, 4)])]
+    storages = [frep.VoxelStorage(sc.grid_dims, sc.low_vertex, sc.world_size).init(ctx, sc.shape) for sc in scs]
+    batch = frep.Batch(ctx, storages)
+    times = [0.0, 0.2, 0.4]
+    batch.voxelize(times)
+    for sc, vs, t in zip(scs, storages, times):
+        for prune in (False, True):
+            e = compact.expand(frep.CompactTree.from_storage(ctx, vs, prune=prune).export())
+            orc = oracle_tree(sc, vs.tape, rounding=1, tape_time=t).compact(prune)
+            assert compare_compact(e, orc) == [], (sc.grid_dims, prune)
+    batch.close()
+
+    sc = scenes.animated_csg(40, 3, seed=13, grid_dims=[16, 8, 4], width=64, height=48)
+    tape = frep.Tape(sc.shape)
+    a = frep.VoxelStorage(sc.grid_dims, sc.low_vertex, sc.world_size).init(ctx, tape)
+    b = frep.VoxelStorage(sc.grid_dims, sc.low_vertex, sc.world_size).init(ctx, tape)
+    frep.Voxelizer(ctx, a).voxelize(0.25)
+    frep.Voxelizer(ctx, b).voxelize(0.3, reuse=a)
+    for prune in (False, True):
+        e = compact.expand(frep.CompactTree.from_storage(ctx, b, prune=prune).export())
+        orc = oracle_tree(sc, tape, rounding=1, tape_time=0.3).compact(prune)
+        assert compare_compact(e, orc) == [], prune
