@@ -187,10 +187,9 @@ static frep_status validate_grid(const frep_grid* g) {
 namespace frep {
 namespace dev {
 
-// Writes a tree's static header and its self pointer. The header travels as a
-// kernel parameter, so enqueueing it never waits: a cudaMemcpyAsync from
-// pageable host memory may wait for the stream's earlier work, which blocks
-// the serving scheduler (it creates trees while it holds its lock).
+// Writes a tree's static header and its self pointer (trees in caller
+// memory). The header travels as a kernel parameter: a cudaMemcpyAsync from
+// pageable host memory may wait for the stream's earlier work.
 __global__ void tree_header_write_kernel(const TreeHeader h, TreeHeader* dst, TreeHeader** self) {
     *dst = h;
     *self = dst;
@@ -206,8 +205,9 @@ uint64_t tree_external_bytes(uint64_t node_words, uint64_t tape_words) {
 
 // Creates a tree; with `ext` its header, work prefix and pools are carved
 // from that caller-owned device memory (the serving loop's arena) instead of
-// cudaMalloc'd, the header upload is ordered on `stream`, and nothing is
-// charged to the context's budget.
+// cudaMalloc'd, the device header is written later (write_tree_header, on
+// the stream that first uses the tree), and nothing is charged to the
+// context's budget.
 frep_status tree_create_impl(frep_ctx* ctx, const frep_grid* grid, const frep_voxelize_opts* opts, uint8_t* ext,
                              uint64_t ext_bytes, cudaStream_t stream, frep_tree** out) {
     if (!ctx || !grid || !out) return fail(FREP_ERR_INVALID_ARG, "frep_tree_create: null argument");
@@ -304,10 +304,10 @@ frep_status tree_create_impl(frep_ctx* ctx, const frep_grid* grid, const frep_vo
     t->d_self = reinterpret_cast<frep::dev::TreeHeader**>(t->d_small);
     t->d_prefix = t->d_small + 1;
     t->d_cursor = t->d_small + 3;
-    cudaError_t ce;
-    if (ext) {  // ordered on the caller's stream, without a host wait
-        frep::dev::tree_header_write_kernel<<<1, 1, 0, stream>>>(h, t->hdr, t->d_self);
-        ce = cudaGetLastError();
+    cudaError_t ce = cudaSuccess;
+    if (ext) {  // written later by write_tree_header
+        t->pending_hdr = h;
+        t->hdr_pending = true;
     } else {
         ce = cudaMemcpy(t->hdr, &h, sizeof(h), cudaMemcpyHostToDevice);
         if (ce == cudaSuccess) ce = cudaMemcpy(t->d_self, &t->hdr, sizeof(void*), cudaMemcpyHostToDevice);
@@ -330,6 +330,14 @@ frep_status tree_create_impl(frep_ctx* ctx, const frep_grid* grid, const frep_vo
         ctx->used += bytes;
     }
     *out = t;
+    return FREP_OK;
+}
+
+frep_status write_tree_header(frep_tree* t, cudaStream_t stream) {
+    if (!t->hdr_pending) return FREP_OK;
+    frep::dev::tree_header_write_kernel<<<1, 1, 0, stream>>>(t->pending_hdr, t->hdr, t->d_self);
+    FREP_CUDA(cudaGetLastError());
+    t->hdr_pending = false;
     return FREP_OK;
 }
 

@@ -29,9 +29,15 @@ struct frep_tree;
 namespace frep {
 namespace detail {
 // Trees whose header and pools are carved from caller-owned device memory.
+// With such memory the device header is not written here: the tree keeps it
+// (hdr_pending) until write_tree_header enqueues it on a stream, so that a
+// caller holding a lock creates trees without touching the device.
 uint64_t tree_external_bytes(uint64_t node_words, uint64_t tape_words);
 frep_status tree_create_impl(frep_ctx* ctx, const frep_grid* grid, const frep_voxelize_opts* opts, uint8_t* ext,
                              uint64_t ext_bytes, cudaStream_t stream, frep_tree** out);
+// Enqueues the pending header write of a tree in caller memory (no-op when
+// already written); the tree is usable on `stream` afterwards.
+frep_status write_tree_header(frep_tree* tree, cudaStream_t stream);
 // Camera basis, lights and tree description for one frame (frep_render).
 frep_status fill_render_args(const frep_tree* tree, const frep_camera* cam, const frep_lights* lights,
                              float tape_time, const frep_image* out, RenderArgs* args);
@@ -70,6 +76,8 @@ struct frep_tree {
     frep_voxelize_opts opts{};
     int point_k = 4;  // cells per lane of the last-level pass
     bool external = false;  // header and pools live in caller-owned memory
+    bool hdr_pending = false;              // external: header not yet written to the device
+    frep::dev::TreeHeader pending_hdr{};   //   (write_tree_header)
     float cell_size[FREP_MAX_LEVELS] = {};
     uint32_t node_size[FREP_MAX_LEVELS] = {};
     frep::dev::TreeHeader* hdr = nullptr;

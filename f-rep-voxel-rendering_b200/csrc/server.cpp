@@ -362,7 +362,11 @@ frep_status enqueue_step(frep_server* sv, StepPlan& P) {
     frep_status r = FREP_OK;
     cudaStream_t s = sv->stream;
     Step& st = P.step;
-    if (!P.vtrees.empty()) {
+    // headers of the trees admitted while the step was planned (under the
+    // lock, where nothing is enqueued: a launch can wait for queue space)
+    for (frep_tree* t : P.vtrees)
+        if (r == FREP_OK) r = frep::detail::write_tree_header(t, s);
+    if (r == FREP_OK && !P.vtrees.empty()) {
         if (!sv->batch) {
             r = frep_batch_create(sv->ctx, P.vtrees.data(), (uint32_t)P.vtrees.size(), &sv->batch);
             if (r == FREP_OK && (sv->cfg.interval_warps_per_block || sv->cfg.point_warps_per_block))
