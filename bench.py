@@ -69,6 +69,8 @@ def parse():
                     help="large / stress: tree branching per level (default 16,16,8 / 16,16,4,4)")
     ap.add_argument("--res", default=None, help="render resolution WxH (batch 512x512, large 1920x1080)")
     ap.add_argument("--pool-mb", type=int, default=3072, help="large: node + tape pool size of the tree, MB")
+    ap.add_argument("--point-k", type=int, default=0, choices=(0, 2, 4, 8),
+                    help="large / stress / animated: cells per lane of the last-level pass (0 = library default)")
     ap.add_argument("--no-compact", action="store_true",
                     help="large: skip the compact-tree measurements (compaction time, bytes, render time)")
     args = ap.parse_args()
@@ -279,7 +281,7 @@ def run_ours(args, world, rank, local):
         pool = args.pool_mb << 20
         node_words, tape_words = pool // 4 // 4, pool * 3 // 4 // 8
     vs = frep.VoxelStorage(scene.grid_dims, scene.low_vertex, scene.world_size, rounding=frep.ROUND_OUTWARD,
-                           node_words=node_words, tape_words=tape_words)
+                           node_words=node_words, tape_words=tape_words, point_cells_per_lane=args.point_k)
     vs.init(ctx, scene.shape)
     vox = frep.Voxelizer(ctx, vs)
     # the animated scene alternates two trees, each frame reusing the other
@@ -289,7 +291,7 @@ def run_ours(args, world, rank, local):
     if anim:
         storages.append(frep.VoxelStorage(scene.grid_dims, scene.low_vertex, scene.world_size,
                                           rounding=frep.ROUND_OUTWARD, node_words=node_words,
-                                          tape_words=tape_words).init(ctx, vs.tape))
+                                          tape_words=tape_words, point_cells_per_lane=args.point_k).init(ctx, vs.tape))
     rt = frep.Raytracer(ctx, vs)
     rt.lights = frep.Lights(shadow_mask=scene.shadow_mask)
     W, H = scene.width, scene.height
@@ -412,7 +414,7 @@ def run_ours(args, world, rank, local):
         "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": args.workload_name, "grid": scene.grid_dims, "resolution": [W, H], "shadow_rays": 1,
-                   "tape_instructions": vs.tape.n_instr, "rounding": "outward",
+                   "tape_instructions": vs.tape.n_instr, "rounding": "outward", "point_cells_per_lane": args.point_k or "default",
                    "nodes_per_level": list(info.node_count[:vs.grid_levels]),
                    "l2": "flushed between timed steps (256 MB write, outside the step events)",
                    "parallelism": f"replicas x{world}"},

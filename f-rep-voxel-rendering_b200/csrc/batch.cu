@@ -367,6 +367,9 @@ frep_status check_trees(frep_ctx* ctx, frep_tree* const* trees, uint32_t n, int*
         if (i == 0) *rounding = (int)trees[0]->opts.rounding;
         if ((int)trees[i]->opts.rounding != *rounding)
             return fail(FREP_ERR_INVALID_ARG, "frep_batch: all trees of a batch use the same rounding");
+        // the batch runs its last-level passes with 4 and 2 cells per lane
+        if (trees[i]->point_k == 8)
+            return fail(FREP_ERR_UNSUPPORTED, "frep_batch: tree %u uses 8 cells per lane in its last level", i);
     }
     return FREP_OK;
 }

@@ -224,13 +224,15 @@ frep_status tree_create_impl(frep_ctx* ctx, const frep_grid* grid, const frep_vo
     {
         const uint32_t dl = grid->dims[grid->levels - 1];
         const uint32_t k = t->opts.point_cells_per_lane;
-        if (k != 0 && k != 2 && k != 4) {
+        if (k != 0 && k != 2 && k != 4 && k != 8) {
             delete t;
-            return fail(FREP_ERR_INVALID_ARG, "opts.point_cells_per_lane must be 0, 2 or 4");
+            return fail(FREP_ERR_INVALID_ARG, "opts.point_cells_per_lane must be 0, 2, 4 or 8");
         }
-        if (k == 4 && (dl * dl * dl / 32) % 4 != 0) {
+        if (k && (dl * dl * dl / 32) % k != 0) {
             delete t;
-            return fail(FREP_ERR_INVALID_ARG, "opts.point_cells_per_lane = 4 needs a last-level dim of 8 or more");
+            return fail(FREP_ERR_INVALID_ARG, "opts.point_cells_per_lane = %u does not divide the last level's %u mask "
+                        "words (4 and 8 need a last-level dim that is a multiple of 8)",
+                        k, dl * dl * dl / 32);
         }
         t->point_k = k ? (int)k : frep::point_k_for(dl);
     }

@@ -608,6 +608,8 @@ frep_status frep_server_add_scene(frep_server* sv, const frep_tape* tape, const 
     for (uint32_t l = 0; l < grid->levels; l++)
         if (grid->dims[l] < 4 || grid->dims[l] > 32 || grid->dims[l] % 4)
             return fail(FREP_ERR_INVALID_ARG, "frep_server_add_scene: dims[%u] = %u", l, grid->dims[l]);
+    if (opts && opts->point_cells_per_lane != 0 && opts->point_cells_per_lane != 2 && opts->point_cells_per_lane != 4)
+        return fail(FREP_ERR_INVALID_ARG, "frep_server_add_scene: point_cells_per_lane must be 0, 2 or 4");
     auto S = std::make_unique<Scene>();
     S->tape = *tape;
     S->grid = *grid;

@@ -920,18 +920,27 @@ interval_level_kernel(LevelLaunch p) {
 // The leaf bit is the sign of the point value at the cell's low corner
 // (voxelize_point, main.comp:74-83; tape_eval_point, point.comp:2-63).
 // Each lane evaluates K cells at once (cells grp*32K + k*32 + lane; K = 4, or
-// 2 for nodes too small for 4), so one decoded instruction drives 32*K
-// evaluations and a lane's slot row is one K-float vector. A tape that fits one
+// 2 for nodes too small for 4, or 8 on request), so one decoded instruction
+// drives 32*K evaluations and a lane's slot row is one K-float vector (two
+// for K = 8). A tape that fits one
 // staged chunk stays staged across consecutive items of the same node.
 template <int K>
 struct alignas(4 * K) FK {
     float v[K];
 };
 
+// K = 8: a slot row is two halves of 32 lanes x 16 bytes ([slot][half][lane]),
+// so that each 16-byte access of the warp stays conflict-free.
+constexpr uint32_t K8_HALF = 32 * 16;
+
 template <int K>
 __device__ __forceinline__ FK<K> lds_k(uint32_t a) {
     FK<K> r;
-    if constexpr (K == 4) {
+    if constexpr (K == 8) {
+        const float4 v = lds_f4(a), w = lds_f4(a + K8_HALF);
+        r.v[0] = v.x; r.v[1] = v.y; r.v[2] = v.z; r.v[3] = v.w;
+        r.v[4] = w.x; r.v[5] = w.y; r.v[6] = w.z; r.v[7] = w.w;
+    } else if constexpr (K == 4) {
         const float4 v = lds_f4(a);
         r.v[0] = v.x; r.v[1] = v.y; r.v[2] = v.z; r.v[3] = v.w;
     } else {
@@ -942,7 +951,10 @@ __device__ __forceinline__ FK<K> lds_k(uint32_t a) {
 }
 template <int K>
 __device__ __forceinline__ void sts_k(uint32_t a, const FK<K>& r) {
-    if constexpr (K == 4) sts_f4(a, make_float4(r.v[0], r.v[1], r.v[2], r.v[3]));
+    if constexpr (K == 8) {
+        sts_f4(a, make_float4(r.v[0], r.v[1], r.v[2], r.v[3]));
+        sts_f4(a + K8_HALF, make_float4(r.v[4], r.v[5], r.v[6], r.v[7]));
+    } else if constexpr (K == 4) sts_f4(a, make_float4(r.v[0], r.v[1], r.v[2], r.v[3]));
     else sts_f2(a, make_float2(r.v[0], r.v[1]));
 }
 
@@ -1005,7 +1017,7 @@ point_level_kernel(LevelLaunch p) {
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned char* wbase = smem + (size_t)warp * p.smem_per_warp;
     constexpr uint32_t ROW = 4 * K;  // bytes per lane per slot
-    const uint32_t lane_base = smem_addr(wbase) + lane * ROW;
+    const uint32_t lane_base = smem_addr(wbase) + lane * (K == 8 ? 16u : ROW);
     uint4* stage = reinterpret_cast<uint4*>(wbase + (size_t)p.n_slots * 32 * ROW);
     if (lane == 0) stage[STAGE] = make_uint4(0u, 0u, 0u, 0u);  // sentinel past a full chunk
 
@@ -1348,6 +1360,7 @@ cudaError_t plan_levels(uint32_t n_slots, uint32_t mm_cap, int point_k, int roun
         e = ki == 2 ? plan_interval<2>(four, rounding, iv, plan) : plan_interval<1>(four, rounding, iv, plan);
     if (e != cudaSuccess) return e;
     plan->point_k = point_k;
+    if (point_k == 8) return plan_point<8>(n_slots, plan, point_warps);
     return point_k == 4 ? plan_point<4>(n_slots, plan, point_warps) : plan_point<2>(n_slots, plan, point_warps);
 }
 
@@ -1379,7 +1392,10 @@ cudaError_t launch_level(const LevelLaunch& a, const LevelPlan& plan, int roundi
         b.smem_per_warp = plan.point_smem_per_warp;
         const int w4 = plan.point_warps_per_block == 4;
         const size_t smem = (size_t)plan.point_warps_per_block * plan.point_smem_per_warp;
-        if (plan.point_k == 4) {
+        if (plan.point_k == 8) {
+            if (w4) dev::point_level_kernel<4, 8><<<plan.point_blocks, 128, smem, stream>>>(b);
+            else dev::point_level_kernel<1, 8><<<plan.point_blocks, 32, smem, stream>>>(b);
+        } else if (plan.point_k == 4) {
             if (w4) dev::point_level_kernel<4, 4><<<plan.point_blocks, 128, smem, stream>>>(b);
             else dev::point_level_kernel<1, 4><<<plan.point_blocks, 32, smem, stream>>>(b);
         } else {

@@ -8,9 +8,11 @@ import frep
 import oracle
 
 
-def device_tree(ctx, scene, rounding=1, tape_time=0.0, shorten=True, node_words=0, tape_words=0):
+def device_tree(ctx, scene, rounding=1, tape_time=0.0, shorten=True, node_words=0, tape_words=0,
+                point_cells_per_lane=0):
     vs = frep.VoxelStorage(scene.grid_dims, scene.low_vertex, scene.world_size, rounding=rounding,
-                           shorten=shorten, node_words=node_words, tape_words=tape_words)
+                           shorten=shorten, node_words=node_words, tape_words=tape_words,
+                           point_cells_per_lane=point_cells_per_lane)
     vs.init(ctx, scene.shape)
     frep.Voxelizer(ctx, vs).voxelize(tape_time)
     return vs

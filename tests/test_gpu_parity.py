@@ -73,6 +73,32 @@ def test_last_level_dims(ctx, dims):
     np.testing.assert_array_equal(d_rgba, o_rgba)
 
 
+@pytest.mark.parametrize("dims,k", [((16, 8), 8), ((8, 16), 8), ((4, 4, 8), 8), ((8, 16), 2)])
+def test_last_level_cells_per_lane_option(ctx, dims, k):
+    """frep_voxelize_opts.point_cells_per_lane = 8 (and 2 where 4 is the
+    default): the same tree and image."""
+    sc = _small_random(28, 9, list(dims))
+    vs = device_tree(ctx, sc, rounding=1, point_cells_per_lane=k)
+    exp = vs.export()
+    orc = oracle_tree(sc, vs.tape, rounding=1)
+    assert compare_trees(exp, orc) == []
+    d_rgba, d_hits, o_rgba, o_hits = render_both(ctx, vs, orc, sc, frep.Lights())
+    assert compare_hits(d_hits, o_hits, exp, orc) == []
+    np.testing.assert_array_equal(d_rgba, o_rgba)
+
+
+def test_cells_per_lane_option_is_checked(ctx):
+    sc = _small_random(8, 3, [8, 12])
+    for k in (3, 4, 8):  # 54 mask words per last-level node: neither 4 nor 8 divides it
+        with pytest.raises(frep.FrepError) as e:
+            device_tree(ctx, sc, point_cells_per_lane=k)
+        assert e.value.status == frep._lib.ERR_INVALID_ARG
+    vs = frep.VoxelStorage([8, 16], sc.low_vertex, sc.world_size, point_cells_per_lane=8).init(ctx, sc.shape)
+    with pytest.raises(frep.FrepError) as e:  # batches run 2 or 4 cells per lane
+        frep.Batch(ctx, [vs])
+    assert e.value.status == frep._lib.ERR_UNSUPPORTED
+
+
 def test_wide_tape_scene(ctx):
     """More than 256 constants: only the wide encoding can hold this tape."""
     sc = _small_random(160, 9, [16, 8])
