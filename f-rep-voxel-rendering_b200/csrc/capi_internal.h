@@ -74,7 +74,8 @@ struct frep_tree {
     frep_ctx* ctx = nullptr;
     frep_grid grid{};
     frep_voxelize_opts opts{};
-    int point_k = 4;  // cells per lane of the last-level pass
+    int point_k = 4;  // cells per lane of the last-level pass in batches (its batch kind, 4 or 2)
+    int plain_k = 4;  // cells per lane of its own last-level passes (frep_voxelize and variants)
     bool external = false;  // header and pools live in caller-owned memory
     bool hdr_pending = false;              // external: header not yet written to the device
     frep::dev::TreeHeader pending_hdr{};   //   (write_tree_header)

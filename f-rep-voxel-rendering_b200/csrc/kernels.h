@@ -27,6 +27,9 @@ struct LevelLaunch {
     const uint32_t* eval_list;         // one-tree launches that copy subtrees from a previous
                                        //   tree: the nodes to evaluate (reuse_eval[level] of
                                        //   them, listed by reuse_match_kernel); null = all
+    uint32_t any_point_k;              // 1: a one-tree launch, whose last level runs with the
+                                       //   launch's cells per lane whatever the tree's batch
+                                       //   kind (TreeHeader::point_k); 0: only trees of that kind
 };
 
 // Per-warp global scratch of the interval pass, in u32 words: one keep mask per

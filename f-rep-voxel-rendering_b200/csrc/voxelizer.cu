@@ -1133,13 +1133,13 @@ point_level_kernel(LevelLaunch p) {
 // cells per lane). Interval passes also fix where each tree's next level
 // starts (node_ofs[level + 1]). One block.
 __device__ __forceinline__ unsigned long long level_items(TreeHeader* H, uint32_t L, int point, int k,
-                                                          bool write_ofs, bool reuse) {
+                                                          bool write_ofs, bool reuse, bool any_k) {
     if (L >= H->levels) return 0;
     const bool last = L == H->levels - 1;
     if ((point != 0) != last) return 0;
     const uint32_t dim = H->dims[L];
     const uint32_t words = dim * dim * dim / 32;
-    if (point && H->point_k != (uint32_t)k) return 0;
+    if (point && !any_k && H->point_k != (uint32_t)k) return 0;
     const uint32_t count = level_count(H, L, H->node_cap, H->node_size[L]);
     if (!point && write_ofs) H->node_ofs[L + 1] = H->node_ofs[L] + (unsigned long long)count * H->node_size[L];
     // with reuse, only the listed nodes are evaluated
@@ -1149,13 +1149,13 @@ __device__ __forceinline__ unsigned long long level_items(TreeHeader* H, uint32_
 
 __global__ void __launch_bounds__(1024)
 level_scan_kernel(TreeHeader* const* trees, uint32_t n, uint32_t L, int point, int point_k,
-                  unsigned long long* prefix, unsigned long long* cursor, int reuse) {
+                  unsigned long long* prefix, unsigned long long* cursor, int reuse, int any_k) {
     __shared__ unsigned long long part[1024];
     const uint32_t t = threadIdx.x, T = blockDim.x;
     const uint32_t per = (n + T - 1) / T;
     const uint32_t b = min(n, t * per), e = min(n, b + per);
     unsigned long long sum = 0;
-    for (uint32_t i = b; i < e; i++) sum += level_items(trees[i], L, point, point_k, true, reuse != 0);
+    for (uint32_t i = b; i < e; i++) sum += level_items(trees[i], L, point, point_k, true, reuse != 0, any_k != 0);
     part[t] = sum;
     __syncthreads();
     for (uint32_t off = 1; off < T; off <<= 1) {  // inclusive scan
@@ -1167,7 +1167,7 @@ level_scan_kernel(TreeHeader* const* trees, uint32_t n, uint32_t L, int point, i
     unsigned long long run = part[t] - sum;
     for (uint32_t i = b; i < e; i++) {
         prefix[i] = run;
-        run += level_items(trees[i], L, point, point_k, false, reuse != 0);
+        run += level_items(trees[i], L, point, point_k, false, reuse != 0, any_k != 0);
     }
     if (t == T - 1) prefix[n] = part[t];
     if (t == 0) *cursor = 0ull;
@@ -1381,7 +1381,7 @@ cudaError_t launch_tree_init_staged(dev::TreeHeader* const* trees, uint32_t n, c
 
 cudaError_t launch_level_scan(const LevelLaunch& a, bool point, int point_k, cudaStream_t stream) {
     dev::level_scan_kernel<<<1, 1024, 0, stream>>>(a.trees, a.n_trees, a.level, point ? 1 : 0, point_k, a.prefix,
-                                                   a.cursor, a.eval_list ? 1 : 0);
+                                                   a.cursor, a.eval_list ? 1 : 0, a.any_point_k ? 1 : 0);
     return cudaGetLastError();
 }
 
