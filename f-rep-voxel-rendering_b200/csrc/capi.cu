@@ -228,14 +228,11 @@ frep_status tree_create_impl(frep_ctx* ctx, const frep_grid* grid, const frep_vo
             delete t;
             return fail(FREP_ERR_INVALID_ARG, "opts.point_cells_per_lane must be 0, 2, 4 or 8");
         }
-        // k must divide the node's mask words; 4 also takes dim-4 nodes (2
-        // words) in pairs
-        const uint32_t words = dl * dl * dl / 32;
-        if (k && words % k != 0 && !(k == 4 && words == 2)) {
+        if (k && (dl * dl * dl / 32) % k != 0) {
             delete t;
-            return fail(FREP_ERR_INVALID_ARG, "opts.point_cells_per_lane = %u does not fit the last level's %u mask "
-                        "words (8 needs a last-level dim that is a multiple of 8; 4 one that is 4 or a multiple "
-                        "of 8)", k, words);
+            return fail(FREP_ERR_INVALID_ARG, "opts.point_cells_per_lane = %u does not divide the last level's %u mask "
+                        "words (4 and 8 need a last-level dim that is a multiple of 8)",
+                        k, dl * dl * dl / 32);
         }
         t->point_k = k ? (int)k : frep::point_k_for(dl);
         // Alone, a tree takes 8 cells per lane where its nodes allow (the

@@ -1010,11 +1010,8 @@ __device__ __forceinline__ void pt_exec(const uint4 d, FK<K>& r, uint32_t lane_b
     }
 }
 
-// Registers capped at 80 (24 resident warps: the shared-memory limit of the
-// 4-cells-per-lane plan): with 8 cells per lane 8 bytes of spills instead of
-// 200 at the compiler's own choice of 64.
 template <int WARPS, int K>
-__global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 6 : 24)
+__global__ void __launch_bounds__(WARPS * 32)
 point_level_kernel(LevelLaunch p) {
     extern __shared__ __align__(16) unsigned char smem[];
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -1032,13 +1029,7 @@ point_level_kernel(LevelLaunch p) {
     const uint64_t* staged_pool = nullptr;
     LevelTree T{};
     unsigned long long t_lo = 0, t_hi = 0;
-    uint32_t n_nodes = 0;  // nodes of the current tree this pass evaluates
     bool have_tree = false;
-    // Nodes of fewer mask words than K (dim 4: 2 words) go K / words to an
-    // item (K = 4: a pair of consecutive nodes); the pair is evaluated in one
-    // run of the tape when both nodes use the same tape record (siblings of a
-    // 32-cell group often share one), else in one run per tape.
-    constexpr uint32_t NP = K == 4 ? 2 : 1;
 
     unsigned long long first;
     uint32_t got;
@@ -1052,113 +1043,82 @@ point_level_kernel(LevelLaunch p) {
                 t_lo = __ldcg(&p.prefix[ti]);
                 t_hi = __ldcg(&p.prefix[ti + 1]);
                 T = load_tree(p.trees[ti], L, true);
-                n_nodes = level_count(T.H, L, T.H->node_cap, T.node_size);
-                if (p.eval_list) n_nodes = min(n_nodes, T.H->reuse_eval[L]);
                 have_tree = true;
             }
             const uint32_t dim = T.dim;
             const uint32_t words = dim * dim * dim / 32;      // mask words per node
-            const uint32_t np = (NP > 1 && words < (uint32_t)K) ? NP : 1u;  // nodes per item
-            const uint32_t groups = np > 1 ? 1u : words / K;  // items per node
+            const uint32_t groups = words / K;                // items per node
             const float cs = T.cs;
             const unsigned long long local = item - t_lo;
             const uint32_t grp = (uint32_t)(local % groups);
-            const uint32_t first_node = (uint32_t)(local / groups) * np;
-            uint32_t* recs[NP];
-            uint32_t tidx[NP];
-            uint32_t pending = 0;  // nodes of the item still to evaluate
+            uint32_t node = (uint32_t)(local / groups);
+            if (p.eval_list) node = __ldcg(&p.eval_list[node]);  // the others are copies
+            uint32_t* rec = T.nodes + T.ofs_l + (size_t)node * T.node_size;
+            const uint32_t tape_idx = rec[0];
+            const uint64_t* tape = T.tapes + tape_idx + 1;
+            const uint32_t n = (uint32_t)__ldcg(&T.tapes[tape_idx]);
+            const uint32_t ncx = rec[1], ncy = rec[2], ncz = rec[3];
+            FK<K> px, py, pz, pt;
 #pragma unroll
-            for (uint32_t j = 0; j < NP; j++) {
-                recs[j] = nullptr;
-                tidx[j] = 0u;
-                if (j < np && first_node + j < n_nodes) {
-                    uint32_t node = first_node + j;
-                    if (p.eval_list) node = __ldcg(&p.eval_list[node]);  // the others are copies
-                    recs[j] = T.nodes + T.ofs_l + (size_t)node * T.node_size;
-                    tidx[j] = recs[j][0];
-                    pending |= 1u << j;
+            for (int k = 0; k < K; k++) {
+                const uint32_t cell = grp * 32 * K + k * 32 + lane;
+                const uint32_t cz = cell % dim, cy = (cell / dim) % dim, cx = cell / (dim * dim);
+                px.v[k] = __fadd_rn(T.lx, __fmul_rn((float)(ncx * dim + cx), cs));
+                py.v[k] = __fadd_rn(T.ly, __fmul_rn((float)(ncy * dim + cy), cs));
+                pz.v[k] = __fadd_rn(T.lz, __fmul_rn((float)(ncz * dim + cz), cs));
+                pt.v[k] = T.tt;
+            }
+            sts_k<K>(lane_base + 0 * 32 * ROW, px);
+            sts_k<K>(lane_base + 1 * 32 * ROW, py);
+            sts_k<K>(lane_base + 2 * 32 * ROW, pz);
+            sts_k<K>(lane_base + 3 * 32 * ROW, pt);
+            const bool resident = n <= STAGE && staged_tape == tape_idx && staged_pool == T.tapes;
+            FK<K> r;
+#pragma unroll
+            for (int k = 0; k < K; k++) r.v[k] = 0.0f;
+            uint64_t pre[STAGE / 32];
+            if (!resident) prefetch_chunk(pre, tape, 0, n, lane);
+            for (uint32_t base = 0; base < n; base += STAGE) {
+                const uint32_t m = min(STAGE, n - base);
+                if (!resident) {
+                    __syncwarp();
+                    stage_chunk<true>(stage, pre, ROW, lane, m);
+                    prefetch_chunk(pre, tape, base + STAGE, n, lane);
+                    __syncwarp();
+                }
+                // The decode word of j+1 is read one instruction early.
+                const uint32_t sbase = smem_addr(stage);
+                uint4 dn = lds_u4(sbase);
+                for (uint32_t j = 0; j < m; j++) {
+                    const uint4 d = dn;
+                    dn = lds_u4(sbase + (j + 1) * 16);
+                    switch (d.x) {
+                        case OP_CONST:
+#pragma unroll
+                            for (int k = 0; k < K; k++) r.v[k] = __uint_as_float(d.y);
+                            break;
+#define FREP_PT_CASE(OPC, FA, FB)                         \
+    case OPC | (FA ? F_FWD_A : 0u) | (FB ? F_FWD_B : 0u): \
+        pt_exec<K, OPC, FA, FB>(d, r, lane_base);         \
+        break;
+                        FREP_ALL_CASES(FREP_PT_CASE)
+#undef FREP_PT_CASE
+                        default: break;
+                    }
+                    sts_k<K>(lane_base + d.w, r);
                 }
             }
-            if (NP > 1 && !(pending & 1u)) continue;
-            while (pending) {
-                const uint32_t tape_idx = tidx[__ffs(pending) - 1];
-                const uint64_t* tape = T.tapes + tape_idx + 1;
-                const uint32_t n = (uint32_t)__ldcg(&T.tapes[tape_idx]);
-                FK<K> px, py, pz, pt;
+            staged_tape = n <= STAGE ? tape_idx : 0xFFFFFFFFu;
+            staged_pool = T.tapes;
+            __syncwarp();
+            stat_work += 32ull * K * n;
+            const FK<K> d = lds_k<K>(lane_base);
 #pragma unroll
-                for (int k = 0; k < K; k++) {
-                    // node (k / words of the pair) and cell of value k
-                    const bool second = NP > 1 && np > 1 && (uint32_t)k >= words && (pending & 2u);
-                    const uint32_t* rk = second ? recs[NP - 1] : recs[0];
-                    const uint32_t cell = np > 1 ? ((uint32_t)k % words) * 32 + lane : grp * 32 * K + k * 32 + lane;
-                    const uint32_t cz = cell % dim, cy = (cell / dim) % dim, cx = cell / (dim * dim);
-                    px.v[k] = __fadd_rn(T.lx, __fmul_rn((float)(rk[1] * dim + cx), cs));
-                    py.v[k] = __fadd_rn(T.ly, __fmul_rn((float)(rk[2] * dim + cy), cs));
-                    pz.v[k] = __fadd_rn(T.lz, __fmul_rn((float)(rk[3] * dim + cz), cs));
-                    pt.v[k] = T.tt;
-                }
-                sts_k<K>(lane_base + 0 * 32 * ROW, px);
-                sts_k<K>(lane_base + 1 * 32 * ROW, py);
-                sts_k<K>(lane_base + 2 * 32 * ROW, pz);
-                sts_k<K>(lane_base + 3 * 32 * ROW, pt);
-                const bool resident = n <= STAGE && staged_tape == tape_idx && staged_pool == T.tapes;
-                FK<K> r;
-#pragma unroll
-                for (int k = 0; k < K; k++) r.v[k] = 0.0f;
-                uint64_t pre[STAGE / 32];
-                if (!resident) prefetch_chunk(pre, tape, 0, n, lane);
-                for (uint32_t base = 0; base < n; base += STAGE) {
-                    const uint32_t m = min(STAGE, n - base);
-                    if (!resident) {
-                        __syncwarp();
-                        stage_chunk<true>(stage, pre, ROW, lane, m);
-                        prefetch_chunk(pre, tape, base + STAGE, n, lane);
-                        __syncwarp();
-                    }
-                    // The decode word of j+1 is read one instruction early.
-                    const uint32_t sbase = smem_addr(stage);
-                    uint4 dn = lds_u4(sbase);
-                    for (uint32_t j = 0; j < m; j++) {
-                        const uint4 d = dn;
-                        dn = lds_u4(sbase + (j + 1) * 16);
-                        switch (d.x) {
-                            case OP_CONST:
-#pragma unroll
-                                for (int k = 0; k < K; k++) r.v[k] = __uint_as_float(d.y);
-                                break;
-#define FREP_PT_CASE(OPC, FA, FB)                         \
-        case OPC | (FA ? F_FWD_A : 0u) | (FB ? F_FWD_B : 0u): \
-            pt_exec<K, OPC, FA, FB>(d, r, lane_base);         \
-            break;
-                            FREP_ALL_CASES(FREP_PT_CASE)
-#undef FREP_PT_CASE
-                            default: break;
-                        }
-                        sts_k<K>(lane_base + d.w, r);
-                    }
-                }
-                staged_tape = n <= STAGE ? tape_idx : 0xFFFFFFFFu;
-                staged_pool = T.tapes;
-                __syncwarp();
-                // the item's nodes that use this tape take their words
-                uint32_t done = 0;
-#pragma unroll
-                for (uint32_t j = 0; j < NP; j++)
-                    if (((pending >> j) & 1u) && tidx[j] == tape_idx) done |= 1u << j;
-                pending &= ~done;
-                stat_work += 32ull * (K / np) * __popc(done) * n;
-                const FK<K> d = lds_k<K>(lane_base);
-#pragma unroll
-                for (int k = 0; k < K; k++) {
-                    const uint32_t j = (NP > 1 && np > 1 && (uint32_t)k >= words) ? NP - 1 : 0u;
-                    if (!((done >> j) & 1u)) continue;  // (uniform across the warp)
-                    const uint32_t w = np > 1 ? (uint32_t)k % words : grp * K + k;
-                    const uint32_t leaf_w = __ballot_sync(0xFFFFFFFFu, d.v[k] < 0.0f);
-                    if (lane == 0) {
-                        uint32_t* rj = j ? recs[NP - 1] : recs[0];
-                        rj[4 + w] = leaf_w;
-                        rj[4 + words + w] = 0u;  // the unused second mask word range
-                    }
+            for (int k = 0; k < K; k++) {
+                const uint32_t leaf_w = __ballot_sync(0xFFFFFFFFu, d.v[k] < 0.0f);
+                if (lane == 0) {
+                    rec[4 + grp * K + k] = leaf_w;
+                    rec[4 + words + grp * K + k] = 0u;  // the unused second mask word range
                 }
             }
         }
@@ -1184,10 +1144,7 @@ __device__ __forceinline__ unsigned long long level_items(TreeHeader* H, uint32_
     if (!point && write_ofs) H->node_ofs[L + 1] = H->node_ofs[L] + (unsigned long long)count * H->node_size[L];
     // with reuse, only the listed nodes are evaluated
     const uint32_t evaluated = reuse ? min(count, H->reuse_eval[L]) : count;
-    // k: cells per lane of the pass; nodes of fewer than k mask words (dim 4
-    // with k = 4) go k / words to an item
-    if (point && words < (uint32_t)k) return (evaluated + (k / words) - 1) / (k / words);
-    return (unsigned long long)evaluated * (words / (uint32_t)k);
+    return (unsigned long long)evaluated * (words / (uint32_t)k);  // k: cells per lane of the pass
 }
 
 __global__ void __launch_bounds__(1024)

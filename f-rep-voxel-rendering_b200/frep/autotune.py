@@ -207,7 +207,7 @@ class Autotuner:
             sample = members[:: max(1, len(members) // self.per_class)][: self.per_class]
             best = None
             for dims in BRANCHINGS[res]:
-                ks = [4, 2]  # dim-4 leaves: 4 = nodes in pairs
+                ks = [0] if dims[-1] < 8 else [4, 2]
                 for k in ks:
                     ms = self._time_batch(sample, lambda s, d=dims: d, lambda s, g, k=k: k)
                     self.log.append({"class": key, "dims": list(dims), "point_cells_per_lane": k, "ms": ms})

@@ -166,11 +166,9 @@ typedef struct frep_voxelize_opts {
     uint64_t node_words;      /* node pool capacity in u32 words (0 = automatic)     */
     uint64_t tape_words;      /* tape pool capacity in u64 words (0 = automatic)     */
     uint32_t point_cells_per_lane; /* last-level pass: cells per lane, 2, 4 or 8 (0 =
-                                    * automatic: 4 when dim^3/32 is a multiple of 4,
-                                    * and 8 for a tree voxelized alone when it is a
-                                    * multiple of 8); it must divide dim^3/32, except
-                                    * 4 with dim 4 (nodes evaluated in pairs);
-                                    * batches and the server take 2 or 4 only */
+                                    * automatic: 4 when dim^3/32 is a multiple of 4);
+                                    * it must divide dim^3/32; batches and the server
+                                    * take 2 or 4 only */
     uint32_t separate_tapes;  /* 0: cells of a 32-cell group whose shortened tapes
                                * are identical share one copy (~3x less tape pool);
                                * 1: one copy per cell, as the reference stores them */

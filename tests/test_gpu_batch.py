@@ -188,27 +188,3 @@ def test_set_trees_and_render_frames(ctx):
                                  exp.nodes)
         np.testing.assert_array_equal(cells, want[i][2])
     batch.close()
-
-
-def test_batch_with_leaf_pairs_equals_alone(ctx):
-    """Trees whose dim-4 last level runs 4 cells per lane (two nodes per warp
-    item) voxelize in a batch exactly as alone with the default 2."""
-    import torch
-    scs = [sc for sc in _scenes() if sc.grid_dims[-1] == 4]
-    assert len(scs) >= 3
-    want = [_alone(ctx, sc, 0.0) for sc in scs]
-    storages = [frep.VoxelStorage(sc.grid_dims, sc.low_vertex, sc.world_size, point_cells_per_lane=4)
-                .init(ctx, sc.shape) for sc in scs]
-    batch = frep.Batch(ctx, storages)
-    dev = torch.device("cuda", 0)
-    rgba = [torch.zeros((sc.height, sc.width, 4), dtype=torch.uint8, device=dev) for sc in scs]
-    sizes = [(sc.width, sc.height) for sc in scs]
-    for graph in (False, True):
-        batch.run([sc.camera for sc in scs], sizes, rgba, lights=frep.Lights(shadow_mask=1),
-                  tape_times=[0.0] * len(scs), graph=graph)
-        torch.cuda.synchronize()
-        for i, vs in enumerate(storages):
-            canon, prob = oracle.canonical_of_export(vs.export())
-            assert prob == [] and canon == want[i][0], f"scene {i} tree differs"
-            np.testing.assert_array_equal(rgba[i].cpu().numpy(), want[i][1])
-    batch.close()

@@ -32,15 +32,13 @@ def _total_work(vs):
     return sum(vs.work())
 
 
-@pytest.mark.parametrize("rounding,k", [(0, 0), (1, 0), (1, 4)])
-def test_frames_equal_full_voxelizations(ctx, rounding, k):
-    """k = 4: the dim-4 leaves of the evaluated nodes go two to a warp item
-    (listed nodes, not necessarily siblings)."""
+@pytest.mark.parametrize("rounding", [0, 1])
+def test_frames_equal_full_voxelizations(ctx, rounding):
     sc = scenes.animated_csg(60, 3, seed=11, grid_dims=[16, 8, 4], width=96, height=64)
     tape = frep.Tape(sc.shape)
     assert tape.uses_time
     anim = frep.AnimatedVoxelizer(ctx, lambda: frep.VoxelStorage(sc.grid_dims, sc.low_vertex, sc.world_size,
-                                                                 rounding=rounding, point_cells_per_lane=k), tape)
+                                                                 rounding=rounding), tape)
     full = _storage(sc, tape, ctx, rounding)
     for t in (0.1, 0.13, 0.6, 0.61):
         vs = anim.voxelize(t)
