@@ -209,3 +209,70 @@ def test_tree_occupancy_equals_scenebuilder_point_sampling(which, rounding):
         values = frep.Tape(sc.shape).eval_points(xyzt)
     np.testing.assert_array_equal(occ, (values < 0).reshape(occ.shape))
     assert occ.sum() > 1000
+
+
+def _safe_to_render(blob) -> bool:
+    """The conditions the renderer relies on, restated independently: every
+    interior cell's child index and every node's tape record (and each
+    instruction's slots) lie inside their pools."""
+    b = compact.parse(blob)
+    if b.node_count[0] != 1 or not (4 <= b.n_slots <= 1024):
+        return False
+    sizes, offs = b.node_size, b.node_offset
+    if offs[-1] + b.node_count[-1] * sizes[-1] != len(b.nodes):
+        return False
+    tw = len(b.tapes)
+    for l in range(b.levels):
+        w = b.dims[l] ** 3 // 32
+        last = l == b.levels - 1
+        recs = b.nodes[offs[l]: offs[l] + b.node_count[l] * sizes[l]].reshape(b.node_count[l], sizes[l])
+        for rec in recs:
+            t = int(rec[0])
+            if t >= tw:
+                return False
+            n = int(b.tapes[t] & 0xFFFFFFFF)
+            if t + 1 + n > tw:
+                return False
+            ins = b.tapes[t + 1: t + 1 + n]
+            op = ins & 0xFF
+            slots = np.stack([(ins >> 16) & 0xFFFF, (ins >> 32) & 0xFFFF, ins >> 48])
+            if (op > 12).any() or (slots[0] >= b.n_slots).any() or \
+                    ((op != 0) & ((slots[1] >= b.n_slots) | (slots[2] >= b.n_slots))).any():
+                return False
+            if last:
+                continue
+            inter = rec[1 + w:1 + 2 * w]
+            cells = compact._cells(inter)
+            if len(cells):
+                words, bits = cells // 32, cells % 32
+                below = np.bitwise_count(inter[words] & ((np.uint64(1) << bits.astype(np.uint64)) - 1).astype(np.uint32))
+                child = rec[1 + 3 * w].astype(np.int64) + rec[1 + 2 * w + words].astype(np.int64) + below
+                if (child >= b.node_count[l + 1]).any():
+                    return False
+    return True
+
+
+def test_check_never_accepts_an_unsafe_blob(three_level):
+    """Random word overwrites in the node and tape sections of a valid blob:
+    whatever frep_compact_check accepts must be safe to render."""
+    t = three_level
+    good = compact.pack(t.levels, t.dims, t.node_count, t.node_offset, t.node_size, t.nodes, t.tapes,
+                        t.low_vertex, t.world_size, t.n_slots)
+    assert _safe_to_render(good)
+    rng = np.random.default_rng(7)
+    words = good[120:].view(np.uint32)
+    accepted = 0
+    for _ in range(400):
+        bad = good.copy()
+        bw = bad[120:].view(np.uint32)
+        i = int(rng.integers(len(words)))
+        bw[i] = rng.choice([0, 1, 0xFFFFFFFF, int(words[i]) ^ (1 << int(rng.integers(32))),
+                            int(rng.integers(1 << 32))])
+        try:
+            compact.check(bad)
+        except FrepError as e:
+            assert e.status == ERR_INVALID_ARG
+            continue
+        accepted += 1
+        assert _safe_to_render(bad), i
+    assert accepted > 0  # some overwrites are harmless (leaf masks, instruction constants)
