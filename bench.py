@@ -64,6 +64,9 @@ def parse():
     ap.add_argument("--serve-seconds", type=float, default=10.0,
                     help="batch: seconds of the serving run after the batch measurements (0 = none)")
     ap.add_argument("--serve-rate", type=float, default=1000.0, help="batch: Poisson request rate, requests/s")
+    ap.add_argument("--serve-sweep", default="",
+                    help="batch: extra request rates (comma separated, requests/s), each served for "
+                         "--serve-seconds after the main serving phase; results under serving_sweep")
     ap.add_argument("--serve-budget-gb", type=int, default=120, help="batch: tree arena of the server, GB")
     ap.add_argument("--grid", default=None,
                     help="large / stress: tree branching per level (default 16,16,8 / 16,16,4,4)")
@@ -829,6 +832,16 @@ def run_ours_batch(args, world, rank, local):
     if args.serve_seconds > 0:
         torch.cuda.synchronize()
         line["serving"] = serve_phase(args, ctx, scs, chosen, pools, tuner.warps)
+        sweep = []
+        for rate in (float(v) for v in args.serve_sweep.split(",") if v.strip()):
+            a = argparse.Namespace(**vars(args))
+            a.serve_rate = rate
+            r = serve_phase(a, ctx, scs, chosen, pools, tuner.warps)
+            sweep.append({k: r[k] for k in ("rate_req_s", "p50_ms", "p99_ms", "max_ms", "scenes_per_s",
+                                            "voxelized", "rerendered", "evictions", "failed",
+                                            "max_submit_lag_ms")})
+        if sweep:
+            line["serving_sweep"] = sweep
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         order = cpu_sample_order(n)
