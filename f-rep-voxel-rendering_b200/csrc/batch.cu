@@ -114,6 +114,7 @@ frep_status acquire_area(frep_batch* b, size_t bytes, int* which) {
         A.pending = false;
     }
     if (bytes > A.bytes) {
+        const size_t prev = A.bytes;
         if (A.graph) {
             cudaGraphExecDestroy(A.graph);
             A.graph = nullptr;
@@ -126,7 +127,8 @@ frep_status acquire_area(frep_batch* b, size_t bytes, int* which) {
         A.h = nullptr;
         A.d = nullptr;
         A.bytes = 0;
-        const size_t cap = align_up(bytes + bytes / 4, 4096);
+        // (freeing waits for the device: grow at least twofold)
+        const size_t cap = align_up(std::max(bytes + bytes / 4, 2 * prev), 4096);
         if (b->ctx->used + cap > b->ctx->budget) return fail(FREP_ERR_OOM, "frep_batch: upload area exceeds the budget");
         FREP_CUDA(cudaMallocHost(&A.h, cap));
         FREP_CUDA(cudaMalloc(&A.d, cap));
@@ -153,7 +155,9 @@ frep_status ensure_prefix(frep_batch* b, uint32_t n) {
         cudaFree(b->d_prefix);
         b->d_prefix = nullptr;
     }
-    const uint32_t cap = std::max<uint32_t>(n, 64);
+    // Growing waits for the device: start at 512 trees (a serving step's
+    // default maximum) and double, so that a changing tree set rarely grows it.
+    const uint32_t cap = std::max<uint32_t>(n, std::max<uint32_t>(512, 2 * b->prefix_cap));
     FREP_CUDA(cudaMalloc(&b->d_prefix, sizeof(unsigned long long) * (cap + 2)));
     b->d_cursor = b->d_prefix + cap + 1;
     b->prefix_cap = cap;
@@ -162,6 +166,12 @@ frep_status ensure_prefix(frep_batch* b, uint32_t n) {
 
 frep_status ensure_keep(frep_batch* b, uint64_t words) {
     if (words <= b->keep_words) return FREP_OK;
+    // Growing waits for the device: take half again as much as before when
+    // that fits the budget, so that steps with ever longer tapes grow it
+    // rarely.
+    const uint64_t grown = b->keep_words + b->keep_words / 2;
+    const uint64_t freed = b->keep_words * 4;
+    if (grown > words && b->ctx->used - std::min(b->ctx->used, freed) + grown * 4 <= b->ctx->budget) words = grown;
     if (b->keep) {
         cudaDeviceSynchronize();
         cudaFree(b->keep);
