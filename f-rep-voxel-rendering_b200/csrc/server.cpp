@@ -218,11 +218,13 @@ bool admit(frep_server* sv, Scene& S, uint64_t step) {
 
 frep_status ensure_frames(frep_server* sv, uint64_t bytes) {
     if (bytes <= sv->frames_bytes) return FREP_OK;
+    const uint64_t prev = sv->frames_bytes;
     FREP_CUDA(cudaStreamSynchronize(sv->stream));
     cudaFree(sv->d_frames);
     sv->d_frames = nullptr;
     sv->frames_bytes = 0;
-    const uint64_t cap = align_up(bytes + bytes / 4, 1 << 20);
+    // (growing waits for the stream: at least double)
+    const uint64_t cap = align_up(std::max<uint64_t>(bytes + bytes / 4, 2 * prev), 1 << 20);
     FREP_CUDA(cudaMalloc(&sv->d_frames, cap));
     sv->frames_bytes = cap;
     return FREP_OK;
@@ -231,7 +233,7 @@ frep_status ensure_frames(frep_server* sv, uint64_t bytes) {
 frep_status ensure_ring(frep_server* sv, uint32_t n) {
     if (n <= sv->ring_cap) return FREP_OK;
     FREP_CUDA(cudaStreamSynchronize(sv->stream));
-    const uint32_t cap = std::max<uint32_t>(n, 256);
+    const uint32_t cap = std::max<uint32_t>(n, std::max<uint32_t>(sv->cfg.max_batch, 2 * sv->ring_cap));
     for (int i = 0; i < kRing; i++) {
         cudaFreeHost(sv->h_tab[i]);
         cudaFree(sv->d_tab[i]);
