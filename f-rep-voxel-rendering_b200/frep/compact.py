@@ -124,39 +124,34 @@ def _cells(words: np.ndarray) -> np.ndarray:
 def pack(levels, dims, node_count, node_offset, node_size, nodes, tapes, low_vertex, world_size,
          n_slots) -> np.ndarray:
     """A tree in the reference's node layout -> blob (FREP_COMPACT_LAYOUT):
-    the nodes reachable from the root, every level renumbered in preorder,
-    masks and tape indices unchanged (the tape pool is copied as is)."""
-    order = [np.array([0], np.int64)]
-    for l in range(levels - 1):
-        c3 = dims[l] ** 3
-        nxt = []
-        for src in order[l]:
-            rec = nodes[node_offset[l] + src * node_size[l]:]
-            inter = rec[4 + c3 // 32: 4 + c3 // 16]
-            nxt.append(rec[4 + c3 // 16 + _cells(inter)].astype(np.int64))
-        order.append(np.concatenate(nxt) if nxt else np.zeros(0, np.int64))
-    counts = [len(o) for o in order]
-    sizes = [record_words(d, l == levels - 1) for l, d in enumerate(dims)]
-    out = np.zeros(sum(c * s for c, s in zip(counts, sizes)), np.uint32)
-    at = 0
+    the nodes reachable from the root, every level renumbered in preorder
+    (children in (parent, cell) order), masks and tape indices unchanged (the
+    tape pool is copied as is)."""
+    nodes = np.asarray(nodes, np.uint32)
+    order = np.array([0], np.int64)          # source ids of this level, in preorder
+    counts, records = [], []
     for l in range(levels):
-        c3 = dims[l] ** 3
+        dim = dims[l]
+        c3 = dim ** 3
         w = c3 // 32
         last = l == levels - 1
-        base = 0
-        for src in order[l]:
-            rec = nodes[node_offset[l] + src * node_size[l]:]
-            d = out[at:at + sizes[l]]
-            d[0] = rec[0]
-            d[1:1 + w] = rec[4:4 + w]
-            if not last:
-                inter = rec[4 + w:4 + 2 * w]
-                pc = np.bitwise_count(inter).astype(np.int64)
-                d[1 + w:1 + 2 * w] = inter
-                d[1 + 2 * w:1 + 3 * w] = np.cumsum(pc) - pc
-                d[1 + 3 * w] = base
-                base += int(pc.sum())
-            at += sizes[l]
+        rec = nodes[node_offset[l] + order[:, None] * node_size[l] + np.arange(node_size[l])[None, :]]
+        d = np.zeros((len(order), record_words(dim, last)), np.uint32)
+        d[:, 0] = rec[:, 0]
+        d[:, 1:1 + w] = rec[:, 4:4 + w]
+        counts.append(len(order))
+        if not last:
+            inter = np.ascontiguousarray(rec[:, 4 + w:4 + 2 * w])
+            pc = np.bitwise_count(inter).astype(np.int64)
+            d[:, 1 + w:1 + 2 * w] = inter
+            d[:, 1 + 2 * w:1 + 3 * w] = np.cumsum(pc, axis=1) - pc
+            per = pc.sum(axis=1)
+            d[:, 1 + 3 * w] = np.cumsum(per) - per
+            bits = np.unpackbits(inter.astype("<u4").view(np.uint8), axis=1, bitorder="little")[:, :c3]
+            parent, cell = np.nonzero(bits)
+            order = rec[parent, 4 + c3 // 16 + cell].astype(np.int64)
+        records.append(d.reshape(-1))
+    out = np.concatenate(records) if records else np.zeros(0, np.uint32)
     return build(Blob(levels, list(dims), tuple(low_vertex), float(world_size), COMPACT_LAYOUT, int(n_slots),
                       counts, out, np.ascontiguousarray(tapes, np.uint64)))
 
@@ -180,7 +175,9 @@ class ReferenceLayout:
 
 def expand(blob) -> ReferenceLayout:
     """A blob -> the reference's layout, with node coordinates (in units of
-    the level's node size) and full child lists (0xFFFFFFFF = no child)."""
+    the level's node size) and full child lists (0xFFFFFFFF = no child).
+    Vectorized per level: children are numbered in (parent, cell) order, which
+    is the blob's preorder."""
     b = blob if isinstance(blob, Blob) else parse(blob)
     sizes = [reference_words(d, l == b.levels - 1) for l, d in enumerate(b.dims)]
     offs, at = [], 0
@@ -189,31 +186,35 @@ def expand(blob) -> ReferenceLayout:
         at += n * s
     out = np.zeros(at, np.uint32)
     csz, cofs = b.node_size, b.node_offset
-    coords = [np.zeros((1, 3), np.int64)]
+    coords = np.zeros((1, 3), np.int64)
     for l in range(b.levels):
-        dim = b.dims[l]
+        dim, n = b.dims[l], b.node_count[l]
         c3 = dim ** 3
         w = c3 // 32
         last = l == b.levels - 1
-        nxt = np.zeros((b.node_count[l + 1] if not last else 0, 3), np.int64)
-        for r in range(b.node_count[l]):
-            d = b.nodes[cofs[l] + r * csz[l]: cofs[l] + (r + 1) * csz[l]]
-            o = out[offs[l] + r * sizes[l]: offs[l] + (r + 1) * sizes[l]]
-            o[0] = d[0]
-            o[1:4] = coords[l][r]
-            o[4:4 + w] = d[1:1 + w]
-            if last:
-                continue
-            inter = d[1 + w:1 + 2 * w]
-            o[4 + w:4 + 2 * w] = inter
-            lst = o[4 + 2 * w:4 + 2 * w + c3]
-            lst[:] = 0xFFFFFFFF
-            cells = _cells(inter)
-            ids = int(d[1 + 3 * w]) + np.arange(len(cells))
-            lst[cells] = ids
-            cxyz = np.stack([cells // (dim * dim), (cells // dim) % dim, cells % dim], 1)
-            nxt[ids] = coords[l][r] * dim + cxyz
-        coords.append(nxt)
+        src = b.nodes[cofs[l]: cofs[l] + n * csz[l]].reshape(n, csz[l])
+        dst = out[offs[l]: offs[l] + n * sizes[l]].reshape(n, sizes[l])
+        dst[:, 0] = src[:, 0]
+        dst[:, 1:4] = coords
+        dst[:, 4:4 + w] = src[:, 1:1 + w]
+        if last:
+            break
+        inter = np.ascontiguousarray(src[:, 1 + w:1 + 2 * w])
+        dst[:, 4 + w:4 + 2 * w] = inter
+        bits = np.unpackbits(inter.astype("<u4").view(np.uint8), axis=1, bitorder="little")[:, :c3]
+        parent, cell = np.nonzero(bits)                    # row-major: (parent, cell) order
+        ids = np.arange(len(cell), dtype=np.int64)
+        # each node's base must be the number of children of the nodes before it
+        per = bits.sum(axis=1, dtype=np.int64)
+        starts = np.cumsum(per) - per
+        has = per > 0
+        if len(ids) != b.node_count[l + 1] or not np.array_equal(src[has, 1 + 3 * w].astype(np.int64), starts[has]):
+            raise ValueError(f"level {l}: children are not numbered in preorder")
+        lst = dst[:, 4 + 2 * w:4 + 2 * w + c3]
+        lst[:] = 0xFFFFFFFF
+        lst[parent, cell] = ids
+        cxyz = np.stack([cell // (dim * dim), (cell // dim) % dim, cell % dim], 1)
+        coords = coords[parent] * dim + cxyz
     return ReferenceLayout(b.levels, list(b.dims), list(b.node_count), offs, sizes, out, b.tapes, b.low_vertex,
                            b.world_size, b.n_slots, b.mode)
 
