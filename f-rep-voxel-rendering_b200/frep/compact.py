@@ -15,7 +15,8 @@ last-level node ``[tapeIdx, leaf[W]]``.
 * :func:`expand` — a blob back to the reference's layout (coordinates and full
   child lists restored);
 * :func:`check` — the library's own validation (``frep_compact_check``; host
-  only, no device needed).
+  only, no device needed); :func:`save` / :func:`load` — a blob to and from a
+  file (checked on load).
 """
 from __future__ import annotations
 
@@ -217,6 +218,20 @@ def expand(blob) -> ReferenceLayout:
         coords = coords[parent] * dim + cxyz
     return ReferenceLayout(b.levels, list(b.dims), list(b.node_count), offs, sizes, out, b.tapes, b.low_vertex,
                            b.world_size, b.n_slots, b.mode)
+
+
+def save(blob, path) -> None:
+    """Writes a blob to a file (the bytes as they are: the format is position
+    independent and little endian)."""
+    np.ascontiguousarray(np.frombuffer(bytes(blob), np.uint8) if not isinstance(blob, np.ndarray) else blob,
+                         np.uint8).tofile(str(path))
+
+
+def load(path) -> np.ndarray:
+    """Reads a blob from a file and checks it (frep_compact_check)."""
+    blob = np.fromfile(str(path), np.uint8)
+    check(blob)
+    return blob
 
 
 def check(blob) -> None:

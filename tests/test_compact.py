@@ -276,3 +276,14 @@ def test_check_never_accepts_an_unsafe_blob(three_level):
         accepted += 1
         assert _safe_to_render(bad), i
     assert accepted > 0  # some overwrites are harmless (leaf masks, instruction constants)
+
+
+def test_save_and_load(three_level, tmp_path):
+    t = three_level
+    blob = compact.pack(t.levels, t.dims, t.node_count, t.node_offset, t.node_size, t.nodes, t.tapes,
+                        t.low_vertex, t.world_size, t.n_slots)
+    compact.save(blob, tmp_path / "tree.frepct")
+    np.testing.assert_array_equal(compact.load(tmp_path / "tree.frepct"), blob)
+    (tmp_path / "bad.frepct").write_bytes(bytes(blob[:-8]))
+    with pytest.raises(FrepError):
+        compact.load(tmp_path / "bad.frepct")
