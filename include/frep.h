@@ -399,8 +399,10 @@ typedef struct frep_compact_info {
 /* Builds the compact form of a voxelized tree (which is left unchanged and
  * may then be destroyed or voxelized again). Blocking: waits for the tree's
  * voxelization, runs the compaction on `stream` and waits for it. Device
- * memory: the result (charged to the context's budget) plus temporary
- * scratch of about 16 bytes per source node and 1/4 byte per tape word.
+ * memory: the result (charged to the context's budget) plus, while the call
+ * runs, working buffers of the result's upper bound (when pruning, copied
+ * into an exact one at the end), 16 bytes per node of the largest level,
+ * 1 byte per node (pruning) and 1/2 byte per tape word.
  * FREP_ERR_CAPACITY: the tree's pools overflowed; FREP_ERR_INVALID_ARG: not
  * voxelized or a bad mode. */
 frep_status frep_tree_compact(frep_ctx* ctx, frep_tree* tree, uint32_t mode, void* stream, frep_compact** out);
