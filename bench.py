@@ -100,6 +100,9 @@ def parse():
 
 
 def dist_setup(args):
+    """One process per GPU (torchrun sets RANK / LOCAL_RANK / WORLD_SIZE):
+    NCCL on GPUs; gloo on a host without CUDA (the reference arm's ranks and
+    the CPU tests of this plumbing)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -107,9 +110,12 @@ def dist_setup(args):
         import datetime
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
     return world, rank, local
 
 
@@ -120,11 +126,14 @@ def barrier(world):
 
 
 def max_over_ranks(world, value: float) -> float:
+    """The largest of the ranks' values (timings are reported as the slowest
+    rank's)."""
     if world == 1:
         return value
     import torch
     import torch.distributed as dist
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
