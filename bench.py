@@ -498,15 +498,23 @@ def measure_compact(args, ctx, vs, scene, lights, t, rgba, flush, stream, render
 
 # ---- many-scene batch ----------------------------------------------------------------
 
-def make_batch_scenes(args, world: int = 1):
-    """The batch workload with one orbit camera per scene (seeded)."""
+def make_batch_scenes(args, world: int = 1, indices=None):
+    """The batch workload with one orbit camera per scene (seeded); with
+    `indices`, only those scenes (same shapes and cameras as in the full set)."""
     import numpy as np
     from frep import scenes
+    rng = np.random.default_rng(11)
+    cams = [scenes.orbit_camera(rng) for _ in range(args.scenes)]
+    if indices is not None:
+        jobs = scenes.batch_jobs(args.scenes, seed=3, width=args.width, height=args.height)
+        scs = [scenes.batch_scene(jobs[i]) for i in indices]
+        for sc, i in zip(scs, indices):
+            sc.camera = cams[i]
+        return scs
     procs = max(1, min(32, (os.cpu_count() or 1) // max(1, world)))
     scs = scenes.batch_workload(args.scenes, seed=3, width=args.width, height=args.height, processes=procs)
-    rng = np.random.default_rng(11)
-    for sc in scs:
-        sc.camera = scenes.orbit_camera(rng)
+    for sc, cam in zip(scs, cams):
+        sc.camera = cam
     return scs
 
 
@@ -530,29 +538,50 @@ def cpu_sample_order(n: int):
     return [int(i) for i in np.random.default_rng(17).permutation(n)]
 
 
+# The CPU figures of the batch workload (the reference arm and the GPU arm's
+# cpu_baseline leg) time the same scenes: the first CPU_SAMPLE of a seeded
+# permutation of the batch, each at the grid the GPU arm runs it with.
+CPU_SAMPLE = 20
+
+
+def tuned_grid(table: dict, sc):
+    """(grid dims, point cells per lane) of a batch scene under a tuning table
+    (frep.autotune.load_table); the default branching where it has no entry."""
+    from frep import scenes as S
+    from frep.autotune import Autotuner
+    c = table.get(Autotuner.key(sc.meta["res"], sc.shape.n_instr))
+    if c is None:
+        return tuple(S.DEFAULT_BRANCHING[sc.meta["res"]]), 0
+    return tuple(c.dims), c.point_cells_per_lane
+
+
 def run_reference_batch(args, world, rank):
-    """--impl reference on the batch workload: each step is the next scene of
-    a seeded permutation of the batch, voxelized + rendered by the oracle on
-    all host threads; value = scenes / total seconds."""
+    """--impl reference on the batch workload: step i is scene i of the CPU
+    sample (the GPU arm's cpu_baseline scenes, at the grids the GPU arm's
+    tuning table gives them), voxelized + rendered by the oracle on all host
+    threads; warm-up steps run the first scenes of the sample once more.
+    value = scenes / total seconds."""
     if rank != 0:
         return
-    from frep import scenes as S
-    scs = make_batch_scenes(args)
+    from frep.autotune import load_table
+    table = load_table(args.tune_cache)
+    order = cpu_sample_order(args.scenes)
+    idx = [order[i % CPU_SAMPLE] for i in range(max(args.steps, args.warmup))]
+    built = {i: sc for i, sc in zip(sorted(set(idx)), make_batch_scenes(args, indices=sorted(set(idx))))}
     threads = os.cpu_count() or 1
-    order = cpu_sample_order(len(scs))
-    pick = lambda i: scs[order[i % len(order)]]
     for i in range(args.warmup):
-        sc = pick(i)
-        oracle_scene_seconds(sc, S.DEFAULT_BRANCHING[sc.meta["res"]], threads)
+        sc = built[idx[i]]
+        oracle_scene_seconds(sc, tuned_grid(table, sc)[0], threads)
     times = []
     for i in range(args.steps):
-        sc = pick(args.warmup + i)
-        times.append(oracle_scene_seconds(sc, S.DEFAULT_BRANCHING[sc.meta["res"]], threads))
+        sc = built[idx[i]]
+        times.append(oracle_scene_seconds(sc, tuned_grid(table, sc)[0], threads))
     total = sum(times)
     value = args.steps / total
-    sample = (f"{args.steps} scenes of the batch (seeded permutation, after {args.warmup} warm-up scenes), "
-              f"each voxelized at its default branching + rendered {args.width}x{args.height}; "
-              f"oracle C++ port, {threads} threads")
+    sample = (f"{args.steps} scenes of the batch (the first {min(args.steps, CPU_SAMPLE)} of a seeded permutation, "
+              f"the GPU arm's cpu_baseline sample), each voxelized at the grid the GPU arm's tuning table "
+              f"({'committed' if args.tune_cache else 'none: default'} branchings) gives it + rendered "
+              f"{args.width}x{args.height}; oracle C++ port, {threads} threads")
     line = {
         "metric": METRIC, "value": value, "unit": "scenes/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
@@ -649,6 +678,60 @@ def serve_phase(args, ctx, scs, chosen, pools, warps):
         "steps": st["steps"] - before["steps"], "max_submit_lag_ms": float(1e3 * lag.max()),
         "latency": "scheduled arrival -> image in pinned host memory (p50/p99_ms); server_*: submit -> image",
     }
+
+
+def batch_cpu_baseline(args, scs, chosen) -> dict:
+    """The oracle on the CPU sample (CPU_SAMPLE scenes, at the grids the GPU
+    arm ran them with) on all host threads; beside it the same path on one
+    thread for the sample's first scene, and the reference's own csg::Tape::Eval
+    point-sampling every finest voxel (SceneBuilder::BuildNode semantics,
+    scene_builder.cpp:91-156) of the 16-sphere scene."""
+    threads = os.cpu_count() or 1
+    order = cpu_sample_order(len(scs))[:CPU_SAMPLE]
+    spent = sum(oracle_scene_seconds(scs[i], chosen[i][0], threads) for i in order)
+    one = oracle_scene_seconds(scs[order[0]], chosen[order[0]][0], 1)
+    all_first = oracle_scene_seconds(scs[order[0]], chosen[order[0]][0], threads)
+    out = {"value": len(order) / spent, "unit": "scenes/s", "cores": threads, "kind": "port",
+           "sample": f"{len(order)} scenes of the batch (the first of a seeded permutation; the reference "
+                     f"arm's steps), each at the grid this run used, voxelize + {args.width}x{args.height} "
+                     f"render, oracle C++ port, {threads} threads",
+           "single_core": {"value": 1.0 / one, "unit": "scenes/s", "cores": 1,
+                           "sample": f"scene {order[0]} of the batch ({scs[order[0]].shape.n_instr} "
+                                     f"instructions) on one thread; {1.0 / all_first:.3f} scenes/s on "
+                                     f"{threads} threads"}}
+    ref = reference_point_sampling()
+    if ref:
+        out["reference_tape_eval"] = ref
+    return out
+
+
+def reference_point_sampling():
+    """The reference's own csg::Tape::Eval (compiled from the reference's
+    sources into oracle/_ref) on every finest voxel of the 16-sphere scene
+    (64^3 = 262,144 points, one thread): SceneBuilder's point-only
+    voxelization (scene_builder.cpp:91-156). None when oracle/_ref is absent."""
+    sys.path.insert(0, str(REPO / "oracle"))
+    import numpy as np
+    import oracle
+    if not oracle.ref_available():
+        return None
+    from frep import scenes
+    sc = scenes.spheres_union(16, seed=1)
+    ops, in0, in1, consts, root = sc.shape.flatten()
+    rt = oracle.RefTape(ops, in0, in1, consts, root)
+    fine = 64
+    g = (np.arange(fine, dtype=np.float32) + np.float32(0.0))
+    cs = np.float32(sc.world_size) / np.float32(fine)
+    ax = np.float32(sc.low_vertex[0]) + g * cs
+    X, Y, Z = np.meshgrid(ax, ax, ax, indexing="ij")
+    pts = np.stack([X.ravel(), Y.ravel(), Z.ravel(), np.zeros(fine ** 3, np.float32)], 1)
+    rt.eval(pts[:1024])
+    t0 = time.perf_counter()
+    v = rt.eval(pts)
+    dt = time.perf_counter() - t0
+    return {"value": len(pts) / dt, "unit": "point evals/s", "cores": 1, "kind": "reference",
+            "sample": f"csg::Tape::Eval of the 16-sphere scene ({rt.n_instr} instructions) at all {fine}^3 "
+                      f"finest voxels ({int((v < 0).sum())} inside), {dt:.3f} s"}
 
 
 def run_ours_batch(args, world, rank, local):
@@ -852,16 +935,7 @@ def run_ours_batch(args, world, rank, local):
         if sweep:
             line["serving_sweep"] = sweep
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        threads = os.cpu_count() or 1
-        order = cpu_sample_order(n)
-        spent, done = 0.0, 0
-        while done < min(n, 64) and spent < 15.0:
-            sc = scs[order[done]]
-            spent += oracle_scene_seconds(sc, chosen[order[done]][0], threads)
-            done += 1
-        line["cpu_baseline"] = {"value": done / spent, "unit": "scenes/s", "cores": threads, "kind": "port",
-                                "sample": f"{done} scenes of the batch (seeded permutation, until 15 s), "
-                                          f"voxelize + {W}x{H} render each, oracle C++ port, {threads} threads"}
+        line["cpu_baseline"] = batch_cpu_baseline(args, scs, chosen)
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -152,6 +152,25 @@ class Context:
         L.check(L.lib().frep_ctx_memory(self._h, C.byref(used), C.byref(budget)))
         return used.value, budget.value
 
+    def eval_points(self, tape: "Tape", xyzt) -> np.ndarray:
+        """Tape values at n points (x, y, z, t) on the device, with the point
+        pass's operations (frep_tape_eval_device)."""
+        xyzt = np.ascontiguousarray(xyzt, np.float32).reshape(-1, 4)
+        out = np.zeros(len(xyzt), np.float32)
+        L.check(L.lib().frep_tape_eval_device(self._h, tape.handle, _ptr(xyzt), len(xyzt), _ptr(out)))
+        return out
+
+    def eval_intervals(self, tape: "Tape", boxes, tape_time: float = 0.0,
+                       rounding: int = ROUND_OUTWARD) -> np.ndarray:
+        """Interval bounds of the tape over n boxes (low xyz, high xyz) on the
+        device, with the level passes' operations (frep_tape_eval_intervals).
+        Returns an (n, 2) array of (low, high)."""
+        boxes = np.ascontiguousarray(boxes, np.float32).reshape(-1, 6)
+        out = np.zeros((len(boxes), 2), np.float32)
+        L.check(L.lib().frep_tape_eval_intervals(self._h, tape.handle, _ptr(boxes), len(boxes),
+                                                 float(tape_time), int(rounding), _ptr(out)))
+        return out
+
     def close(self):
         if self._h is not None and self._h.value and L is not None and L._lib is not None:
             L.lib().frep_ctx_destroy(self._h)
@@ -472,8 +491,8 @@ class CompactTree:
 
     @classmethod
     def from_blob(cls, ctx: Context, blob) -> "CompactTree":
-        arr = np.ascontiguousarray(np.frombuffer(bytes(blob), np.uint8) if not isinstance(blob, np.ndarray) else blob,
-                                   np.uint8)
+        from .compact import as_bytes
+        arr = as_bytes(blob)
         h = C.c_void_p()
         L.check(L.lib().frep_compact_import(ctx._h, _ptr(arr), arr.nbytes, C.byref(h)))
         return cls(ctx, h)

@@ -106,6 +106,11 @@ class CompactInfo(C.Structure):
                 ("node_words", C.c_uint64), ("tape_words", C.c_uint64), ("device_bytes", C.c_uint64)]
 
 
+class AutotuneOpts(C.Structure):
+    _fields_ = [("per_class", C.c_uint32), ("reps", C.c_uint32), ("width", C.c_uint32), ("height", C.c_uint32),
+                ("margin", C.c_float), ("force", C.c_uint32), ("refine", C.c_uint32)]
+
+
 class Image(C.Structure):
     _fields_ = [("rgba8", C.c_void_p), ("hits", C.c_void_p)]
 
@@ -124,6 +129,8 @@ _SIGS = {
     "frep_tape_get_instrs": (C.c_int, [_P, _P, C.c_uint32]),
     "frep_tape_get_reference": (C.c_int, [_P, _P, _P]),
     "frep_tape_eval": (C.c_int, [_P, _P, C.c_uint32, _P]),
+    "frep_tape_eval_device": (C.c_int, [_P, _P, _P, C.c_uint32, _P]),
+    "frep_tape_eval_intervals": (C.c_int, [_P, _P, _P, C.c_uint32, C.c_float, C.c_uint32, _P]),
     "frep_tape_destroy": (None, [_P]),
     "frep_ctx_create": (C.c_int, [C.c_int, C.c_uint64, C.POINTER(_P)]),
     "frep_ctx_destroy": (None, [_P]),
@@ -175,6 +182,16 @@ _SIGS = {
     "frep_compact_export": (C.c_int, [_P, _P, C.c_uint64, C.POINTER(C.c_uint64)]),
     "frep_compact_check": (C.c_int, [_P, C.c_uint64]),
     "frep_compact_import": (C.c_int, [_P, _P, C.c_uint64, C.POINTER(_P)]),
+    "frep_fit_pools": (C.c_int, [_P, _P, _P, _P, C.c_uint32, C.c_float, _P, _P]),
+    "frep_tuning_create": (C.c_int, [C.POINTER(_P)]),
+    "frep_tuning_destroy": (None, [_P]),
+    "frep_tuning_load": (C.c_int, [_P, C.c_char_p, C.c_char_p]),
+    "frep_tuning_save": (C.c_int, [_P, C.c_char_p, C.c_char_p]),
+    "frep_tuning_lookup": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32), _P,
+                                     C.POINTER(C.c_uint32)]),
+    "frep_tuning_warps": (C.c_int, [_P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
+    "frep_batch_autotune": (C.c_int, [_P, _P, _P, _P, C.c_uint32, C.POINTER(LightsStruct), _P, C.c_float,
+                                      C.POINTER(AutotuneOpts), _P]),
 }
 
 

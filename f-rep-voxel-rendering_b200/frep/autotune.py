@@ -1,4 +1,5 @@
-"""Pool sizing and the batch autotuner.
+"""Pool sizing and the batch autotuner: a thin wrapper of the C-ABI's
+frep_fit_pools and frep_batch_autotune (csrc/autotune.cpp, host C++).
 
 The reference fixes one scene's branching by hand (``gridDims`` in
 vulkan/src/main.cpp:16) and sizes its buffers for the worst case
@@ -10,23 +11,24 @@ both chosen per scene:
   no more;
 * ``Autotuner`` picks, per (effective resolution, tape-size class), the grid
   branching and the cells per lane of the last-level pass by timing batched
-  voxelize + render of a few scenes of that class on the device, and picks the
+  voxelize + render of a few scenes of that class on the device (the median of
+  several runs; a candidate must beat the incumbent by a margin), and picks the
   tapes (warps) per block of the level passes for the whole batch. Choices are
-  cached in a JSON file keyed by device name, so a later run reuses them.
+  kept in a JSON file keyed by device name, so a later run reuses them.
 """
 from __future__ import annotations
 
+import ctypes as C
 import json
 import math
 import os
-import time
 from dataclasses import dataclass, field
 
-from . import Batch, Context, Lights, ROUND_OUTWARD, Tape, VoxelStorage, Voxelizer
+from . import Context, Lights
 from . import _lib as L
 
-# Candidate branchings per effective resolution: every level a multiple of 4
-# from 4 to 32, two to four levels.
+# Candidate branchings per effective resolution (csrc/autotune.cpp holds the
+# table the tuner times; this copy documents it for Python callers).
 BRANCHINGS = {
     64: [(16, 4), (8, 8), (4, 16), (4, 4, 4)],
     128: [(16, 8), (8, 16), (32, 4), (8, 4, 4)],
@@ -36,6 +38,10 @@ BRANCHINGS = {
 }
 
 SIZE_CLASSES = (256, 1024, 4096)  # tape-length class bounds (instructions)
+
+# The tuning the benchmark uses by default: frep_batch_autotune's choices on a
+# B200 for the 512-scene batch workload (regenerate with bench.py --retune).
+DEFAULT_TABLE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning_b200.json")
 
 
 def size_class(n_instr: int) -> int:
@@ -61,38 +67,27 @@ class Pool:
 
 def fit_pools(ctx: Context, tapes, grids, low_vertex, world_size, tape_times=None, margin: float = 0.02,
               start_bytes: int = 1 << 30) -> list[Pool]:
-    """Node and tape words each (tape, grid) needs: one voxelization into a
-    scratch tree per distinct grid (grown by doubling on overflow), plus
-    `margin` and 4096 words of slack. Voxelization is deterministic up to the
-    order of child ids, so a tree sized this way never overflows on the same
-    tape and time."""
-    scratch: dict[tuple, VoxelStorage] = {}
-    sizes: dict[tuple, int] = {}
-    out = []
-    for i, (tape, dims) in enumerate(zip(tapes, grids)):
-        key = tuple(int(d) for d in dims)
-        t = 0.0 if tape_times is None else float(tape_times[i])
-        while True:
-            vs = scratch.get(key)
-            if vs is None:
-                b = sizes.setdefault(key, start_bytes)
-                vs = VoxelStorage(key, low_vertex, world_size, rounding=ROUND_OUTWARD,
-                                  node_words=b // 4 // 4, tape_words=b * 3 // 4 // 8)
-                vs.init(ctx, tape)
-                scratch[key] = vs
-            vs.tape = tape
-            Voxelizer(ctx, vs).voxelize(t)
-            info = vs.sync(raise_on_overflow=False)
-            if not info.overflow:
-                break
-            vs.cleanup()
-            del scratch[key]
-            sizes[key] *= 2
-        out.append(Pool(int(info.node_words_used * (1 + margin)) + 4096,
-                        int(info.tape_words_used * (1 + margin)) + 4096))
-    for vs in scratch.values():
-        vs.cleanup()
-    return out
+    """Node and tape words each (tape, grid) needs (frep_fit_pools): one
+    voxelization into a scratch tree per distinct grid (grown by doubling on
+    overflow), plus `margin` and 4096 words of slack. Voxelization is
+    deterministic up to the order of child ids, so a tree sized this way
+    never overflows on the same tape and time."""
+    n = len(tapes)
+    if n == 0:
+        return []
+    handles = (C.c_void_p * n)(*[t.handle.value for t in tapes])
+    gr = (L.Grid * n)()
+    for i, dims in enumerate(grids):
+        gr[i].levels = len(dims)
+        for j, d in enumerate(dims):
+            gr[i].dims[j] = int(d)
+        gr[i].low_vertex[:] = [float(v) for v in low_vertex]
+        gr[i].world_size = float(world_size)
+    times = None if tape_times is None else (C.c_float * n)(*[float(t) for t in tape_times])
+    nw = (C.c_uint64 * n)()
+    tw = (C.c_uint64 * n)()
+    L.check(L.lib().frep_fit_pools(ctx._h, handles, gr, times, n, float(margin), nw, tw))
+    return [Pool(int(a), int(b)) for a, b in zip(nw, tw)]
 
 
 @dataclass
@@ -102,28 +97,43 @@ class Choice:
     ms_per_scene: float = float("nan")
 
 
-@dataclass
+def load_table(path, device: str | None = None) -> dict:
+    """The tuned choices of a cache file ("res:class" -> Choice) without
+    touching a device: the entry of `device`, else of "NVIDIA B200", else the
+    file's first entry. {} when the file is absent or unreadable."""
+    if not path or not os.path.exists(path):
+        return {}
+    try:
+        data = json.loads(open(path).read())
+        entry = data.get(device) or data.get("NVIDIA B200") or next(iter(data.values()), {})
+        return {k: Choice(tuple(v["dims"]), v["point_cells_per_lane"], v["ms_per_scene"])
+                for k, v in entry.get("choices", {}).items()}
+    except (ValueError, KeyError, TypeError, StopIteration, AttributeError):
+        return {}
+
+
 class Autotuner:
-    """Measured choice of branching and last-level tile per scene class."""
+    """Measured choice of branching and last-level tile per scene class
+    (frep_batch_autotune), with the tapes per block for the batch."""
 
-    ctx: Context
-    cache_path: str | None = None
-    per_class: int = 4        # scenes timed per class
-    reps: int = 3             # timed batched runs per candidate
-    choices: dict = field(default_factory=dict)   # "res:class" -> Choice
-    warps: tuple = (0, 0)     # interval / point warps per block for the batch
-    log: list = field(default_factory=list)
-
-    def __post_init__(self):
+    def __init__(self, ctx: Context, cache_path: str | None = None, per_class: int = 4, reps: int = 5,
+                 margin: float = 0.03):
+        self.ctx = ctx
+        self.cache_path = cache_path
+        self.per_class = per_class
+        self.reps = reps
+        self.margin = margin
+        self.log: list = []
+        self._h = C.c_void_p()
+        L.check(L.lib().frep_tuning_create(C.byref(self._h)))
         self.device = self._device_name()
-        if self.cache_path and os.path.exists(self.cache_path):
-            try:
-                data = json.loads(open(self.cache_path).read()).get(self.device, {})
-                for k, v in data.get("choices", {}).items():
-                    self.choices[k] = Choice(tuple(v["dims"]), v["point_cells_per_lane"], v["ms_per_scene"])
-                self.warps = tuple(data.get("warps", (0, 0)))
-            except (ValueError, KeyError, TypeError):
-                self.choices = {}
+        if cache_path and os.path.exists(cache_path):
+            L.check(L.lib().frep_tuning_load(self._h, cache_path.encode(), self.device.encode()))
+
+    def __del__(self):
+        if L is not None and L._lib is not None and getattr(self, "_h", None) and self._h.value:
+            L.lib().frep_tuning_destroy(self._h)
+            self._h = C.c_void_p()
 
     @staticmethod
     def _device_name() -> str:
@@ -133,99 +143,46 @@ class Autotuner:
         except Exception:
             return "unknown"
 
-    def save(self) -> None:
-        if not self.cache_path:
-            return
-        data = {}
-        if os.path.exists(self.cache_path):
-            try:
-                data = json.loads(open(self.cache_path).read())
-            except ValueError:
-                data = {}
-        data[self.device] = {
-            "choices": {k: {"dims": list(c.dims), "point_cells_per_lane": c.point_cells_per_lane,
-                            "ms_per_scene": c.ms_per_scene} for k, c in self.choices.items()},
-            "warps": list(self.warps),
-        }
-        os.makedirs(os.path.dirname(os.path.abspath(self.cache_path)), exist_ok=True)
-        with open(self.cache_path, "w") as f:
-            json.dump(data, f, indent=1)
+    def save(self, path: str | None = None) -> None:
+        path = path or self.cache_path
+        if path:
+            os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
+            L.check(L.lib().frep_tuning_save(self._h, path.encode(), self.device.encode()))
 
     @staticmethod
     def key(res: int, n_instr: int) -> str:
         return f"{int(res)}:{size_class(n_instr)}"
 
+    @property
+    def warps(self) -> tuple:
+        a, b = C.c_uint32(), C.c_uint32()
+        L.check(L.lib().frep_tuning_warps(self._h, C.byref(a), C.byref(b)))
+        return int(a.value), int(b.value)
+
     def choice_for(self, res: int, n_instr: int) -> Choice | None:
-        return self.choices.get(self.key(res, n_instr))
+        levels, k = C.c_uint32(), C.c_uint32()
+        dims = (C.c_uint32 * L.MAX_LEVELS)()
+        L.check(L.lib().frep_tuning_lookup(self._h, int(res), int(n_instr), C.byref(levels), dims, C.byref(k)))
+        if levels.value == 0:
+            return None
+        return Choice(tuple(int(d) for d in dims[: levels.value]), int(k.value))
 
-    # ---- measurement ----------------------------------------------------------------
-
-    def _time_batch(self, scenes, dims_of, k_of, warps=(0, 0)) -> float:
-        """Device ms per scene of batched voxelize + render (graph replay)."""
-        import torch
-        tapes = [s.shape for s in scenes]
-        grids = [dims_of(s) for s in scenes]
-        pools = fit_pools(self.ctx, tapes, grids, scenes[0].low_vertex, scenes[0].world_size)
-        storages = []
-        for s, g, p in zip(scenes, grids, pools):
-            vs = VoxelStorage(g, s.low_vertex, s.world_size, rounding=ROUND_OUTWARD, node_words=p.node_words,
-                              tape_words=p.tape_words, point_cells_per_lane=k_of(s, g))
-            storages.append(vs.init(self.ctx, s.shape))
-        batch = Batch(self.ctx, storages)
-        batch.set_tuning(*warps)
-        dev = torch.device("cuda", self.ctx.device)
-        rgba = [torch.empty((s.height, s.width, 4), dtype=torch.uint8, device=dev) for s in scenes]
-        cams = [s.camera for s in scenes]
-        sizes = [(s.width, s.height) for s in scenes]
-        lights = Lights(shadow_mask=scenes[0].shadow_mask)
-        stream = torch.cuda.current_stream()
-        batch.run(cams, sizes, rgba, lights=lights, graph=True, stream=stream)
-        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
-        ev[0].record(stream)
-        for _ in range(self.reps):
-            batch.run(cams, sizes, rgba, lights=lights, graph=True, stream=stream)
-        ev[1].record(stream)
-        torch.cuda.synchronize()
-        ms = ev[0].elapsed_time(ev[1]) / self.reps / len(scenes)
-        batch.close()
-        for vs in storages:
-            vs.cleanup()
-        return ms
-
-    def tune(self, scenes, force: bool = False) -> None:
-        """Fills `choices` for every (resolution, size class) present in
-        `scenes` (those already cached are kept unless `force`), then the
-        batch's warps per block on a mixed sample."""
+    def tune(self, scenes, force: bool = False, refine: bool = False) -> None:
+        """Tunes every (resolution, size class) present in `scenes` that the
+        cache lacks (all of them with force; cached ones re-timed against
+        their cached choice with refine), then saves the cache."""
+        import time
         t0 = time.perf_counter()
-        classes: dict[str, list] = {}
-        for s in scenes:
-            classes.setdefault(self.key(s.meta["res"], s.shape.n_instr), []).append(s)
-        for key, members in sorted(classes.items()):
-            if key in self.choices and not force:
-                continue
-            res = int(key.split(":")[0])
-            sample = members[:: max(1, len(members) // self.per_class)][: self.per_class]
-            best = None
-            for dims in BRANCHINGS[res]:
-                ks = [0] if dims[-1] < 8 else [4, 2]
-                for k in ks:
-                    ms = self._time_batch(sample, lambda s, d=dims: d, lambda s, g, k=k: k)
-                    self.log.append({"class": key, "dims": list(dims), "point_cells_per_lane": k, "ms": ms})
-                    if best is None or ms < best.ms_per_scene:
-                        best = Choice(tuple(dims), k, ms)
-            self.choices[key] = best
-        # batch-wide tapes per block, on up to 32 scenes spread over the classes
-        if force or self.warps == (0, 0):
-            mixed = scenes[:: max(1, len(scenes) // 32)][:32]
-            dims_of = lambda s: self.apply(s)[0]
-            k_of = lambda s, g: self.apply(s)[1]
-            best_w, best_ms = (0, 0), None
-            for w in [(0, 0), (1, 1), (4, 4), (1, 4), (4, 1)]:
-                ms = self._time_batch(mixed, dims_of, k_of, w)
-                self.log.append({"warps": list(w), "ms": ms})
-                if best_ms is None or ms < best_ms:
-                    best_w, best_ms = w, ms
-            self.warps = best_w
+        n = len(scenes)
+        tapes = (C.c_void_p * n)(*[s.shape.handle.value for s in scenes])
+        res = (C.c_uint32 * n)(*[int(s.meta["res"]) for s in scenes])
+        cams = (L.CameraStruct * n)(*[s.camera.struct(s.width, s.height) for s in scenes])
+        lights = Lights(shadow_mask=scenes[0].shadow_mask).struct()
+        low = (C.c_float * 3)(*[float(v) for v in scenes[0].low_vertex])
+        opts = L.AutotuneOpts(self.per_class, self.reps, scenes[0].width, scenes[0].height, float(self.margin),
+                              1 if force else 0, 1 if refine else 0)
+        L.check(L.lib().frep_batch_autotune(self.ctx._h, tapes, res, cams, n, C.byref(lights), low,
+                                            float(scenes[0].world_size), C.byref(opts), self._h))
         self.log.append({"tune_seconds": time.perf_counter() - t0})
         self.save()
 

@@ -220,11 +220,19 @@ def expand(blob) -> ReferenceLayout:
                            b.world_size, b.n_slots, b.mode)
 
 
+def as_bytes(blob) -> np.ndarray:
+    """The blob's bytes as a contiguous uint8 array: an ndarray of any dtype
+    (e.g. a blob held as u32 or u64 words) is reinterpreted, not converted
+    value by value; anything else goes through bytes()."""
+    if isinstance(blob, np.ndarray):
+        return np.ascontiguousarray(blob).view(np.uint8).ravel()
+    return np.frombuffer(bytes(blob), np.uint8)
+
+
 def save(blob, path) -> None:
     """Writes a blob to a file (the bytes as they are: the format is position
     independent and little endian)."""
-    np.ascontiguousarray(np.frombuffer(bytes(blob), np.uint8) if not isinstance(blob, np.ndarray) else blob,
-                         np.uint8).tofile(str(path))
+    as_bytes(blob).tofile(str(path))
 
 
 def load(path) -> np.ndarray:
@@ -236,6 +244,5 @@ def load(path) -> np.ndarray:
 
 def check(blob) -> None:
     """frep_compact_check on a host blob; raises FrepError with the first problem."""
-    arr = np.ascontiguousarray(np.frombuffer(bytes(blob), np.uint8) if not isinstance(blob, np.ndarray) else blob,
-                               np.uint8)
+    arr = as_bytes(blob)
     L.check(L.lib().frep_compact_check(arr.ctypes.data_as(C.c_void_p), arr.nbytes))

@@ -280,6 +280,30 @@ def _batch_scene(job):
     return sc
 
 
+def batch_jobs(n_scenes: int = 512, seed: int = 3, width: int = 512, height: int = 512, shadows: bool = True,
+               branching: dict | None = None, min_prims: int = 4, max_prims: int = 1024) -> list:
+    """The scene descriptions of batch_workload without building them: one
+    tuple (index, seed, primitive count, resolution, grid dims, width,
+    height, shadows) per scene; batch_scene(job) builds one."""
+    rng = np.random.default_rng(seed)
+    counts = np.exp(rng.uniform(np.log(min_prims), np.log(max_prims), n_scenes))
+    counts = np.clip(np.round(counts), min_prims, max_prims).astype(int)
+    res = rng.choice(np.array(BATCH_RESOLUTIONS), n_scenes)
+    br = dict(DEFAULT_BRANCHING)
+    br.update(branching or {})
+    return [(i, seed * 1_000_003 + i, int(counts[i]), int(res[i]), tuple(br[int(res[i])]), width, height, shadows)
+            for i in range(n_scenes)]
+
+
+def batch_scene(job):
+    """One scene of batch_workload from its batch_jobs entry, its shape a
+    compiled frep.Tape."""
+    from . import Tape
+    sc = _batch_scene(job)
+    sc.shape = Tape.from_dag(*sc.shape)
+    return sc
+
+
 def batch_workload(n_scenes: int = 512, seed: int = 3, width: int = 512, height: int = 512,
                    shadows: bool = True, branching: dict | None = None, min_prims: int = 4,
                    max_prims: int = 1024, processes: int = 0) -> list:
@@ -291,14 +315,7 @@ def batch_workload(n_scenes: int = 512, seed: int = 3, width: int = 512, height:
     builds the expressions in that many spawned worker processes (expression
     building is Python-bound: about 0.25 ms per primitive)."""
     from . import Tape
-    rng = np.random.default_rng(seed)
-    counts = np.exp(rng.uniform(np.log(min_prims), np.log(max_prims), n_scenes))
-    counts = np.clip(np.round(counts), min_prims, max_prims).astype(int)
-    res = rng.choice(np.array(BATCH_RESOLUTIONS), n_scenes)
-    br = dict(DEFAULT_BRANCHING)
-    br.update(branching or {})
-    jobs = [(i, seed * 1_000_003 + i, int(counts[i]), int(res[i]), tuple(br[int(res[i])]), width, height, shadows)
-            for i in range(n_scenes)]
+    jobs = batch_jobs(n_scenes, seed, width, height, shadows, branching, min_prims, max_prims)
     if processes > 1 and n_scenes > 1:
         import multiprocessing as mp
         with mp.get_context("spawn").Pool(processes) as pool:

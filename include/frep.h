@@ -126,11 +126,27 @@ frep_status frep_tape_eval(const frep_tape* tape, const float* xyzt, uint32_t n,
 
 void frep_tape_destroy(frep_tape* tape);
 
+typedef struct frep_ctx frep_ctx;
+
+/* csg::Tape::Eval (tape.cpp:274-302) on the device for many points at once:
+ * n points of (x, y, z, t) in host memory, n values back in host memory. The
+ * operations and rounding of the last-level point pass (point.comp:2-63), so
+ * a value here is the one that pass compares with 0. Synchronous; working
+ * memory comes from the context's budget for the duration of the call. */
+frep_status frep_tape_eval_device(frep_ctx* ctx, const frep_tape* tape, const float* xyzt, uint32_t n, float* out);
+
+/* The interval extension the level passes compute (tape_eval_interval,
+ * interval.comp:8-160) over n caller-given boxes: box i is 6 floats (low x,
+ * y, z, high x, y, z) in host memory, T = [tape_time, tape_time]; out[2i],
+ * out[2i+1] = the interval's low and high bound. rounding: FREP_ROUND_*
+ * (below). With FREP_ROUND_OUTWARD every interval contains the tape's exact
+ * value at every point of its box. Synchronous. */
+frep_status frep_tape_eval_intervals(frep_ctx* ctx, const frep_tape* tape, const float* boxes, uint32_t n,
+                                     float tape_time, uint32_t rounding, float* out);
+
 /* ---------------------------------------------------------------------------
  * Device context
  * ------------------------------------------------------------------------- */
-
-typedef struct frep_ctx frep_ctx;
 
 /* Opens `device` with an HBM budget in bytes (0 = 90% of free memory). Replaces
  * the Vulkan device/VMA set-up of EngineBase::Init (engine_base.cpp:45-160). */
@@ -220,11 +236,15 @@ frep_status frep_voxelize_reuse(frep_ctx* ctx, frep_tree* tree, const frep_tree*
  * instead of a cudaMalloc'd buffer, and the root tape is copied straight from
  * `tape` (pageable memory: the call returns once the driver has staged it).
  * No counterpart in the reference.
- *   - Limit: each warp of a block needs n + 2m 32-bit words (n instructions,
- *     m of them MIN/MAX, each rounded up to 32), and one block must fit the
- *     8 MiB: n + 2m <= 524288 with 4 warps per block (2097152 with one);
- *     longer tapes return FREP_ERR_UNSUPPORTED. Long tapes run on fewer
- *     blocks than frep_voxelize uses, so they take longer.
+ *   - Limit: each warp of a block needs k * (n + 2m) 32-bit words (n
+ *     instructions, m of them MIN/MAX, each term rounded up to 32; k = 1 or 2
+ *     cells per lane, as the plan for the tape's slot count picks), and one
+ *     block (1 or 4 warps) must fit the 8 MiB, 2^21 words. Every root tape
+ *     with n + 2m <= 262,000 is accepted whatever the plan; longer ones only
+ *     when the plan uses fewer cells per lane or warps per block, and
+ *     FREP_ERR_UNSUPPORTED otherwise (the tree is untouched and stays usable).
+ *     Long tapes run on fewer blocks than frep_voxelize uses, so they take
+ *     longer.
  *   - Its first call on a device looks up the array's device address; make that
  *     first call before any stream capture.
  *   - Every call on a device shares the one array: calls whose work overlaps
@@ -508,6 +528,64 @@ frep_status frep_batch_get_info(const frep_batch* batch, frep_batch_info* info);
  * shared memory allows. Takes effect at the next voxelization. */
 frep_status frep_batch_set_tuning(frep_batch* batch, uint32_t interval_warps_per_block,
                                   uint32_t point_warps_per_block);
+
+/* ---------------------------------------------------------------------------
+ * Pool sizing and the batch autotuner. The reference fixes one scene's
+ * branching by hand (gridDims, vulkan/src/main.cpp:16) and sizes its buffers
+ * for the worst case (voxel_storage.h:45-47, 512 MiB of tapes); a batch of
+ * hundreds of scenes needs both chosen per scene.
+ * ------------------------------------------------------------------------- */
+
+/* Node and tape words each (tape, grid) needs: one voxelization (outward
+ * rounding, shortening on) into a scratch tree per distinct grid, grown by
+ * doubling on overflow, then the words used times (1 + margin) plus 4096.
+ * tape_times may be NULL (all 0). Blocking. */
+frep_status frep_fit_pools(frep_ctx* ctx, const frep_tape* const* tapes, const frep_grid* grids,
+                           const float* tape_times, uint32_t n, float margin, uint64_t* node_words,
+                           uint64_t* tape_words);
+
+/* Tuned choices: per class of scenes (effective resolution per axis, tape
+ * size class: < 256, < 1024, < 4096 or more instructions) a grid branching and
+ * the last level's cells per lane, and for the whole batch the tapes per block
+ * of the level passes. */
+typedef struct frep_tuning frep_tuning;
+frep_status frep_tuning_create(frep_tuning** out);
+void frep_tuning_destroy(frep_tuning* tuning);
+/* JSON keyed by device name; load takes `device`'s entry, else "NVIDIA B200",
+ * else the file's first. save keeps the other devices' entries. */
+frep_status frep_tuning_load(frep_tuning* tuning, const char* path, const char* device);
+frep_status frep_tuning_save(const frep_tuning* tuning, const char* path, const char* device);
+/* The choice for a scene: *levels = 0 when its class has none. */
+frep_status frep_tuning_lookup(const frep_tuning* tuning, uint32_t resolution, uint32_t n_instr, uint32_t* levels,
+                               uint32_t dims[FREP_MAX_LEVELS], uint32_t* point_cells_per_lane);
+/* The tapes per block to pass to frep_batch_set_tuning (0 = automatic). */
+frep_status frep_tuning_warps(const frep_tuning* tuning, uint32_t* interval_warps_per_block,
+                              uint32_t* point_warps_per_block);
+
+typedef struct frep_autotune_opts {
+    uint32_t per_class;      /* scenes timed per class (0 = 4)                             */
+    uint32_t reps;           /* timed runs per candidate; the median counts (0 = 5)        */
+    uint32_t width, height;  /* frame size of the timed renders (0 = 512 x 512)            */
+    float margin;            /* a candidate replaces the incumbent only when faster by this
+                              * fraction (0 = 0.03)                                        */
+    uint32_t force;          /* 1: tune every class afresh, cached choices ignored         */
+    uint32_t refine;         /* 1: re-time cached classes too, the cached choice first      */
+} frep_autotune_opts;
+
+/* Fills `tuning` for every class present among the n scenes (tapes[i] at
+ * effective resolution resolutions[i], one of 64, 128, 256, 512, 1024,
+ * rendered with cameras[i] and `lights`, grid from low_vertex / world_size):
+ * each candidate branching and last-level tile is timed as batched voxelize +
+ * render of up to per_class scenes of the class under CUDA graph replay (the
+ * median of reps runs); then the tapes per block on up to 32 scenes spread
+ * over the batch. The incumbent of a class (its cached choice, else the
+ * first candidate) is kept unless a candidate beats it by `margin`, so a
+ * repeated tuning keeps its choices. Classes already in `tuning` are skipped
+ * unless force or refine. Blocking; allocates and frees its own trees. */
+frep_status frep_batch_autotune(frep_ctx* ctx, const frep_tape* const* tapes, const uint32_t* resolutions,
+                                const frep_camera* cameras, uint32_t n, const frep_lights* lights,
+                                const float low_vertex[3], float world_size, const frep_autotune_opts* opts,
+                                frep_tuning* tuning);
 
 /* Profiling of plain (non-graph) batch calls: with profiling on,
  * frep_batch_voxelize and frep_batch_render record events between their

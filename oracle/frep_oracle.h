@@ -16,10 +16,13 @@
 // Parity pin: the reference's own tests hold no golden vectors for this path,
 // and its GLSL cannot run here (no graphics stack), so the shader restatement
 // is "parity unpinned" against the reference's GPU output. What IS pinned:
-// the tape compiler against the reference's csg::Tape (byte-exact), the point
-// interpreter against csg::Tape::Eval (bit-exact for algebraic tapes), every
-// interval against FP64 dense sampling, and the directed-rounding helpers
-// against exact rational arithmetic.
+// the tape compiler against the reference's csg::Tape (byte-exact,
+// tests/test_compiler.py), the point interpreter against csg::Tape::Eval
+// (bit-exact for algebraic tapes), outward intervals of sampled cells of
+// whole trees against FP64 dense sampling with a rigorous error bound
+// (tests/test_containment.py; the device's in tests/test_gpu_containment.py),
+// and oracle_directed against exact rational arithmetic
+// (tests/test_math_ulp.py).
 //
 // Every float operation rounds on its own (built with -ffp-contract=off);
 // transcendentals come from include/frep/frep_math.h, the library's definition.

@@ -287,3 +287,16 @@ def test_save_and_load(three_level, tmp_path):
     (tmp_path / "bad.frepct").write_bytes(bytes(blob[:-8]))
     with pytest.raises(FrepError):
         compact.load(tmp_path / "bad.frepct")
+
+
+def test_save_and_check_reinterpret_word_arrays(three_level, tmp_path):
+    """A blob held as u32 or u64 words is the same bytes: save() and check()
+    reinterpret it instead of converting each word to a byte."""
+    t = three_level
+    blob = compact.pack(t.levels, t.dims, t.node_count, t.node_offset, t.node_size, t.nodes, t.tapes,
+                        t.low_vertex, t.world_size, t.n_slots)
+    assert blob.nbytes % 8 == 0
+    for words in (blob.view(np.uint32), blob.view(np.uint64)):
+        compact.check(words)
+        compact.save(words, tmp_path / "w.frepct")
+        np.testing.assert_array_equal(compact.load(tmp_path / "w.frepct"), blob)

@@ -53,14 +53,18 @@ def test_orbit_camera_looks_at_origin():
 
 
 def test_autotuner_cache_round_trip(tmp_path):
-    path = str(tmp_path / "tune.json")
-    t = Autotuner(ctx=None, cache_path=path)
-    t.choices["256:2"] = Choice((16, 4, 4), 2, 0.5)
-    t.warps = (1, 4)
-    t.save()
-    u = Autotuner(ctx=None, cache_path=path)
-    assert u.choices["256:2"].dims == (16, 4, 4)
-    assert u.choices["256:2"].point_cells_per_lane == 2
+    """The Python wrapper reads and writes the C++ tuner's cache file."""
+    import json
+    path = tmp_path / "tune.json"
+    path.write_text(json.dumps({"NVIDIA B200": {"choices": {"256:2": {"dims": [16, 4, 4], "point_cells_per_lane": 2,
+                                                                      "ms_per_scene": 0.5}},
+                                                "warps": [1, 4]}}))
+    t = Autotuner(ctx=None, cache_path=str(path))
+    copy = str(tmp_path / "copy.json")
+    t.save(copy)
+    u = Autotuner(ctx=None, cache_path=copy)
+    assert u.choice_for(256, 1500).dims == (16, 4, 4)
+    assert u.choice_for(256, 1500).point_cells_per_lane == 2
     assert u.warps == (1, 4)
 
     class S:
