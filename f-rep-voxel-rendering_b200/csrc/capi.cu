@@ -220,7 +220,10 @@ frep_status tree_create_impl(frep_ctx* ctx, const frep_grid* grid, const frep_vo
     t->grid = *grid;
     if (opts) t->opts = *opts;
     else { t->opts.rounding = FREP_ROUND_OUTWARD; t->opts.shorten = 1; }
-    if (t->opts.rounding > 1) { delete t; return fail(FREP_ERR_INVALID_ARG, "opts.rounding must be 0 or 1"); }
+    if (t->opts.rounding > FREP_ROUND_HYBRID) {
+        delete t;
+        return fail(FREP_ERR_INVALID_ARG, "opts.rounding must be FREP_ROUND_NEAREST, _OUTWARD or _HYBRID");
+    }
     {
         const uint32_t dl = grid->dims[grid->levels - 1];
         const uint32_t k = t->opts.point_cells_per_lane;

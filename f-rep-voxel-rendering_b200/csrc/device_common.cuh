@@ -210,6 +210,103 @@ __device__ __forceinline__ float2 iv_apply(uint32_t op, uint64_t w, float2 a, fl
     }
 }
 
+// ---- hybrid affine mode (FREP_ROUND_HYBRID) ----------------------------------
+// A slot carries its outward interval and an affine form over the cell's axes,
+// A = c + x ex + y ey + z ez + [-e, e] (ex, ey, ez in [-1, 1]). Each
+// instruction computes the outward interval of its operands' intervals (the
+// formulas above) and the affine form; the slot keeps the interval intersected
+// with the form's range. Centres and coefficients are rounded to nearest and
+// every rounding error is added to e, rounded up (af_err bounds the error of
+// a nearest-rounded result r by |r| 2^-23 + 2^-149). Sums of error terms run
+// left to right, so the oracle (oracle/frep_oracle.cpp) computes the same bits.
+struct Af {
+    float c, x, y, z, e;
+};
+__device__ __forceinline__ float af_err(float r) { return __fadd_ru(__fmul_ru(fabsf(r), 0x1p-23f), 0x1p-149f); }
+__device__ __forceinline__ float af_rad(const Af& a) {
+    return __fadd_ru(__fadd_ru(__fadd_ru(fabsf(a.x), fabsf(a.y)), fabsf(a.z)), a.e);
+}
+__device__ __forceinline__ Af af_hull(float2 v) {
+    const float c = __fmul_rn(__fadd_rn(v.x, v.y), 0.5f);
+    return Af{c, 0.0f, 0.0f, 0.0f, max_sel(__fsub_ru(v.y, c), __fsub_ru(c, v.x))};
+}
+// The interval intersected with the form's range (a NaN form leaves it as is).
+__device__ __forceinline__ float2 af_tighten(float2 v, const Af& a) {
+    const float r = af_rad(a);
+    return make_float2(max_sel(v.x, __fsub_rd(a.c, r)), min_sel(v.y, __fadd_ru(a.c, r)));
+}
+__device__ __forceinline__ Af af_addsub(const Af& a, const Af& b, bool sub) {
+    Af r;
+    r.c = sub ? __fsub_rn(a.c, b.c) : __fadd_rn(a.c, b.c);
+    r.x = sub ? __fsub_rn(a.x, b.x) : __fadd_rn(a.x, b.x);
+    r.y = sub ? __fsub_rn(a.y, b.y) : __fadd_rn(a.y, b.y);
+    r.z = sub ? __fsub_rn(a.z, b.z) : __fadd_rn(a.z, b.z);
+    r.e = __fadd_ru(__fadd_ru(a.e, b.e),
+                    __fadd_ru(__fadd_ru(af_err(r.c), af_err(r.x)), __fadd_ru(af_err(r.y), af_err(r.z))));
+    return r;
+}
+__device__ __forceinline__ Af af_mul(const Af& a, const Af& b, bool square) {
+    Af r;
+    const float ra = af_rad(a);
+    if (square) {  // (c + s)^2 = c^2 + 2 c s + s^2 with s^2 in [0, ra^2] = h +- h
+        const float h = __fmul_ru(__fmul_ru(ra, ra), 0.5f);
+        const float cc = __fmul_rn(a.c, a.c);
+        r.c = __fadd_rn(cc, h);
+        r.x = __fmul_rn(__fmul_rn(a.c, a.x), 2.0f);
+        r.y = __fmul_rn(__fmul_rn(a.c, a.y), 2.0f);
+        r.z = __fmul_rn(__fmul_rn(a.c, a.z), 2.0f);
+        const float lin = __fmul_ru(__fmul_ru(fabsf(a.c), 2.0f), a.e);
+        r.e = __fadd_ru(__fadd_ru(__fadd_ru(lin, h), __fadd_ru(af_err(cc), af_err(r.c))),
+                        __fadd_ru(__fadd_ru(af_err(r.x), af_err(r.y)), af_err(r.z)));
+        return r;
+    }
+    const float rb = af_rad(b);
+    r.c = __fmul_rn(a.c, b.c);
+    const float x1 = __fmul_rn(a.c, b.x), x2 = __fmul_rn(b.c, a.x);
+    const float y1 = __fmul_rn(a.c, b.y), y2 = __fmul_rn(b.c, a.y);
+    const float z1 = __fmul_rn(a.c, b.z), z2 = __fmul_rn(b.c, a.z);
+    r.x = __fadd_rn(x1, x2);
+    r.y = __fadd_rn(y1, y2);
+    r.z = __fadd_rn(z1, z2);
+    const float lin = __fadd_ru(__fmul_ru(fabsf(a.c), b.e), __fmul_ru(fabsf(b.c), a.e));
+    const float rnd = __fadd_ru(__fadd_ru(__fadd_ru(af_err(x1), af_err(x2)), __fadd_ru(af_err(y1), af_err(y2))),
+                                __fadd_ru(__fadd_ru(af_err(z1), af_err(z2)),
+                                          __fadd_ru(__fadd_ru(af_err(r.x), af_err(r.y)), af_err(r.z))));
+    r.e = __fadd_ru(__fadd_ru(lin, __fmul_ru(ra, rb)), __fadd_ru(af_err(r.c), rnd));
+    return r;
+}
+// The form of an input axis k (0, 1, 2) over [lo, hi].
+__device__ __forceinline__ Af af_axis(float lo, float hi, int k) {
+    const float c = __fmul_rn(__fadd_rn(lo, hi), 0.5f);
+    const float r = max_sel(__fsub_ru(hi, c), __fsub_ru(c, lo));
+    return Af{c, k == 0 ? r : 0.0f, k == 1 ? r : 0.0f, k == 2 ? r : 0.0f, 0.0f};
+}
+// One hybrid instruction: the outward interval of the operands' intervals and
+// the form (MIN/MAX: the chosen operand's form when the choice is decided).
+// Returns the tightened interval; *f receives the form.
+__device__ __forceinline__ float2 hy_apply(uint32_t op, uint64_t w, float2 a, float2 b, const Af& fa, const Af& fb,
+                                           bool square, uint32_t choice, Af* f) {
+    const float2 v = op == OP_CONST ? make_float2(w_const(w), w_const(w)) : iv_apply<1>(op, w, a, b);
+    switch (op) {
+        case OP_CONST: *f = Af{v.x, 0.0f, 0.0f, 0.0f, 0.0f}; break;
+        case OP_ADD: *f = af_addsub(fa, fb, false); break;
+        case OP_SUB: *f = af_addsub(fa, fb, true); break;
+        case OP_NEG: *f = Af{-fa.c, -fa.x, -fa.y, -fa.z, fa.e}; break;
+        case OP_MUL: *f = af_mul(fa, fb, square); break;
+        case OP_COPY: *f = fa; break;
+        case OP_MIN:
+        case OP_MAX: *f = choice == MM_FIRST ? fa : (choice == MM_SECOND ? fb : af_hull(v)); break;
+        default: *f = af_hull(v); break;  // DIV SQRT EXP SIN COS: the interval's hull
+    }
+    return af_tighten(v, *f);
+}
+// MIN/MAX choice from two intervals (interval.comp:140-155).
+__device__ __forceinline__ uint32_t mm_choice(uint32_t op, float2 a, float2 b) {
+    const bool first_low = a.y < b.x, second_low = b.y < a.x;
+    return op == OP_MIN ? (first_low ? MM_FIRST : (second_low ? MM_SECOND : MM_BOTH))
+                        : (first_low ? MM_SECOND : (second_low ? MM_FIRST : MM_BOTH));
+}
+
 // Point evaluation of one instruction (point.comp:41-81).
 __device__ __forceinline__ float pt_apply(uint32_t op, uint64_t w, float a, float b) {
     switch (op) {

@@ -61,6 +61,45 @@ __global__ void eval_intervals_kernel(const uint64_t* __restrict__ tape, uint32_
     out[i] = slots[i];
 }
 
+// The hybrid affine mode (FREP_ROUND_HYBRID): each slot row holds the
+// interval and the affine form, 8 floats (lo, hi, c, x | y, z, e, 0).
+__global__ void eval_hybrid_kernel(const uint64_t* __restrict__ tape, uint32_t n_instr,
+                                   const float* __restrict__ boxes, uint32_t n, float tape_time,
+                                   float4* __restrict__ slots, float2* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float* b6 = boxes + 6 * (size_t)i;
+    auto row = [&](uint32_t s) { return slots + 2 * ((size_t)s * n + i); };
+    for (int k = 0; k < 3; k++) {
+        const Af f = af_axis(b6[k], b6[3 + k], k);
+        row(k)[0] = make_float4(b6[k], b6[3 + k], f.c, f.x);
+        row(k)[1] = make_float4(f.y, f.z, f.e, 0.0f);
+    }
+    row(3)[0] = make_float4(tape_time, tape_time, tape_time, 0.0f);
+    row(3)[1] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    for (uint32_t j = 0; j < n_instr; j++) {
+        const uint64_t w = __ldg(&tape[j]);
+        const uint32_t op = w_op(w);
+        float2 v;
+        Af f;
+        if (op == OP_CONST) {
+            v = make_float2(w_const(w), w_const(w));
+            f = Af{v.x, 0.0f, 0.0f, 0.0f, 0.0f};
+        } else {
+            const uint32_t sb = is_binary(op) ? w_b(w) : 0u;
+            const float4 a0 = row(w_a(w))[0], a1 = row(w_a(w))[1];
+            const float4 b0 = row(sb)[0], b1 = row(sb)[1];
+            const float2 a = make_float2(a0.x, a0.y), b = make_float2(b0.x, b0.y);
+            const Af fa{a0.z, a0.w, a1.x, a1.y, a1.z}, fb{b0.z, b0.w, b1.x, b1.y, b1.z};
+            const uint32_t c = is_mm(op) ? mm_choice(op, a, b) : 0u;
+            v = hy_apply(op, w, a, b, fa, fb, op == OP_MUL && w_a(w) == w_b(w), c, &f);
+        }
+        row(w_out(w))[0] = make_float4(v.x, v.y, f.c, f.x);
+        row(w_out(w))[1] = make_float4(f.y, f.z, f.e, 0.0f);
+    }
+    out[i] = make_float2(row(0)[0].x, row(0)[0].y);
+}
+
 }  // namespace dev
 }  // namespace frep
 
@@ -141,20 +180,25 @@ extern "C" frep_status frep_tape_eval_intervals(frep_ctx* ctx, const frep_tape* 
                                                 float tape_time, uint32_t rounding, float* out) {
     if (!ctx || !tape || (n && (!boxes || !out)))
         return fail(FREP_ERR_INVALID_ARG, "frep_tape_eval_intervals: null argument");
-    if (rounding > FREP_ROUND_OUTWARD) return fail(FREP_ERR_INVALID_ARG, "frep_tape_eval_intervals: rounding %u", rounding);
+    if (rounding > FREP_ROUND_HYBRID) return fail(FREP_ERR_INVALID_ARG, "frep_tape_eval_intervals: rounding %u", rounding);
     if (n == 0) return FREP_OK;
     if (tape->ct.instrs.empty()) return fail(FREP_ERR_INVALID_ARG, "frep_tape_eval_intervals: empty tape");
     const uint32_t n_slots = std::max<uint32_t>(tape->ct.n_slots, 4);
     EvalBuffers buf;
     uint8_t *d_in, *d_slots, *d_out;
-    frep_status st = eval_common(ctx, tape, n, (uint64_t)n * 24, (uint64_t)n * n_slots * 8, (uint64_t)n * 8, &buf,
-                                 &d_in, &d_slots, &d_out, "frep_tape_eval_intervals");
+    const uint64_t row_bytes = rounding == FREP_ROUND_HYBRID ? 32 : 8;
+    frep_status st = eval_common(ctx, tape, n, (uint64_t)n * 24, (uint64_t)n * n_slots * row_bytes, (uint64_t)n * 8,
+                                 &buf, &d_in, &d_slots, &d_out, "frep_tape_eval_intervals");
     if (st != FREP_OK) return st;
     FREP_CUDA(cudaMemcpy(d_in, boxes, (size_t)n * 24, cudaMemcpyHostToDevice));
     const uint32_t threads = 128, blocks = (n + threads - 1) / threads;
     const auto* t = static_cast<const uint64_t*>(buf.p);
     const uint32_t ni = (uint32_t)tape->ct.instrs.size();
-    if (rounding == FREP_ROUND_OUTWARD)
+    if (rounding == FREP_ROUND_HYBRID)
+        frep::dev::eval_hybrid_kernel<<<blocks, threads>>>(t, ni, reinterpret_cast<const float*>(d_in), n, tape_time,
+                                                           reinterpret_cast<float4*>(d_slots),
+                                                           reinterpret_cast<float2*>(d_out));
+    else if (rounding == FREP_ROUND_OUTWARD)
         frep::dev::eval_intervals_kernel<1><<<blocks, threads>>>(t, ni, reinterpret_cast<const float*>(d_in), n,
                                                                   tape_time, reinterpret_cast<float2*>(d_slots),
                                                                   reinterpret_cast<float2*>(d_out));

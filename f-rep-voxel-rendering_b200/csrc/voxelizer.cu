@@ -119,6 +119,47 @@ __device__ __forceinline__ uint32_t find_tree(const unsigned long long* prefix, 
 
 __host__ __device__ inline int point_k_of(uint32_t dim) { return (dim * dim * dim / 32) % 4 == 0 ? 4 : 2; }
 
+// log2(dim) for a power-of-two node dim, else NOT_POW2: lets the per-item
+// and per-cell index arithmetic use shifts instead of integer division for
+// dims 4, 8, 16 and 32 (the usual ones).
+constexpr uint32_t NOT_POW2 = 0xFFu;
+__device__ __forceinline__ uint32_t dim_shift(uint32_t dim) {
+    return (dim & (dim - 1)) == 0 ? (uint32_t)(__ffs(dim) - 1) : NOT_POW2;
+}
+
+// Node and mask-word group of a work item: `local` counts the tree's items of
+// this pass, `groups` items per node (dim^3 / 32 / cells-per-lane, a power of
+// two exactly when dim is, with gsh its log2).
+__device__ __forceinline__ void split_item(unsigned long long local, uint32_t groups, uint32_t gsh, uint32_t* node,
+                                           uint32_t* grp) {
+    if (gsh != NOT_POW2) {
+        *grp = (uint32_t)local & (groups - 1);
+        *node = (uint32_t)(local >> gsh);
+    } else if (local < (1ull << 32)) {
+        const uint32_t l = (uint32_t)local;
+        *grp = l % groups;
+        *node = l / groups;
+    } else {
+        *grp = (uint32_t)(local % groups);
+        *node = (uint32_t)(local / groups);
+    }
+}
+
+// Cell coordinates inside a node from the bit index z + dim*y + dim^2*x
+// (utils.comp:6).
+__device__ __forceinline__ void cell_xyz(uint32_t cell, uint32_t dim, uint32_t sh, uint32_t* cx, uint32_t* cy,
+                                         uint32_t* cz) {
+    if (sh != NOT_POW2) {
+        *cz = cell & (dim - 1);
+        *cy = (cell >> sh) & (dim - 1);
+        *cx = cell >> (2 * sh);
+    } else {
+        *cz = cell % dim;
+        *cy = (cell / dim) % dim;
+        *cx = cell / (dim * dim);
+    }
+}
+
 // What a level pass needs of one tree, read from its header when a warp
 // moves on to that tree.
 struct LevelTree {
@@ -126,7 +167,7 @@ struct LevelTree {
     uint32_t* nodes;
     uint64_t* tapes;
     unsigned long long tape_cap, ofs_l, ofs_next, child_cap;
-    uint32_t dim, node_size, node_size_next, shorten, share;
+    uint32_t dim, dim_sh, node_size, node_size_next, shorten, share;
     float cs, lx, ly, lz, tt;
 };
 
@@ -137,6 +178,7 @@ __device__ __forceinline__ LevelTree load_tree(TreeHeader* H, uint32_t L, bool p
     t.tapes = H->tapes;
     t.tape_cap = H->tape_cap;
     t.dim = H->dims[L];
+    t.dim_sh = dim_shift(t.dim);
     t.node_size = H->node_size[L];
     t.ofs_l = H->node_ofs[L];
     t.shorten = H->shorten;
@@ -269,40 +311,51 @@ __device__ __forceinline__ IVK<KI> iv_exec(const uint4 d, uint32_t lane_base, ui
     return r;
 }
 
-// Backward liveness walk of one item's cells over a tape of at most 64 slots
-// (shorten.comp:148-186): lane l keeps, for each of its KI cells, the set of
-// live slots as a 64-bit mask. From the last instruction down, an instruction
-// is kept where its output slot is live; the output then dies and the inputs
-// its choice uses (both for arithmetic, the chosen ones for MIN/MAX, none for
-// CONST) become live. Writes the kept masks of the tape (one ballot per
-// instruction and cell group) to keep[], and counts kept instructions and the
-// grouping signature per cell.
-//
-// U, the union of every cell's live sets: an instruction whose output is not
-// in U is dead for all the warp's cells and changes nothing. A chunk is walked
-// in one of two ways, chosen from how many of the previous chunk's
-// instructions were live somewhere (the top chunk as if all were): below half,
-// each step jumps (one ballot)
-// straight to the next instruction whose output is in U, with U kept exact —
-// long tapes of which each cell keeps a few percent (the root level) skip
-// most instructions; otherwise every instruction is visited and U is left to
-// be recomputed (one reduction) when the jumps resume. Measured: the 2048^3
-// scene's level 0 2.45 -> 1.65 ms with the jumps; the stress scene's level 2
-// (short, mostly live tapes) 212 ms with jumps everywhere, 167 ms without.
-template <int KI>
-__device__ __forceinline__ void walk_regs(const uint64_t* tape, uint32_t n, int mm, const uint2* mmb,
-                                          uint32_t* keep, const uint32_t (&ok_w)[KI], uint32_t lane,
-                                          uint32_t (&kept)[KI], uint32_t (&sig)[KI]) {
-    uint64_t lv[KI];
-    uint32_t any_ok = 0;
+// 32 x 32 bit-matrix transpose across a warp: lane j holds row j (bit c =
+// entry (j, c)); lane c gets column c (bit j = entry (j, c)). Five butterfly
+// steps, each swapping the off-diagonal s-blocks with lane ^ s.
+__device__ __forceinline__ uint32_t transpose32(uint32_t x, uint32_t lane) {
+    const uint32_t masks[5] = {0x0000FFFFu, 0x00FF00FFu, 0x0F0F0F0Fu, 0x33333333u, 0x55555555u};
 #pragma unroll
-    for (int h = 0; h < KI; h++) {
-        lv[h] = (ok_w[h] >> lane) & 1u;  // slot 0 (the result) is live
-        any_ok |= ok_w[h];
+    for (int i = 0; i < 5; i++) {
+        const uint32_t sh = 16u >> i, m = masks[i];
+        const uint32_t t = __shfl_xor_sync(0xFFFFFFFFu, x, sh);
+        x = (lane & sh) ? ((x & ~m) | ((t & ~m) >> sh)) : ((x & m) | ((t & m) << sh));
     }
-    uint64_t U = any_ok ? 1ull : 0ull;  // union of the live sets (exact while u_ok)
-    bool u_ok = true, plain = true;  // (the top chunk: mostly live)
-    int mm_top = mm;  // MIN/MAX instructions before the current chunk's end
+    return x;
+}
+
+// Backward liveness walk of one item's cells over a tape of at most 32 * S
+// slots (shorten.comp:148-186). The live sets are kept transposed and spread
+// over the lanes: lane l holds, per cell group h (32 cells) and q < S, the
+// 32-bit mask of the group's cells for which slot 32 q + l is live. From the
+// last instruction down, an instruction's keep mask is the mask of its output
+// slot (one shuffle, the same in every lane); the output then dies and the
+// inputs its choice uses (both for arithmetic, the chosen ones for MIN/MAX,
+// none for CONST) become live for the cells that kept it: three predicated
+// lane updates, whatever the number of cells.
+//
+// Per 32-instruction chunk the keep masks go to keep[]; each cell's kept
+// count and grouping signature (kept positions and MIN/MAX rewrites) come
+// from the chunk's masks transposed to one word per cell.
+//
+// A chunk is walked in one of two ways, chosen from how many of the previous
+// chunk's instructions were live somewhere (the top chunk as if all were):
+// below half, each step jumps (one ballot) straight to the next instruction
+// whose output is live in some cell; otherwise every instruction is visited.
+// Long tapes of which each cell keeps a few percent (the root level) skip
+// most instructions.
+template <int KI, int S>
+__device__ __forceinline__ void walk_lanes(const uint64_t* tape, uint32_t n, int mm, const uint2* mmb,
+                                           uint32_t* keep, const uint32_t (&ok_w)[KI], uint32_t lane,
+                                           uint32_t (&kept)[KI], uint32_t (&sig)[KI]) {
+    uint32_t lv[S][KI];
+#pragma unroll
+    for (int q = 0; q < S; q++)
+#pragma unroll
+        for (int h = 0; h < KI; h++) lv[q][h] = (q == 0 && lane == 0) ? ok_w[h] : 0u;  // slot 0: the result
+    bool plain = true;  // (the top chunk: mostly live)
+    int mm_top = mm;    // MIN/MAX instructions before the current chunk's end
     for (int hi = (int)n; hi > 0; hi -= 32) {
         const int lo = max(0, hi - 32);
         const int m = hi - lo;
@@ -318,108 +371,92 @@ __device__ __forceinline__ void walk_regs(const uint64_t* tape, uint32_t n, int 
 #pragma unroll
         for (int h = 0; h < KI; h++)
             cb[h] = ism ? mmb[(mbase + __popc(mball & lanemask_lt())) * KI + h] : make_uint2(0u, 0u);
-        uint32_t my_keep[KI];
+        uint32_t my_keep[KI], my_f[KI], my_s[KI];  // this lane's instruction: keep / chosen-input masks
 #pragma unroll
-        for (int h = 0; h < KI; h++) my_keep[h] = 0;
+        for (int h = 0; h < KI; h++) my_keep[h] = my_f[h] = my_s[h] = 0u;
         int live = 0;  // instructions of this chunk live in some cell
-        if (plain) {
-            for (int j = m - 1; j >= 0; j--) {
-                const uint32_t q = __shfl_sync(0xFFFFFFFFu, pk, j);
-                const uint32_t o = q & 63u, a = (q >> 6) & 63u, b = (q >> 12) & 63u, op = q >> 18;
-                uint32_t k[KI], kb[KI], anyk = 0;
+        int j = m - 1;
+        while (j >= 0) {
+            if (!plain) {
+                uint32_t u0 = 0, u1 = 0;
 #pragma unroll
                 for (int h = 0; h < KI; h++) {
-                    k[h] = (uint32_t)(lv[h] >> o) & 1u;
-                    kb[h] = __ballot_sync(0xFFFFFFFFu, k[h]);
-                    anyk |= kb[h];
+                    u0 |= lv[0][h];
+                    if constexpr (S == 2) u1 |= lv[S - 1][h];
                 }
-                if (anyk) {
-                    const bool arith = op == OP_ADD || op == OP_SUB || op == OP_MUL || op == OP_DIV;
-                    const bool mmop = is_mm(op);
-                    live++;
-#pragma unroll
-                    for (int h = 0; h < KI; h++) {
-                        uint32_t f, sc;
-                        if (mmop) {
-                            f = (__shfl_sync(0xFFFFFFFFu, cb[h].x, j) >> lane) & 1u;
-                            sc = (__shfl_sync(0xFFFFFFFFu, cb[h].y, j) >> lane) & 1u;
-                        } else {
-                            f = op != OP_CONST;
-                            sc = arith;
-                        }
-                        f &= k[h];
-                        sc &= k[h];
-                        lv[h] &= ~(1ull << o);
-                        if (f) lv[h] |= 1ull << a;
-                        if (sc) lv[h] |= 1ull << b;
-                        kept[h] += k[h];
-                        sig[h] += (k[h] + f + 2u * sc) * (uint32_t)(lo + j + 1) * 0x9E3779B1u;
-                    }
-                }
-                if ((int)lane == j) {
-#pragma unroll
-                    for (int h = 0; h < KI; h++) my_keep[h] = kb[h];
-                }
-            }
-            u_ok = false;  // (U is not maintained on this path)
-        } else {
-            if (!u_ok) {
-                U = 0;
-#pragma unroll
-                for (int h = 0; h < KI; h++)
-                    U |= (uint64_t)__reduce_or_sync(0xFFFFFFFFu, (uint32_t)lv[h]) |
-                         (uint64_t)__reduce_or_sync(0xFFFFFFFFu, (uint32_t)(lv[h] >> 32)) << 32;
-                u_ok = true;
-            }
-            int j = m - 1;
-            while (j >= 0) {
+                const uint64_t U = (uint64_t)__ballot_sync(0xFFFFFFFFu, u0 != 0u) |
+                                   (S == 2 ? (uint64_t)__ballot_sync(0xFFFFFFFFu, u1 != 0u) << 32 : 0ull);
                 const uint32_t cand = __ballot_sync(0xFFFFFFFFu, (int)lane <= j && ((U >> (pk & 63u)) & 1ull));
                 if (!cand) break;
                 j = 31 - __clz(cand);
-                const uint32_t q = __shfl_sync(0xFFFFFFFFu, pk, j);
-                const uint32_t o = q & 63u, a = (q >> 6) & 63u, b = (q >> 12) & 63u, op = q >> 18;
+            }
+            const uint32_t q = __shfl_sync(0xFFFFFFFFu, pk, j);
+            const uint32_t o = q & 63u, a = (q >> 6) & 63u, b = (q >> 12) & 63u, op = q >> 18;
+            uint32_t k[KI], anyk = 0;
+#pragma unroll
+            for (int h = 0; h < KI; h++) {
+                const uint32_t src = (S == 2 && o >= 32u) ? lv[S - 1][h] : lv[0][h];
+                k[h] = __shfl_sync(0xFFFFFFFFu, src, o & 31u);
+                anyk |= k[h];
+            }
+            if (anyk) {
                 const bool arith = op == OP_ADD || op == OP_SUB || op == OP_MUL || op == OP_DIV;
                 const bool mmop = is_mm(op);
-                uint32_t fany = 0, sany = 0;
+                const bool at_o = lane == (o & 31u), at_a = lane == (a & 31u), at_b = lane == (b & 31u);
+                live++;
 #pragma unroll
                 for (int h = 0; h < KI; h++) {
-                    const uint32_t k = (uint32_t)(lv[h] >> o) & 1u;
-                    const uint32_t kb = __ballot_sync(0xFFFFFFFFu, k);
                     uint32_t f, sc;
                     if (mmop) {
-                        f = (__shfl_sync(0xFFFFFFFFu, cb[h].x, j) >> lane) & 1u;
-                        sc = (__shfl_sync(0xFFFFFFFFu, cb[h].y, j) >> lane) & 1u;
+                        f = __shfl_sync(0xFFFFFFFFu, cb[h].x, j);
+                        sc = __shfl_sync(0xFFFFFFFFu, cb[h].y, j);
                     } else {
-                        f = op != OP_CONST;
-                        sc = arith;
+                        f = op != OP_CONST ? ~0u : 0u;
+                        sc = arith ? ~0u : 0u;
                     }
-                    f &= k;
-                    sc &= k;
-                    lv[h] &= ~(1ull << o);
-                    if (f) lv[h] |= 1ull << a;
-                    if (sc) lv[h] |= 1ull << b;
-                    kept[h] += k;
-                    sig[h] += (k + f + 2u * sc) * (uint32_t)(lo + j + 1) * 0x9E3779B1u;
-                    if ((int)lane == j) my_keep[h] = kb;
-                    if (mmop) {
-                        fany |= __ballot_sync(0xFFFFFFFFu, f);
-                        sany |= __ballot_sync(0xFFFFFFFFu, sc);
-                    } else {  // the output is live in some cell: so are the inputs it reads
-                        fany |= op != OP_CONST;
-                        sany |= arith;
+                    f &= k[h];
+                    sc &= k[h];
+                    // clear the output slot, then set the inputs the choice uses
+                    if (at_o) {
+                        if (S == 1 || o < 32u) lv[0][h] = 0u;
+                        else lv[S - 1][h] = 0u;
+                    }
+                    if (at_a) {
+                        if (S == 1 || a < 32u) lv[0][h] |= f;
+                        else lv[S - 1][h] |= f;
+                    }
+                    if (at_b) {
+                        if (S == 1 || b < 32u) lv[0][h] |= sc;
+                        else lv[S - 1][h] |= sc;
+                    }
+                    if ((int)lane == j) {
+                        my_keep[h] = k[h];
+                        if (mmop) {
+                            my_f[h] = f;
+                            my_s[h] = sc;
+                        }
                     }
                 }
-                U &= ~(1ull << o);
-                if (fany) U |= 1ull << a;
-                if (sany) U |= 1ull << b;
-                live++;
-                j--;
             }
+            j--;
         }
         plain = 2 * live >= m;  // the next chunk's mode, from this one's liveness
         if ((int)lane < m) {
             if constexpr (KI == 1) keep[lo + lane] = my_keep[0];
             else reinterpret_cast<uint2*>(keep)[lo + lane] = make_uint2(my_keep[0], my_keep[1]);
+        }
+        // per cell: the chunk's kept instructions and MIN/MAX rewrites
+#pragma unroll
+        for (int h = 0; h < KI; h++) {
+            if (!__any_sync(0xFFFFFFFFu, my_keep[h] != 0u)) continue;
+            const uint32_t kc = transpose32(my_keep[h], lane);
+            kept[h] += __popc(kc);
+            uint32_t fc = 0, sc = 0;
+            if (__any_sync(0xFFFFFFFFu, (my_f[h] | my_s[h]) != 0u)) {
+                fc = transpose32(my_f[h], lane);
+                sc = transpose32(my_s[h], lane);
+            }
+            sig[h] = sig[h] * 0x9E3779B1u + (kc ^ (uint32_t)lo) * 0x85EBCA6Bu + fc * 0xC2B2AE35u + sc * 0x27D4EB2Fu;
         }
         mm_top = mbase;
     }
@@ -444,10 +481,13 @@ template <int ROUND, int WARPS, int KI>
 __global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 5 : 20)
 interval_level_kernel(LevelLaunch p) {
     extern __shared__ __align__(16) unsigned char smem[];
-    constexpr uint32_t ROWB = 8 * KI;  // bytes per lane per slot
+    static_assert(ROUND != 2 || KI == 1, "the hybrid affine mode runs one cell per lane");
+    // bytes per lane per slot: KI intervals; the hybrid mode's 8 floats (lo, hi,
+    // c, x | y, z, e, 0) as two conflict-free half rows of 16 bytes per lane
+    constexpr uint32_t ROWB = ROUND == 2 ? 32 : 8 * KI;
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned char* wbase = smem + (size_t)warp * p.smem_per_warp;
-    const uint32_t lane_base = smem_addr(wbase) + lane * ROWB;
+    const uint32_t lane_base = smem_addr(wbase) + lane * (ROUND == 2 ? 16u : ROWB);
     uint4* stage = reinterpret_cast<uint4*>(wbase + (size_t)p.n_slots * 32 * ROWB);
     uint32_t* live = reinterpret_cast<uint32_t*>(wbase + (size_t)p.n_slots * 32 * ROWB + (STAGE + 1) * 16);
     if (lane == 0) stage[STAGE] = make_uint4(0u, 0u, 0u, 0u);  // sentinel past a full chunk
@@ -498,9 +538,9 @@ interval_level_kernel(LevelLaunch p) {
             const uint32_t dim = T.dim;
             const uint32_t words = dim * dim * dim / 32;  // mask words per node
             const uint32_t groups = words / KI;           // items per node
-            const unsigned long long local = item - t_lo;
-            const uint32_t grp = (uint32_t)(local % groups);
-            uint32_t node = (uint32_t)(local / groups);
+            uint32_t node, grp;
+            split_item(item - t_lo, groups, T.dim_sh == NOT_POW2 ? NOT_POW2 : 3 * T.dim_sh - 5 - (KI == 2),
+                       &node, &grp);
             if (p.eval_list) node = __ldcg(&p.eval_list[node]);  // the others are copies
             uint32_t* rec = T.nodes + T.ofs_l + (size_t)node * T.node_size;
             const uint32_t tape_idx = rec[0];
@@ -514,7 +554,8 @@ interval_level_kernel(LevelLaunch p) {
 #pragma unroll
             for (int h = 0; h < KI; h++) {
                 cell[h] = grp * 32 * KI + h * 32 + lane;
-                const uint32_t cz = cell[h] % dim, cy = (cell[h] / dim) % dim, cx = cell[h] / (dim * dim);
+                uint32_t cx, cy, cz;
+                cell_xyz(cell[h], dim, T.dim_sh, &cx, &cy, &cz);
                 gx[h] = ncx * dim + cx;
                 gy[h] = ncy * dim + cy;
                 gz[h] = ncz * dim + cz;
@@ -527,16 +568,62 @@ interval_level_kernel(LevelLaunch p) {
                 bz.v[h] = make_float2(loz, __fadd_rn(loz, cs));
                 bt.v[h] = make_float2(T.tt, T.tt);
             }
+            uint32_t mm = 0;
+            IVK<KI> r;
+            uint64_t pre[STAGE / 32];
+            prefetch_chunk(pre, tape, 0, n, lane);
+            if constexpr (ROUND == 2) {
+                // ---- forward pass, hybrid affine mode (device_common.cuh) ----
+                const float2 ax[3] = {bx.v[0], by.v[0], bz.v[0]};
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    const Af f = af_axis(ax[k].x, ax[k].y, k);
+                    sts_f4(lane_base + k * 32 * ROWB, make_float4(ax[k].x, ax[k].y, f.c, f.x));
+                    sts_f4(lane_base + k * 32 * ROWB + 512, make_float4(f.y, f.z, f.e, 0.0f));
+                }
+                sts_f4(lane_base + 3 * 32 * ROWB, make_float4(T.tt, T.tt, T.tt, 0.0f));
+                sts_f4(lane_base + 3 * 32 * ROWB + 512, make_float4(0.0f, 0.0f, 0.0f, 0.0f));
+                for (uint32_t base = 0; base < n; base += STAGE) {
+                    const uint32_t m = min(STAGE, n - base);
+                    __syncwarp();
+                    stage_chunk<false>(stage, pre, ROWB, lane, m);
+                    prefetch_chunk(pre, tape, base + STAGE, n, lane);
+                    __syncwarp();
+                    const uint32_t sbase = smem_addr(stage);
+                    for (uint32_t j = 0; j < m; j++) {
+                        const uint4 d = lds_u4(sbase + j * 16);
+                        float2 v;
+                        Af f;
+                        if (d.x == OP_CONST) {
+                            const float c = __uint_as_float(d.y);
+                            v = make_float2(c, c);
+                            f = Af{c, 0.0f, 0.0f, 0.0f, 0.0f};
+                        } else {
+                            const float4 a0 = lds_f4(lane_base + d.y), a1 = lds_f4(lane_base + d.y + 512);
+                            const float4 b0 = lds_f4(lane_base + d.z), b1 = lds_f4(lane_base + d.z + 512);
+                            const float2 a = make_float2(a0.x, a0.y), b = make_float2(b0.x, b0.y);
+                            const Af fa{a0.z, a0.w, a1.x, a1.y, a1.z}, fb{b0.z, b0.w, b1.x, b1.y, b1.z};
+                            uint32_t c = 0;
+                            if (is_mm(d.x)) {
+                                c = mm_choice(d.x, a, b);
+                                const uint2 ch = make_uint2(__ballot_sync(0xFFFFFFFFu, c & 1u),
+                                                            __ballot_sync(0xFFFFFFFFu, c & 2u));
+                                if (lane == 0 && mm < p.mm_cap) mmb[mm] = ch;
+                                mm++;
+                            }
+                            v = hy_apply(d.x, 0ull, a, b, fa, fb, d.x == OP_MUL && d.y == d.z, c, &f);
+                        }
+                        sts_f4(lane_base + d.w, make_float4(v.x, v.y, f.c, f.x));
+                        sts_f4(lane_base + d.w + 512, make_float4(f.y, f.z, f.e, 0.0f));
+                    }
+                }
+            } else {
             sts_iv<KI>(lane_base + 0 * 32 * ROWB, bx);
             sts_iv<KI>(lane_base + 1 * 32 * ROWB, by);
             sts_iv<KI>(lane_base + 2 * 32 * ROWB, bz);
             sts_iv<KI>(lane_base + 3 * 32 * ROWB, bt);
 
             // ---- forward interval pass (interval.comp:121-160) ----
-            uint32_t mm = 0;
-            IVK<KI> r;
-            uint64_t pre[STAGE / 32];
-            prefetch_chunk(pre, tape, 0, n, lane);
             for (uint32_t base = 0; base < n; base += STAGE) {
                 const uint32_t m = min(STAGE, n - base);
                 __syncwarp();
@@ -558,6 +645,7 @@ interval_level_kernel(LevelLaunch p) {
                     }
                     sts_iv<KI>(lane_base + d.w, r);
                 }
+            }
             }
             __syncwarp();
             stat_work += 32ull * KI * n;
@@ -615,10 +703,12 @@ interval_level_kernel(LevelLaunch p) {
                     kept[h] = 0;
                     sig[h] = 0;
                 }
-                if (p.n_slots <= 64) {
-                    // per-cell slot bitsets in registers, like the reference's
-                    // per-thread bitset: no shared memory on the walk's path
-                    walk_regs<KI>(tape, n, (int)mm, mmb, keep, ok_w, lane, kept, sig);
+                if (p.n_slots <= 32) {
+                    // live sets spread over the lanes' registers: no shared
+                    // memory on the walk's path
+                    walk_lanes<KI, 1>(tape, n, (int)mm, mmb, keep, ok_w, lane, kept, sig);
+                } else if (p.n_slots <= 64) {
+                    walk_lanes<KI, 2>(tape, n, (int)mm, mmb, keep, ok_w, lane, kept, sig);
                 } else {
                     // wider slot files: transposed bitsets, live[s][h] bit l =
                     // slot s is live for cell grp*32*KI + h*32 + l. The
@@ -1049,9 +1139,10 @@ point_level_kernel(LevelLaunch p) {
             const uint32_t words = dim * dim * dim / 32;      // mask words per node
             const uint32_t groups = words / K;                // items per node
             const float cs = T.cs;
-            const unsigned long long local = item - t_lo;
-            const uint32_t grp = (uint32_t)(local % groups);
-            uint32_t node = (uint32_t)(local / groups);
+            constexpr uint32_t LOG2K = K == 8 ? 3 : (K == 4 ? 2 : 1);
+            uint32_t node, grp;
+            split_item(item - t_lo, groups, T.dim_sh == NOT_POW2 ? NOT_POW2 : 3 * T.dim_sh - 5 - LOG2K, &node,
+                       &grp);
             if (p.eval_list) node = __ldcg(&p.eval_list[node]);  // the others are copies
             uint32_t* rec = T.nodes + T.ofs_l + (size_t)node * T.node_size;
             const uint32_t tape_idx = rec[0];
@@ -1062,7 +1153,8 @@ point_level_kernel(LevelLaunch p) {
 #pragma unroll
             for (int k = 0; k < K; k++) {
                 const uint32_t cell = grp * 32 * K + k * 32 + lane;
-                const uint32_t cz = cell % dim, cy = (cell / dim) % dim, cx = cell / (dim * dim);
+                uint32_t cx, cy, cz;
+                cell_xyz(cell, dim, T.dim_sh, &cx, &cy, &cz);
                 px.v[k] = __fadd_rn(T.lx, __fmul_rn((float)(ncx * dim + cx), cs));
                 py.v[k] = __fadd_rn(T.ly, __fmul_rn((float)(ncy * dim + cy), cs));
                 pz.v[k] = __fadd_rn(T.lz, __fmul_rn((float)(ncz * dim + cz), cs));
@@ -1325,6 +1417,9 @@ static cudaError_t plan_point(uint32_t n_slots, LevelPlan* plan, int warps_hint)
 
 template <int KI>
 static cudaError_t plan_interval(bool four, int rounding, uint32_t iv, LevelPlan* plan) {
+    if (rounding == 2)
+        return four ? occupancy(dev::interval_level_kernel<2, 4, 1>, 128, 4 * iv, &plan->blocks)
+                    : occupancy(dev::interval_level_kernel<2, 1, 1>, 32, iv, &plan->blocks);
     if (four)
         return rounding ? occupancy(dev::interval_level_kernel<1, 4, KI>, 128, 4 * iv, &plan->blocks)
                         : occupancy(dev::interval_level_kernel<0, 4, KI>, 128, 4 * iv, &plan->blocks);
@@ -1343,9 +1438,13 @@ cudaError_t plan_levels(uint32_t n_slots, uint32_t mm_cap, int point_k, int roun
     const auto iv_bytes = [&](uint32_t k) {
         return (n_slots * 256 * k + (dev::STAGE + 1) * 16 + n_slots * 4 * k + 15) / 16 * 16;
     };
-    const int ki = interval_ki == 1 || interval_ki == 2 ? interval_ki : (16 * iv_bytes(2) <= 227 * 1024 ? 2 : 1);
+    // The hybrid affine mode: one cell per lane, 32-byte slot rows (four
+    // times an interval's).
+    const int ki = rounding == 2 ? 1
+                                 : (interval_ki == 1 || interval_ki == 2 ? interval_ki
+                                                                         : (16 * iv_bytes(2) <= 227 * 1024 ? 2 : 1));
     plan->interval_ki = ki;
-    const uint32_t iv = iv_bytes((uint32_t)ki);
+    const uint32_t iv = rounding == 2 ? iv_bytes(4) : iv_bytes((uint32_t)ki);
     plan->smem_per_warp = iv;
     // Four warps (four tapes) per block when they fit in shared memory, else
     // one; a hint of 1 or 4 overrides the choice where shared memory allows.
@@ -1410,7 +1509,10 @@ cudaError_t launch_level(const LevelLaunch& a, const LevelPlan& plan, int roundi
     const size_t smem = (size_t)w * plan.smem_per_warp;
     const int tpb = 32 * w;
 #define FREP_IV_LAUNCH(R, W, KI) dev::interval_level_kernel<R, W, KI><<<plan.blocks, tpb, smem, stream>>>(b)
-    if ((interval_ki ? interval_ki : plan.interval_ki) == 2) {
+    if (rounding == 2) {
+        if (w == 4) FREP_IV_LAUNCH(2, 4, 1);
+        else FREP_IV_LAUNCH(2, 1, 1);
+    } else if ((interval_ki ? interval_ki : plan.interval_ki) == 2) {
         if (w == 4) {
             if (rounding) FREP_IV_LAUNCH(1, 4, 2);
             else FREP_IV_LAUNCH(0, 4, 2);

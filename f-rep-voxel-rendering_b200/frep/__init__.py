@@ -24,10 +24,11 @@ from . import _lib as L
 from ._lib import FrepError
 
 __all__ = ["csg", "Tape", "Context", "VoxelStorage", "Voxelizer", "Camera", "Lights", "Raytracer",
-           "FrepError", "ROUND_NEAREST", "ROUND_OUTWARD", "TreeExport", "CompactTree"]
+           "FrepError", "ROUND_NEAREST", "ROUND_OUTWARD", "ROUND_HYBRID", "TreeExport", "CompactTree"]
 
 ROUND_NEAREST = 0
 ROUND_OUTWARD = 1
+ROUND_HYBRID = 2   # outward intervals intersected with affine forms (include/frep.h)
 
 
 def _ptr(a: np.ndarray):

@@ -173,8 +173,18 @@ typedef struct frep_grid {
 
 enum {
     FREP_ROUND_NEAREST = 0,   /* the reference's round-to-nearest intervals       */
-    FREP_ROUND_OUTWARD = 1    /* directed rounding: every interval is conservative */
+    FREP_ROUND_OUTWARD = 1,   /* directed rounding: every interval is conservative */
+    FREP_ROUND_HYBRID = 2     /* outward intervals intersected with affine forms  */
 };
+/* FREP_ROUND_HYBRID is this library's own mode, the working counterpart of
+ * the reference's abandoned affine evaluator (vulkan/shaders/tape/affine.comp,
+ * commented out): every slot also carries an affine form over the cell's
+ * axes, c + x ex + y ey + z ez + [-e, e], with every rounding error added to e
+ * (rounded up), and keeps its outward interval intersected with the form's
+ * range. Conservative like FREP_ROUND_OUTWARD and never looser; much tighter
+ * where intervals suffer from the dependency problem (polynomials such as
+ * the reference's TangleCube, x^4 - 8 x^2 + ...), so fewer cells stay
+ * ambiguous. The interval passes run one cell per lane with 32-byte slot rows. */
 
 typedef struct frep_voxelize_opts {
     uint32_t rounding;        /* FREP_ROUND_*                                        */

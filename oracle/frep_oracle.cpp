@@ -175,10 +175,130 @@ inline Iv interval_op(uint32_t op, uint64_t w, Iv a, Iv b, int rounding) {
     return a;
 }
 
+// ---- hybrid affine mode (rounding 2; this library's own, see frep.h) --------
+// Each slot carries its outward interval and an affine form over the cell's
+// axes, A = c + x ex + y ey + z ez + [-e, e] (ex, ey, ez in [-1, 1]); every
+// instruction computes the outward interval of its operands' intervals and the
+// affine form, and the slot keeps the interval intersected with the form's
+// range. Forms take their centre and coefficients rounded to nearest and add
+// every rounding error to e, rounded up. Evaluated with FE_DOWNWARD active
+// (as the outward intervals are); nearest operations switch the mode.
+struct Af {
+    float c, x, y, z, e;
+};
+inline float rn_add(float a, float b) { std::fesetround(FE_TONEAREST); const float r = a + b; std::fesetround(FE_DOWNWARD); return r; }
+inline float rn_sub(float a, float b) { std::fesetround(FE_TONEAREST); const float r = a - b; std::fesetround(FE_DOWNWARD); return r; }
+inline float rn_mul(float a, float b) { std::fesetround(FE_TONEAREST); const float r = a * b; std::fesetround(FE_DOWNWARD); return r; }
+// bound on the error of a round-to-nearest result r: |r| 2^-23 + 2^-149, up
+inline float af_err(float r) { return add_up(mul_up(std::fabs(r), 0x1p-23f), 0x1p-149f); }
+// radius of the non-constant part, summed left to right, rounded up
+inline float af_rad(const Af& a) {
+    return add_up(add_up(add_up(std::fabs(a.x), std::fabs(a.y)), std::fabs(a.z)), a.e);
+}
+inline Af af_hull(Iv v) {
+    const float c = rn_mul(rn_add(v.lo, v.hi), 0.5f);
+    return {c, 0.0f, 0.0f, 0.0f, max_sel(sub_up(v.hi, c), sub_up(c, v.lo))};
+}
+// the interval intersected with the form's range (NaN forms leave it as is)
+inline Iv af_tighten(Iv v, const Af& a) {
+    const float r = af_rad(a);
+    return {max_sel(v.lo, sub_dn(a.c, r)), min_sel(v.hi, add_up(a.c, r))};
+}
+inline Af af_addsub(const Af& a, const Af& b, bool sub) {
+    Af r;
+    r.c = sub ? rn_sub(a.c, b.c) : rn_add(a.c, b.c);
+    r.x = sub ? rn_sub(a.x, b.x) : rn_add(a.x, b.x);
+    r.y = sub ? rn_sub(a.y, b.y) : rn_add(a.y, b.y);
+    r.z = sub ? rn_sub(a.z, b.z) : rn_add(a.z, b.z);
+    r.e = add_up(add_up(a.e, b.e), add_up(add_up(af_err(r.c), af_err(r.x)), add_up(af_err(r.y), af_err(r.z))));
+    return r;
+}
+inline Af af_mul(const Af& a, const Af& b, bool square) {
+    Af r;
+    const float ra = af_rad(a);
+    if (square) {  // (c + s)^2 = c^2 + 2 c s + s^2, s^2 in [0, ra^2] = h +- h
+        const float h = mul_up(mul_up(ra, ra), 0.5f);
+        const float cc = rn_mul(a.c, a.c);
+        r.c = rn_add(cc, h);
+        r.x = rn_mul(rn_mul(a.c, a.x), 2.0f);
+        r.y = rn_mul(rn_mul(a.c, a.y), 2.0f);
+        r.z = rn_mul(rn_mul(a.c, a.z), 2.0f);
+        const float lin = mul_up(mul_up(std::fabs(a.c), 2.0f), a.e);
+        r.e = add_up(add_up(add_up(lin, h), add_up(af_err(cc), af_err(r.c))),
+                     add_up(add_up(af_err(r.x), af_err(r.y)), af_err(r.z)));
+        return r;
+    }
+    const float rb = af_rad(b);
+    r.c = rn_mul(a.c, b.c);
+    const float x1 = rn_mul(a.c, b.x), x2 = rn_mul(b.c, a.x);
+    const float y1 = rn_mul(a.c, b.y), y2 = rn_mul(b.c, a.y);
+    const float z1 = rn_mul(a.c, b.z), z2 = rn_mul(b.c, a.z);
+    r.x = rn_add(x1, x2);
+    r.y = rn_add(y1, y2);
+    r.z = rn_add(z1, z2);
+    const float lin = add_up(mul_up(std::fabs(a.c), b.e), mul_up(std::fabs(b.c), a.e));
+    const float rnd = add_up(add_up(add_up(af_err(x1), af_err(x2)), add_up(af_err(y1), af_err(y2))),
+                             add_up(add_up(af_err(z1), af_err(z2)),
+                                    add_up(add_up(af_err(r.x), af_err(r.y)), af_err(r.z))));
+    r.e = add_up(add_up(lin, mul_up(ra, rb)), add_up(af_err(r.c), rnd));
+    return r;
+}
+
+Iv eval_hybrid(const uint64_t* tape, uint32_t n, std::vector<Iv>& slots, std::vector<Af>& forms,
+               const float* lo3, const float* hi3, float t, uint8_t* choices) {
+    RoundMode mode(FE_DOWNWARD);
+    for (int k = 0; k < 3; k++) {
+        slots[k] = {lo3[k], hi3[k]};
+        const float c = rn_mul(rn_add(lo3[k], hi3[k]), 0.5f);
+        const float r = max_sel(sub_up(hi3[k], c), sub_up(c, lo3[k]));
+        forms[k] = {c, k == 0 ? r : 0.0f, k == 1 ? r : 0.0f, k == 2 ? r : 0.0f, 0.0f};
+    }
+    slots[3] = {t, t};
+    forms[3] = {t, 0.0f, 0.0f, 0.0f, 0.0f};
+    uint32_t mm = 0;
+    for (uint32_t i = 0; i < n; i++) {
+        const uint64_t w = tape[i];
+        const uint32_t op = i_op(w);
+        const Iv a = op == OP_CONST ? Iv{0, 0} : slots[i_a(w)];
+        const Iv b = op == OP_CONST ? Iv{0, 0} : slots[i_b(w)];
+        const Af fa = op == OP_CONST ? Af{} : forms[i_a(w)];
+        const Af fb = op == OP_CONST ? Af{} : forms[i_b(w)];
+        const Iv v = interval_op(op, w, a, b, 1);
+        Af f;
+        switch (op) {
+            case OP_CONST: f = {v.lo, 0.0f, 0.0f, 0.0f, 0.0f}; break;
+            case OP_ADD: f = af_addsub(fa, fb, false); break;
+            case OP_SUB: f = af_addsub(fa, fb, true); break;
+            case OP_NEG: f = {-fa.c, -fa.x, -fa.y, -fa.z, fa.e}; break;
+            case OP_MUL: f = af_mul(fa, fb, i_a(w) == i_b(w)); break;
+            case OP_COPY: f = fa; break;
+            case OP_MIN:
+            case OP_MAX: {
+                const bool first_low = a.hi < b.lo, second_low = b.hi < a.lo;
+                const uint8_t c = op == OP_MIN ? (first_low ? MM_FIRST : (second_low ? MM_SECOND : MM_BOTH))
+                                               : (first_low ? MM_SECOND : (second_low ? MM_FIRST : MM_BOTH));
+                if (choices) choices[mm] = c;
+                mm++;
+                f = c == MM_FIRST ? fa : (c == MM_SECOND ? fb : af_hull(v));
+                break;
+            }
+            default: f = af_hull(v); break;  // DIV SQRT EXP SIN COS: the interval's hull
+        }
+        slots[i_out(w)] = af_tighten(v, f);
+        forms[i_out(w)] = f;
+    }
+    return slots[0];
+}
+
 // tape_eval_interval (interval.comp:121-160): slots 0..3 = box x, y, z and
 // [t, t]; MIN/MAX record FIRST/SECOND/BOTH with strict comparisons.
+// rounding 2 = the hybrid affine mode (eval_hybrid).
 Iv eval_interval(const uint64_t* tape, uint32_t n, std::vector<Iv>& slots, const float* lo3,
                  const float* hi3, float t, int rounding, uint8_t* choices) {
+    if (rounding == 2) {
+        std::vector<Af> forms(slots.size());
+        return eval_hybrid(tape, n, slots, forms, lo3, hi3, t, choices);
+    }
     slots[0] = {lo3[0], hi3[0]};
     slots[1] = {lo3[1], hi3[1]};
     slots[2] = {lo3[2], hi3[2]};
