@@ -59,12 +59,19 @@ def parse():
     ap.add_argument("--scenes", type=int, default=512, help="batch: number of scenes")
     ap.add_argument("--plain-steps", type=int, default=2, help="batch: timed passes of the plain launch loop")
     ap.add_argument("--no-tune", action="store_true", help="batch: default branching, no autotuning")
-    ap.add_argument("--tune-cache", default=None, help="batch: autotuner cache file (JSON)")
+    ap.add_argument("--tune-cache", default=None,
+                    help="batch: tuning file to start from and to write (default: read the committed "
+                         "f-rep-voxel-rendering_b200/frep/tuning_b200.json, write nothing)")
+    ap.add_argument("--retune", action="store_true",
+                    help="batch: re-time every class against its tuned choice (the incumbent is kept "
+                         "unless beaten by the tuner's margin)")
+    ap.add_argument("--serve-inflight", type=int, default=0,
+                    help="batch: steps the server keeps on the device (0 = library default)")
     ap.add_argument("--budget-gb", type=int, default=150, help="HBM budget of the context, GB")
-    ap.add_argument("--serve-seconds", type=float, default=10.0,
+    ap.add_argument("--serve-seconds", type=float, default=60.0,
                     help="batch: seconds of the serving run after the batch measurements (0 = none)")
     ap.add_argument("--serve-rate", type=float, default=1000.0, help="batch: Poisson request rate, requests/s")
-    ap.add_argument("--serve-sweep", default="",
+    ap.add_argument("--serve-sweep", default="200,2000",
                     help="batch: extra request rates (comma separated, requests/s), each served for "
                          "--serve-seconds after the main serving phase; results under serving_sweep")
     ap.add_argument("--serve-budget-gb", type=int, default=120, help="batch: tree arena of the server, GB")
@@ -538,6 +545,13 @@ def cpu_sample_order(n: int):
     return [int(i) for i in np.random.default_rng(17).permutation(n)]
 
 
+def tuning_table():
+    """The committed tuning of the batch workload (frep.autotune.DEFAULT_TABLE),
+    None when absent."""
+    from frep.autotune import DEFAULT_TABLE
+    return DEFAULT_TABLE if os.path.exists(DEFAULT_TABLE) else None
+
+
 # The CPU figures of the batch workload (the reference arm and the GPU arm's
 # cpu_baseline leg) time the same scenes: the first CPU_SAMPLE of a seeded
 # permutation of the batch, each at the grid the GPU arm runs it with.
@@ -564,7 +578,7 @@ def run_reference_batch(args, world, rank):
     if rank != 0:
         return
     from frep.autotune import load_table
-    table = load_table(args.tune_cache)
+    table = load_table(args.tune_cache or tuning_table())
     order = cpu_sample_order(args.scenes)
     idx = [order[i % CPU_SAMPLE] for i in range(max(args.steps, args.warmup))]
     built = {i: sc for i, sc in zip(sorted(set(idx)), make_batch_scenes(args, indices=sorted(set(idx))))}
@@ -580,7 +594,7 @@ def run_reference_batch(args, world, rank):
     value = args.steps / total
     sample = (f"{args.steps} scenes of the batch (the first {min(args.steps, CPU_SAMPLE)} of a seeded permutation, "
               f"the GPU arm's cpu_baseline sample), each voxelized at the grid the GPU arm's tuning table "
-              f"({'committed' if args.tune_cache else 'none: default'} branchings) gives it + rendered "
+              f"({'given' if args.tune_cache else ('committed' if tuning_table() else 'none: default')} branchings) gives it + rendered "
               f"{args.width}x{args.height}; oracle C++ port, {threads} threads")
     line = {
         "metric": METRIC, "value": value, "unit": "scenes/s", "n_gpus": args.gpus, "steps": args.steps,
@@ -614,7 +628,7 @@ def serve_phase(args, ctx, scs, chosen, pools, warps):
     n_req = max(1, int(args.serve_rate * args.serve_seconds))
     arrivals = np.cumsum(rng.exponential(1.0 / args.serve_rate, n_req))
     srv = frep.Server(ctx, hbm_budget_bytes=args.serve_budget_gb << 30, lights=frep.Lights(shadow_mask=1),
-                      warps=warps)
+                      warps=warps, max_inflight=args.serve_inflight)
     wides = [sc.shape.wide() for sc in scs]
     recent = collections.deque(maxlen=64)
     plan = []
@@ -748,9 +762,9 @@ def run_ours_batch(args, world, rank, local):
 
     # ---- untimed setup: autotune, size the pools, build resident trees -------
     t0 = time.perf_counter()
-    tuner = Autotuner(ctx, cache_path=args.tune_cache)
+    tuner = Autotuner(ctx, cache_path=args.tune_cache or tuning_table(), save_path=args.tune_cache)
     if not args.no_tune:
-        tuner.tune(scs)
+        tuner.tune(scs, refine=args.retune)
     t_tune = time.perf_counter() - t0
     chosen = [tuner.apply(sc) for sc in scs]
     pools = fit_pools(ctx, [sc.shape for sc in scs], [d for d, _ in chosen], scs[0].low_vertex, scs[0].world_size)

@@ -117,9 +117,12 @@ class Autotuner:
     (frep_batch_autotune), with the tapes per block for the batch."""
 
     def __init__(self, ctx: Context, cache_path: str | None = None, per_class: int = 4, reps: int = 5,
-                 margin: float = 0.03):
+                 margin: float = 0.03, save_path: str | None = "same"):
+        """cache_path: tuning file to start from; save_path: where tune()
+        writes the result ("same": cache_path; None: nowhere)."""
         self.ctx = ctx
         self.cache_path = cache_path
+        self.save_path = save_path
         self.per_class = per_class
         self.reps = reps
         self.margin = margin
@@ -144,7 +147,7 @@ class Autotuner:
             return "unknown"
 
     def save(self, path: str | None = None) -> None:
-        path = path or self.cache_path
+        path = path or (self.cache_path if self.save_path == "same" else self.save_path)
         if path:
             os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
             L.check(L.lib().frep_tuning_save(self._h, path.encode(), self.device.encode()))
