@@ -88,12 +88,13 @@ class Report:
 
 
 def check_tree(export, root_wide, root_slots, low, world_size, tape_time, interval_fn, *, nodes_per_level=24,
-               cells_per_node=48, per_axis=9, seed=0, report=None):
+               cells_per_node=48, per_axis=9, seed=0, report=None, root_cells=None):
     """Runs checks (a)-(c) on a sample of `export`'s nodes (a frep TreeExport
     or an oracle.OracleTree: levels, dims, node_count, node_offset,
     node_size, nodes, tapes). interval_fn(wide, n_slots, boxes (M, 6), t)
     returns the (M, 2) intervals to check (the device's or the oracle's).
-    Ambiguous and classified cells are preferred: they carry the tight bounds."""
+    Ambiguous and classified cells are preferred: they carry the tight bounds.
+    root_cells: cells sampled in the root node (default cells_per_node)."""
     rng = np.random.default_rng(seed)
     rep = report or Report()
     dims = list(export.dims)
@@ -115,9 +116,10 @@ def check_tree(export, root_wide, root_slots, low, world_size, tape_time, interv
             inter = np.unpackbits(rec[4 + W:4 + 2 * W].astype("<u4").view(np.uint8), bitorder="little").astype(bool)
             marked = np.nonzero(leaf | inter)[0]
             rest = np.nonzero(~(leaf | inter))[0]
-            k1 = min(len(marked), cells_per_node * 3 // 4)
+            want = root_cells if (lvl == 0 and root_cells) else cells_per_node
+            k1 = min(len(marked), want * 3 // 4)
             sel = list(rng.choice(marked, size=k1, replace=False)) if k1 else []
-            k2 = min(len(rest), cells_per_node - k1)
+            k2 = min(len(rest), want - k1)
             sel += list(rng.choice(rest, size=k2, replace=False)) if k2 else []
             cells = np.array(sorted(sel), np.int64)
             if len(cells) == 0:

@@ -81,7 +81,7 @@ def test_device_outward_tree_is_sound(ctx, name, make, t):
         return iv
 
     rep = check_tree(exp, vs.tape.wide(), vs.tape.n_slots, sc.low_vertex, sc.world_size, t, device_intervals,
-                     nodes_per_level=12, cells_per_node=32, per_axis=9, seed=1)
+                     nodes_per_level=12, cells_per_node=32, per_axis=9, seed=1, root_cells=64)
     s = rep.summary()
     s.update(tape_instructions=vs.tape.n_instr, grid=list(sc.grid_dims), tape_time=t)
     _REPORT[name] = s
