@@ -475,10 +475,11 @@ __device__ __forceinline__ void walk_lanes(const uint64_t* tape, uint32_t n, int
 // with the tape, and in shared memory they would cap the resident warps for
 // every tree of a batch at what its longest tape allows.
 template <int ROUND, int WARPS, int KI>
-// At least 20 warps per SM (5 blocks of 4 or 20 of 1): caps registers at 96,
-// which measured ~11 % faster than the unbounded 128 (more warps hide the
-// shared-memory and branch latencies of the interpreter); a cap of 80 spills.
-__global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 5 : 20)
+// At least 16 warps per SM (4 blocks of 4 or 16 of 1): up to 128 registers.
+// Shared memory already limits a batch's plan to about 16 resident warps, and
+// a cap of 96 registers spills inside the forward pass: on a 128-scene batch
+// the level-1 pass measured 35.0 ms with the cap and 26.7 ms without.
+__global__ void __launch_bounds__(WARPS * 32, WARPS == 4 ? 4 : 16)
 interval_level_kernel(LevelLaunch p) {
     extern __shared__ __align__(16) unsigned char smem[];
     static_assert(ROUND != 2 || KI == 1, "the hybrid affine mode runs one cell per lane");
