@@ -234,7 +234,7 @@ frep_status prepare_voxelize(frep_batch* b, const frep_tape* const* tapes, TapeS
     if (r == FREP_OK)
         r = ensure_keep(b, (uint64_t)std::max(b->plan4.blocks * b->plan4.warps_per_block,
                                               b->plan2.blocks * b->plan2.warps_per_block) *
-                               frep::warp_scratch(st->longest, st->mm, (uint32_t)b->plan4.interval_ki).stride);
+                               frep::warp_scratch(st->longest, st->mm, (uint32_t)b->plan4.interval_ki, b->rounding != 2).stride);
     return r;
 }
 
@@ -265,9 +265,11 @@ frep_status enqueue_voxelize(frep_batch* b, const uint8_t* d_area, const TapeSta
     a.cursor = b->d_cursor;
     a.n_trees = n;
     a.keep_scratch = b->keep;
-    const frep::WarpScratch ws = frep::warp_scratch(st.longest, st.mm, (uint32_t)b->plan4.interval_ki);
+    const frep::WarpScratch ws = frep::warp_scratch(st.longest, st.mm, (uint32_t)b->plan4.interval_ki, b->rounding != 2);
     a.keep_stride = ws.stride;
     a.mm_ofs = ws.mm_ofs;
+    a.item_ofs = ws.item_ofs;
+    a.item_cap = ws.item_cap;
     a.n_slots = st.slots;
     a.mm_cap = st.mm;
     const int ki0 = level0_cells(b);

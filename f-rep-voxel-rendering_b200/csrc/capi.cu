@@ -429,6 +429,8 @@ frep_status enqueue_tree_levels(frep_tree* tree, const frep_tape* tape, float ta
     a.keep_scratch = keep;
     a.keep_stride = ws.stride;
     a.mm_ofs = ws.mm_ofs;
+    a.item_ofs = ws.item_ofs;
+    a.item_cap = ws.item_cap;
     a.n_slots = std::max<uint32_t>(tape->ct.n_slots, 4);
     a.mm_cap = std::max<uint32_t>(tape->ct.n_minmax, 1);
     a.eval_list = prev ? tree->reuse_list : nullptr;
@@ -501,7 +503,8 @@ frep_status voxelize_impl(frep_ctx* ctx, frep_tree* tree, const frep_tree* prev,
     frep_status pst = ensure_plan(tree, tape, "frep_voxelize");
     if (pst != FREP_OK) return pst;
     // Per-warp scratch: a keep mask per instruction, a choice-mask pair per MIN/MAX.
-    const frep::WarpScratch ws = frep::warp_scratch(n, tape->ct.n_minmax, (uint32_t)tree->plan.interval_ki);
+    const frep::WarpScratch ws = frep::warp_scratch(n, tape->ct.n_minmax, (uint32_t)tree->plan.interval_ki,
+                                                    tree->opts.rounding != FREP_ROUND_HYBRID);
     const uint64_t keep_words = (uint64_t)tree->plan.blocks * tree->plan.warps_per_block * ws.stride;
     if (keep_words > tree->keep_words) {
         if (tree->keep) {

@@ -30,20 +30,33 @@ struct LevelLaunch {
     uint32_t any_point_k;              // 1: a one-tree launch, whose last level runs with the
                                        //   launch's cells per lane whatever the tree's batch
                                        //   kind (TreeHeader::point_k); 0: only trees of that kind
+    uint32_t item_ofs;                 // per-warp scratch, u32 words: where the item tapes start
+    uint32_t item_cap;                 //   and how many u64 words they may take (0 = no item
+                                       //   pruning in the interval passes)
 };
 
 // Per-warp global scratch of the interval pass, in u32 words: one keep mask per
-// instruction of the longest tape, then a pair of choice masks per MIN/MAX.
+// instruction of the longest tape, then a pair of choice masks per MIN/MAX,
+// then (with item pruning) the work items' pruned tapes, u64 words.
 struct WarpScratch {
-    uint32_t stride;  // words per warp
-    uint32_t mm_ofs;  // where the choice masks start
+    uint32_t stride;    // words per warp
+    uint32_t mm_ofs;    // where the choice masks start
+    uint32_t item_ofs;  // where the item tapes start
+    uint32_t item_cap;  // u64 words of item tapes (0 = no item pruning)
 };
+// At most this many u64 words of item tapes per warp (~256 KB, below 2^15 so
+// that an item tape's offset and length pack into 15 bits each): a group of
+// up to 32 items of one node stores the pruned tapes that fit, the others run
+// on the node's tape.
+constexpr uint32_t kItemTapeWords = 32752;
 // ki: cells per lane of the interval pass (a keep mask and a choice-mask pair
-// per group of 32 cells).
-inline WarpScratch warp_scratch(uint32_t longest, uint32_t mm_cap, uint32_t ki) {
+// per group of 32 cells). items: room for item tapes.
+inline WarpScratch warp_scratch(uint32_t longest, uint32_t mm_cap, uint32_t ki, bool items = false) {
     const uint32_t k = (ki * (longest ? longest : 1u) + 31u) / 32u * 32u;
     const uint32_t m = (2u * ki * (mm_cap ? mm_cap : 1u) + 31u) / 32u * 32u;
-    return WarpScratch{k + m, k};
+    const uint64_t want = 32ull * (longest ? longest : 1u);
+    const uint32_t ic = items ? (uint32_t)(want < kItemTapeWords ? (want + 15u) / 16u * 16u : kItemTapeWords) : 0u;
+    return WarpScratch{k + m + 2u * ic, k, k + m, ic};
 }
 
 

@@ -462,6 +462,159 @@ __device__ __forceinline__ void walk_lanes(const uint64_t* tape, uint32_t n, int
     }
 }
 
+// ---- item-level pruning (this library's addition) ----------------------------------
+//
+// Before the cells of a work item are evaluated, the node's tape is evaluated
+// once over the item's bounding box and shortened there, like a cell's tape;
+// the cells then run that shorter tape. This is exact: for algebraic tapes
+// (no SIN/COS/EXP, whose rounding is not monotone) whose every interval over
+// the item box is finite, each formula of interval.comp:8-111 is monotone in
+// its operands' bounds in both roundings, so every cell's interval lies inside
+// the item's; a MIN/MAX decided over the item box is decided the same way in
+// every cell and an instruction dead for the item is dead for every cell. A
+// cell's child tape, the node tape shortened by the cell's choices, is then
+// the item tape shortened by the same choices, word for word. An item box
+// that is empty (low > 0) or inside (high < 0) makes every cell of the item
+// empty or a leaf without evaluating them.
+//
+// Up to 32 consecutive items of one node are prepared together, one per lane
+// (the same forward pass and backward walk as cells, one box per lane); each
+// item's tape goes to the warp's item scratch while it fits. Returns per lane
+// (one item) a packed plan: bits 0-1 the mode, 0 = run the node's tape, 1 =
+// run the item tape, 2 = every cell empty, 3 = every cell a leaf; bits 2-16
+// the item tape's offset in the scratch, bits 17-31 its length (both below
+// 2^15: the scratch holds at most kItemTapeWords < 2^15 words).
+struct ItemNode {  // the node of a group of items, and its tree's frame
+    uint32_t dim, dim_sh, ncx, ncy, ncz;
+    float cs, lx, ly, lz, tt;
+};
+template <int ROUND, int KI>
+__device__ __noinline__ uint32_t prepare_items(const uint64_t* tape, uint32_t n, const ItemNode T, uint32_t grp,
+                                               uint32_t g, uint32_t lane_base, uint4* stage, uint32_t* keep,
+                                               uint2* mmb, uint64_t* items, uint32_t mm_cap, uint32_t n_slots,
+                                               uint32_t item_cap) {
+    constexpr uint32_t ROWB = 8 * KI;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t dim = T.dim, ncx = T.ncx, ncy = T.ncy, ncz = T.ncz;
+    const bool valid = lane < g;
+    // the item's cells are 32 * KI consecutive bit indices: their bounding box
+    const uint32_t c0 = (grp + (valid ? lane : 0u)) * 32u * KI, c1 = c0 + 32u * KI - 1u;
+    uint32_t x0, y0, z0, x1, y1, z1;
+    cell_xyz(c0, dim, T.dim_sh, &x0, &y0, &z0);
+    cell_xyz(c1, dim, T.dim_sh, &x1, &y1, &z1);
+    if (x0 != x1) {
+        y0 = 0;
+        y1 = dim - 1;
+        z0 = 0;
+        z1 = dim - 1;
+    } else if (y0 != y1) {
+        z0 = 0;
+        z1 = dim - 1;
+    }
+    // the cells' own box formula (voxelizer/main.comp:113-126), so the item box
+    // contains each of them exactly
+    const float cs = T.cs;
+    const uint32_t glo[3] = {ncx * dim + x0, ncy * dim + y0, ncz * dim + z0};
+    const uint32_t ghi[3] = {ncx * dim + x1, ncy * dim + y1, ncz * dim + z1};
+    const float low[3] = {T.lx, T.ly, T.lz};
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        IVK<1> b;
+        b.v[0] = make_float2(__fadd_rn(low[k], __fmul_rn((float)glo[k], cs)),
+                             __fadd_rn(__fadd_rn(low[k], __fmul_rn((float)ghi[k], cs)), cs));
+        sts_iv<1>(lane_base + k * 32 * ROWB, b);
+    }
+    {
+        IVK<1> b;
+        b.v[0] = make_float2(T.tt, T.tt);
+        sts_iv<1>(lane_base + 3 * 32 * ROWB, b);
+    }
+    uint32_t mm = 0;
+    bool fin = true, trans = false;
+    IVK<1> r;
+    uint64_t pre[STAGE / 32];
+    prefetch_chunk(pre, tape, 0, n, lane);
+    for (uint32_t base = 0; base < n; base += STAGE) {
+        const uint32_t m = min(STAGE, n - base);
+        __syncwarp();
+        stage_chunk<false>(stage, pre, ROWB, lane, m);
+        prefetch_chunk(pre, tape, base + STAGE, n, lane);
+        __syncwarp();
+        const uint32_t sbase = smem_addr(stage);
+        for (uint32_t j = 0; j < m; j++) {
+            const uint4 d = lds_u4(sbase + j * 16);
+            if (d.x == OP_CONST) {
+                const float c = __uint_as_float(d.y);
+                r.v[0] = make_float2(c, c);
+            } else {
+                trans |= d.x == OP_SIN || d.x == OP_COS || d.x == OP_EXP;
+                r = iv_exec<ROUND, 1>(d, lane_base, lane, mmb, mm, mm_cap);
+            }
+            fin &= fabsf(r.v[0].x) <= 3.40282347e38f && fabsf(r.v[0].y) <= 3.40282347e38f;
+            sts_iv<1>(lane_base + d.w, r);
+        }
+    }
+    __syncwarp();
+    if (trans || mm > mm_cap) return 0u;  // the whole group runs the node's tape
+    const IVK<1> res = lds_iv<1>(lane_base);
+    const bool empty = res.v[0].x > 0.0f, full = !empty && res.v[0].y < 0.0f;
+    uint32_t plan = 0;
+    if (valid && fin && empty) plan = 2;
+    if (valid && fin && full) plan = 3;
+    const uint32_t cand = __ballot_sync(0xFFFFFFFFu, valid && fin && !empty && !full);
+    if (!cand || n_slots > 64) return plan;
+    uint32_t ok_w[1] = {cand}, kept[1] = {0}, sig[1] = {0};
+    if (n_slots <= 32) walk_lanes<1, 1>(tape, n, (int)mm, mmb, keep, ok_w, lane, kept, sig);
+    else walk_lanes<1, 2>(tape, n, (int)mm, mmb, keep, ok_w, lane, kept, sig);
+    __syncwarp();
+    // the items whose tape is shorter, in lane order, while the scratch holds them
+    const bool want = ((cand >> lane) & 1u) && kept[0] < n;
+    const uint32_t mine = want ? kept[0] : 0u;
+    uint32_t incl = mine;
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if ((int)lane >= o) incl += v;
+    }
+    const bool fits = want && incl <= item_cap;
+    const uint32_t wmask = __ballot_sync(0xFFFFFFFFu, fits);
+    const uint32_t my_off = incl - mine;
+    if (fits) plan = 1u | my_off << 2 | mine << 17;
+    if (!wmask) return plan;
+    // copy: chunk-outer, one ballot + one coalesced store per item tape that
+    // keeps some instruction of the chunk; a MIN/MAX decided for the item
+    // becomes a COPY of the chosen operand (shorten.comp:148-186)
+    uint32_t run = 0, mm_run = 0;
+    for (uint32_t b = 0; b < n; b += 32) {
+        const uint32_t idx = b + lane;
+        const bool v = idx < n;
+        const uint64_t w = v ? __ldcg(&tape[idx]) : 0ull;
+        const uint32_t km = v ? keep[idx] : 0u;
+        const bool ism = v && is_mm(w_op(w));
+        const uint32_t mball = __ballot_sync(0xFFFFFFFFu, ism);
+        const uint2 cb = ism ? mmb[mm_run + __popc(mball & lanemask_lt())] : make_uint2(0u, 0u);
+        uint32_t pending = wmask & __reduce_or_sync(0xFFFFFFFFu, km);
+        while (pending) {
+            const int sel = __ffs(pending) - 1;
+            pending &= pending - 1;
+            const bool kb = (km >> sel) & 1u;
+            uint64_t wo = w;
+            if (kb && ism) {
+                const uint32_t c = ((cb.x >> sel) & 1u) | (((cb.y >> sel) & 1u) << 1);
+                if (c == MM_FIRST) wo = (w & ~0xFFull) | OP_COPY;
+                else if (c == MM_SECOND) wo = (w & ~0xFFull & ~(0xFFFFull << 32)) | OP_COPY | ((uint64_t)w_b(w) << 32);
+            }
+            const uint32_t kball = __ballot_sync(0xFFFFFFFFu, kb);
+            const uint32_t dst = __shfl_sync(0xFFFFFFFFu, my_off, sel);
+            const uint32_t rr = __shfl_sync(0xFFFFFFFFu, run, sel);
+            if (kb) items[dst + rr + __popc(kball & lanemask_lt())] = wo;
+            if ((int)lane == sel) run += __popc(kball);
+        }
+        mm_run += __popc(mball);
+    }
+    __syncwarp();
+    return plan;
+}
+
 // ---- interval level pass -------------------------------------------------------
 //
 // A work item is KI whole mask words of a node (32 * KI cells); lane l
@@ -523,6 +676,15 @@ interval_level_kernel(LevelLaunch p) {
         stat_work = 0;
     };
 
+    // item pruning: the prepared group of items (one node, lanes = items)
+    uint64_t* items = nullptr;
+    if constexpr (ROUND < 2)
+        if (p.item_cap && L > 0) items = reinterpret_cast<uint64_t*>(keep + p.item_ofs);
+    // (the items pg_first .. pg_first + pg_g - 1, consecutive in this warp's
+    // fetches; this lane's plan is item pg_first + lane's)
+    unsigned long long pg_first = 0;
+    uint32_t pg_g = 0, p_plan = 0;
+
     unsigned long long first;
     uint32_t got;
     while ((got = fetch_items(p.cursor, total, chunk, &first)) != 0) {
@@ -547,8 +709,40 @@ interval_level_kernel(LevelLaunch p) {
             const uint32_t tape_idx = rec[0];
             const uint32_t ncx = rec[1], ncy = rec[2], ncz = rec[3];
             const uint64_t* tape = T.tapes + tape_idx + 1;
-            const uint32_t n = (uint32_t)__ldcg(&T.tapes[tape_idx]);
+            const uint32_t n_node = (uint32_t)__ldcg(&T.tapes[tape_idx]);
+            uint32_t n = n_node;  // length of the tape the cells run (the item's, when pruned)
             const float cs = T.cs;
+
+            if constexpr (ROUND < 2) {
+                if (items && 32u * KI < dim * dim * dim) {
+                    if (item - pg_first >= pg_g) {
+                        // the rest of this node's items in the fetched chunk, up to 32
+                        const uint32_t g = min(min(32u, groups - grp), got - it);
+                        p_plan = prepare_items<ROUND, KI>(
+                            tape, n_node, ItemNode{dim, T.dim_sh, ncx, ncy, ncz, cs, T.lx, T.ly, T.lz, T.tt}, grp, g,
+                            lane_base, stage, keep, mmb, items, p.mm_cap, p.n_slots, p.item_cap);
+                        pg_first = item;
+                        pg_g = g;
+                    }
+                    const uint32_t plan = __shfl_sync(0xFFFFFFFFu, p_plan, (int)(item - pg_first));
+                    const uint32_t mode = plan & 3u;
+                    if (mode == 1) {
+                        tape = items + ((plan >> 2) & 0x7FFFu);
+                        n = plan >> 17;
+                    } else if (mode >= 2) {  // every cell empty (2) or a leaf (3): no evaluation
+#pragma unroll
+                        for (int h = 0; h < KI; h++) {
+                            rec[4 + 2 * words + grp * 32 * KI + h * 32 + lane] = 0xFFFFFFFFu;
+                            if (lane == 0) {
+                                rec[4 + grp * KI + h] = mode == 3 ? 0xFFFFFFFFu : 0u;
+                                rec[4 + words + grp * KI + h] = 0u;
+                            }
+                        }
+                        stat_work += 32ull * KI * n_node;
+                        continue;
+                    }
+                }
+            }
 
             uint32_t cell[KI], gx[KI], gy[KI], gz[KI];
             IVK<KI> bx, by, bz, bt;
@@ -649,7 +843,8 @@ interval_level_kernel(LevelLaunch p) {
             }
             }
             __syncwarp();
-            stat_work += 32ull * KI * n;
+            // the reference's work: every cell evaluates its node's tape
+            stat_work += 32ull * KI * n_node;
 
             // ---- classification (voxelizer/main.comp:88-108) ----
             const IVK<KI> res = lds_iv<KI>(lane_base);
@@ -690,7 +885,7 @@ interval_level_kernel(LevelLaunch p) {
 #pragma unroll
             for (int h = 0; h < KI; h++) {
                 child_tape[h] = tape_idx;
-                child_len[h] = n;
+                child_len[h] = n_node;
             }
             if (any_ok && T.shorten) {
                 // ---- backward liveness (shorten.comp:148-186) ----
@@ -814,7 +1009,8 @@ interval_level_kernel(LevelLaunch p) {
                 uint32_t leader[KI], lead_w[KI], group[KI];
 #pragma unroll
                 for (int h = 0; h < KI; h++) {
-                    do_short[h] = ok[h] && kept[h] < n;  // "not shorter -> reuse" (:188-191)
+                    // "not shorter -> reuse" (:188-191), against the node's tape
+                    do_short[h] = ok[h] && kept[h] < n_node;
                     const unsigned long long key = do_short[h] && T.share
                                                        ? ((unsigned long long)sig[h] << 32 | kept[h]) * 2ull + 1ull
                                                        : 2ull * (lane + 1);
