@@ -479,11 +479,12 @@ __device__ __forceinline__ void walk_lanes(const uint64_t* tape, uint32_t n, int
 //
 // Up to 32 consecutive items of one node are prepared together, one per lane
 // (the same forward pass and backward walk as cells, one box per lane); each
-// item's tape goes to the warp's item scratch while it fits. Returns per lane
-// (one item) a packed plan: bits 0-1 the mode, 0 = run the node's tape, 1 =
-// run the item tape, 2 = every cell empty, 3 = every cell a leaf; bits 2-16
-// the item tape's offset in the scratch, bits 17-31 its length (both below
-// 2^15: the scratch holds at most kItemTapeWords < 2^15 words).
+// item's tape goes to the warp's item scratch, on a 16-word boundary, while
+// it fits. Returns per lane (one item) a packed plan: bits 0-1 the mode, 0 =
+// run the node's tape, 1 = run the item tape, 2 = every cell empty, 3 = every
+// cell a leaf; bits 2-16 the item tape's offset in the scratch / 16, bits
+// 17-31 its length (item tapes of 2^15 words or more are not stored; the
+// scratch holds at most kItemTapeWords <= 2^19 words).
 struct ItemNode {  // the node of a group of items, and its tree's frame
     uint32_t dim, dim_sh, ncx, ncy, ncz;
     float cs, lx, ly, lz, tt;
@@ -568,8 +569,8 @@ __device__ __noinline__ uint32_t prepare_items(const uint64_t* tape, uint32_t n,
     else walk_lanes<1, 2>(tape, n, (int)mm, mmb, keep, ok_w, lane, kept, sig);
     __syncwarp();
     // the items whose tape is shorter, in lane order, while the scratch holds them
-    const bool want = ((cand >> lane) & 1u) && kept[0] < n;
-    const uint32_t mine = want ? kept[0] : 0u;
+    const bool want = ((cand >> lane) & 1u) && kept[0] < n && kept[0] < 32768u;
+    const uint32_t mine = want ? (kept[0] + 15u) & ~15u : 0u;
     uint32_t incl = mine;
     for (int o = 1; o < 32; o <<= 1) {
         const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
@@ -578,7 +579,7 @@ __device__ __noinline__ uint32_t prepare_items(const uint64_t* tape, uint32_t n,
     const bool fits = want && incl <= item_cap;
     const uint32_t wmask = __ballot_sync(0xFFFFFFFFu, fits);
     const uint32_t my_off = incl - mine;
-    if (fits) plan = 1u | my_off << 2 | mine << 17;
+    if (fits) plan = 1u | (my_off >> 4) << 2 | kept[0] << 17;
     if (!wmask) return plan;
     // copy: chunk-outer, one ballot + one coalesced store per item tape that
     // keeps some instruction of the chunk; a MIN/MAX decided for the item
@@ -727,7 +728,7 @@ interval_level_kernel(LevelLaunch p) {
                     const uint32_t plan = __shfl_sync(0xFFFFFFFFu, p_plan, (int)(item - pg_first));
                     const uint32_t mode = plan & 3u;
                     if (mode == 1) {
-                        tape = items + ((plan >> 2) & 0x7FFFu);
+                        tape = items + ((plan >> 2) & 0x7FFFu) * 16u;
                         n = plan >> 17;
                     } else if (mode >= 2) {  // every cell empty (2) or a leaf (3): no evaluation
 #pragma unroll

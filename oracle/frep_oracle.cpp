@@ -294,7 +294,7 @@ Iv eval_hybrid(const uint64_t* tape, uint32_t n, std::vector<Iv>& slots, std::ve
 // [t, t]; MIN/MAX record FIRST/SECOND/BOTH with strict comparisons.
 // rounding 2 = the hybrid affine mode (eval_hybrid).
 Iv eval_interval(const uint64_t* tape, uint32_t n, std::vector<Iv>& slots, const float* lo3,
-                 const float* hi3, float t, int rounding, uint8_t* choices) {
+                 const float* hi3, float t, int rounding, uint8_t* choices, Iv* trace = nullptr) {
     if (rounding == 2) {
         std::vector<Af> forms(slots.size());
         return eval_hybrid(tape, n, slots, forms, lo3, hi3, t, choices);
@@ -312,6 +312,7 @@ Iv eval_interval(const uint64_t* tape, uint32_t n, std::vector<Iv>& slots, const
         const Iv a = op == OP_CONST ? Iv{0, 0} : slots[i_a(w)];
         const Iv b = op == OP_CONST ? Iv{0, 0} : slots[i_b(w)];
         slots[i_out(w)] = interval_op(op, w, a, b, rounding);
+        if (trace) trace[i] = slots[i_out(w)];
         if (op == OP_MIN) {
             const uint8_t c = a.hi < b.lo ? MM_FIRST : (b.hi < a.lo ? MM_SECOND : MM_BOTH);
             if (choices) choices[mm] = c;
@@ -591,6 +592,13 @@ void oracle_eval_interval(const uint64_t* tape, uint32_t n_instr, uint32_t n_slo
     Iv r = eval_interval(tape, n_instr, slots, lo3, hi3, t, rounding, choices);
     out_lohi[0] = r.lo;
     out_lohi[1] = r.hi;
+}
+
+void oracle_eval_interval_trace(const uint64_t* tape, uint32_t n_instr, uint32_t n_slots,
+                                const float* lo3, const float* hi3, float t, int rounding,
+                                float* trace) {
+    std::vector<Iv> slots(std::max<uint32_t>(n_slots, 4));
+    eval_interval(tape, n_instr, slots, lo3, hi3, t, rounding, nullptr, reinterpret_cast<Iv*>(trace));
 }
 
 float oracle_eval_point(const uint64_t* tape, uint32_t n_instr, uint32_t n_slots, float x,

@@ -38,6 +38,11 @@ extern "C" {
 void oracle_eval_interval(const uint64_t* tape, uint32_t n_instr, uint32_t n_slots,
                           const float* lo3, const float* hi3, float t, int rounding,
                           float* out_lohi, uint8_t* choices);
+// Every instruction's result interval (trace: 2 floats per instruction;
+// rounding 0 or 1), for tests of properties of the intermediate values.
+void oracle_eval_interval_trace(const uint64_t* tape, uint32_t n_instr, uint32_t n_slots,
+                                const float* lo3, const float* hi3, float t, int rounding,
+                                float* trace);
 float oracle_eval_point(const uint64_t* tape, uint32_t n_instr, uint32_t n_slots, float x,
                         float y, float z, float t);
 void oracle_eval_gradient(const uint64_t* tape, uint32_t n_instr, uint32_t n_slots, float x,

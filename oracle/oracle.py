@@ -45,6 +45,7 @@ def oracle_lib() -> C.CDLL:
             build()
         lib = C.CDLL(str(ORACLE_LIB))
         lib.oracle_eval_interval.argtypes = [_P, C.c_uint32, C.c_uint32, _P, _P, C.c_float, C.c_int, _P, _P]
+        lib.oracle_eval_interval_trace.argtypes = [_P, C.c_uint32, C.c_uint32, _P, _P, C.c_float, C.c_int, _P]
         lib.oracle_eval_point.argtypes = [_P, C.c_uint32, C.c_uint32, C.c_float, C.c_float, C.c_float, C.c_float]
         lib.oracle_eval_point.restype = C.c_float
         lib.oracle_eval_gradient.argtypes = [_P, C.c_uint32, C.c_uint32, C.c_float, C.c_float, C.c_float,
@@ -172,6 +173,16 @@ def eval_interval(wide, n_slots, lo, hi, t=0.0, rounding=0):
     ch = np.zeros(max(n_mm, 1), np.uint8)
     oracle_lib().oracle_eval_interval(_p(wide), len(wide), n_slots, _p(lo), _p(hi), t, rounding, _p(out), _p(ch))
     return out, ch[:n_mm]
+
+
+def eval_interval_trace(wide, n_slots, lo, hi, t=0.0, rounding=0) -> np.ndarray:
+    """Every instruction's result interval, (n, 2) float32."""
+    wide = np.ascontiguousarray(wide, np.uint64)
+    lo = np.ascontiguousarray(lo, np.float32)
+    hi = np.ascontiguousarray(hi, np.float32)
+    out = np.zeros((len(wide), 2), np.float32)
+    oracle_lib().oracle_eval_interval_trace(_p(wide), len(wide), n_slots, _p(lo), _p(hi), t, rounding, _p(out))
+    return out
 
 
 def eval_point(wide, n_slots, x, y, z, t=0.0) -> float:
