@@ -11,6 +11,10 @@ the whole batch voxelized and rendered (one frep_batch_run, CUDA graph
 replay). The same trees are also run as 512 sequential plain launches
 (frep_voxelize + frep_render per scene) for the batched/plain ratio.
 
+`--workload small`: the min-union of 16 spheres on a {16, 4} = 64^3 tree over
+[-1.5, 1.5]^3, 256x256 orthographic, one ray per pixel; one step = one
+voxelization + one frame.
+
 `--workload large`: one scene of 256 primitives on a {16, 16, 8} = 2048^3
 tree, 1920x1080 perspective + shadow rays; one step = one voxelization + one
 frame.
@@ -52,7 +56,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=("batch", "large", "stress", "animated"), default="batch")
+    ap.add_argument("--workload", choices=("batch", "small", "large", "stress", "animated"), default="batch")
     ap.add_argument("--frames", type=int, default=30, help="stress: animation frames (T = frame / frames)")
     ap.add_argument("--no-reuse", action="store_true",
                     help="animated: re-voxelize every frame in full (no reuse of the previous frame's tree)")
@@ -85,10 +89,10 @@ def parse():
                     help="large: skip the compact-tree measurements (compaction time, bytes, render time)")
     args = ap.parse_args()
     if args.grid is None:
-        args.grid = "16,16,4,4" if args.workload == "stress" else "16,16,8"
+        args.grid = {"stress": "16,16,4,4", "small": "16,4"}.get(args.workload, "16,16,8")
     args.grid_dims = tuple(int(v) for v in args.grid.split(","))
     if args.res is None:
-        args.res = "512x512" if args.workload == "batch" else "1920x1080"
+        args.res = {"batch": "512x512", "small": "256x256"}.get(args.workload, "1920x1080")
     args.width, args.height = (int(v) for v in args.res.lower().split("x"))
     fine = 1
     for d in args.grid_dims:
@@ -98,6 +102,8 @@ def parse():
     elif args.workload == "stress":
         args.workload_name = (f"stress_twisted_gyroid_64spheres_{fine}cube_{args.width}x{args.height}_shadow_"
                               f"{args.frames}frames")
+    elif args.workload == "small":
+        args.workload_name = f"spheres16_union_{fine}cube_{args.width}x{args.height}_ortho"
     elif args.workload == "animated":
         args.workload_name = (f"animated_csg_256prim_4orbiting_{fine}cube_{args.width}x{args.height}_shadow_"
                               f"60fps_{'full' if args.no_reuse else 'reuse'}")
@@ -216,6 +222,11 @@ def make_scene(args, grid_dims=None):
         return scenes.stress_gyroid(grid_dims=dims, width=args.width, height=args.height)
     if args.workload == "animated":
         return scenes.animated_csg(256, 4, seed=2, grid_dims=dims, width=args.width, height=args.height)
+    if args.workload == "small":
+        # min-union of 16 spheres over [-1.5, 1.5]^3, orthographic view down +z
+        sc = scenes.spheres_union(16, width=args.width, height=args.height)
+        sc.grid_dims = list(dims)
+        return sc
     return scenes.random_csg(256, seed=2, grid_dims=dims, width=args.width, height=args.height, shadows=True)
 
 
@@ -269,7 +280,7 @@ def run_reference(args, world, rank):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "impl": "reference",
         "config": {"workload": args.workload_name, "grid": list(args.grid_dims), "resolution": [args.width, args.height],
-                   "shadow_rays": 1, "rounding": "outward"},
+                   "shadow_rays": 1 if scene.shadow_mask else 0, "rounding": "outward"},
         "cpu_baseline": {"value": value, "unit": "scenes/s", "cores": threads, "kind": "port",
                          "sample": f"{args.steps} scenes on grid {list(sample_dims)} (voxelize + "
                                    f"{args.width}x{args.height} render), oracle C++ port, {threads} threads"},
@@ -432,7 +443,8 @@ def run_ours(args, world, rank, local):
         "metric": METRIC, "value": value, "unit": "scenes/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": args.workload_name, "grid": scene.grid_dims, "resolution": [W, H], "shadow_rays": 1,
+        "config": {"workload": args.workload_name, "grid": scene.grid_dims, "resolution": [W, H],
+                   "shadow_rays": 1 if scene.shadow_mask else 0,
                    "tape_instructions": vs.tape.n_instr, "rounding": "outward", "point_cells_per_lane": args.point_k or "default",
                    "nodes_per_level": list(info.node_count[:vs.grid_levels]),
                    "l2": "flushed between timed steps (256 MB write, outside the step events)",

@@ -502,10 +502,25 @@ frep_status voxelize_impl(frep_ctx* ctx, frep_tree* tree, const frep_tree* prev,
 
     frep_status pst = ensure_plan(tree, tape, "frep_voxelize");
     if (pst != FREP_OK) return pst;
-    // Per-warp scratch: a keep mask per instruction, a choice-mask pair per MIN/MAX.
-    const frep::WarpScratch ws = frep::warp_scratch(n, tape->ct.n_minmax, (uint32_t)tree->plan.interval_ki,
-                                                    tree->opts.rounding != FREP_ROUND_HYBRID);
-    const uint64_t keep_words = (uint64_t)tree->plan.blocks * tree->plan.warps_per_block * ws.stride;
+    // Per-warp scratch: a keep mask per instruction, a choice-mask pair per
+    // MIN/MAX, and room for item tapes (item-level pruning) when that room is
+    // at most a quarter of the tree's own pools and the context's budget
+    // holds it; else the passes run without item pruning (the same trees).
+    // Each tree keeps its scratch between voxelizations, so the bound keeps
+    // many small resident trees from each holding item room.
+    const uint64_t warps = (uint64_t)tree->plan.blocks * tree->plan.warps_per_block;
+    frep::WarpScratch ws = frep::warp_scratch(n, tape->ct.n_minmax, (uint32_t)tree->plan.interval_ki,
+                                              tree->opts.rounding != FREP_ROUND_HYBRID);
+    if (ws.item_cap) {
+        const uint64_t item_bytes = warps * ws.item_cap * 8;
+        const uint64_t pool_bytes = tree->node_cap * 4 + tree->tape_cap * 8;
+        const bool fits = warps * ws.stride <= tree->keep_words ||
+                          ctx->used - std::min<uint64_t>(ctx->used, tree->keep_words * 4) + warps * ws.stride * 4 <=
+                              ctx->budget;
+        if (item_bytes * 4 > pool_bytes || !fits)
+            ws = frep::warp_scratch(n, tape->ct.n_minmax, (uint32_t)tree->plan.interval_ki, false);
+    }
+    const uint64_t keep_words = warps * ws.stride;
     if (keep_words > tree->keep_words) {
         if (tree->keep) {
             cudaStreamSynchronize(tree->stream);

@@ -44,11 +44,12 @@ struct WarpScratch {
     uint32_t item_ofs;  // where the item tapes start
     uint32_t item_cap;  // u64 words of item tapes (0 = no item pruning)
 };
-// At most this many u64 words of item tapes per warp (1 MB; a multiple of 16
-// and at most 2^19, so that an item tape's offset / 16 packs into 15 bits): a
-// group of up to 32 items of one node stores the pruned tapes that fit, the
-// others run on the node's tape.
-constexpr uint32_t kItemTapeWords = 131072;
+// At most this many u64 words of item tapes per warp (256 KB; a multiple of
+// 16 and at most 2^19, so that an item tape's offset / 16 packs into 15
+// bits): a group of up to 32 items of one node stores the pruned tapes that
+// fit, the others run on the node's tape. (On the 128-scene batch, 1 MB per
+// warp executed exactly the same instructions.)
+constexpr uint32_t kItemTapeWords = 32768;
 // ki: cells per lane of the interval pass (a keep mask and a choice-mask pair
 // per group of 32 cells). items: room for item tapes.
 inline WarpScratch warp_scratch(uint32_t longest, uint32_t mm_cap, uint32_t ki, bool items = false) {
