@@ -557,6 +557,16 @@ def cpu_sample_order(n: int):
     return [int(i) for i in np.random.default_rng(17).permutation(n)]
 
 
+# DRAM bytes (read + write) per launch of each (level, kind) level pass of the
+# default workload (512 scenes at 512x512, the committed tuning table), kinds
+# 0 interval, 1 point 4 cells/lane, 2 point 2 cells/lane: one ncu capture of
+# dram__bytes_read.sum + dram__bytes_write.sum (one pass per launch) of
+#   python bench.py --steps 2 --warmup 3 --no-cpu-baseline --serve-seconds 0 --serve-sweep '' --plain-steps 1
+# summarised in profiles/batch_512scenes_dram_per_launch.txt.
+NCU_DRAM_BYTES_512 = {(0, 0): 7.833e9, (1, 0): 23.989e9, (1, 1): 1.222e9, (1, 2): 0.509e9,
+                      (2, 1): 0.377e9, (2, 2): 13.085e9}
+
+
 def tuning_table():
     """The committed tuning of the batch workload (frep.autotune.DEFAULT_TABLE),
     None when absent."""
@@ -884,9 +894,15 @@ def run_ours_batch(args, world, rank, local):
     achieved = float(ops[dom]) / (dom_ms / 1e3) / 1e12
     kind_name = ["interval_level_kernel", "point_level_kernel (4 cells/lane)", "point_level_kernel (2 cells/lane)"]
     total_ops = float(ops.sum())
+    default_workload = (n == 512 and (W, H) == (512, 512) and not args.tune_cache and not args.retune
+                        and tuning_table() is not None)
+    traffic = NCU_DRAM_BYTES_512.get((int(dom[0]), int(dom[1]))) if default_workload else None
     roofline = {
         "bound": "fp32", "kernel": kind_name[dom[1]], "level": int(dom[0]), "achieved": achieved,
-        "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": None,
+        "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": traffic,
+        "traffic_unit": "bytes per launch",
+        "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of this launch kind on this workload "
+                           "(profiles/batch_512scenes_dram_per_launch.txt)") if traffic else None,
         "peak_source": "nominal FP32 issue: 148 SMs x 128 lanes x MEASURED_PEAKS.json sm_max_mhz "
                        "(the file holds no FP32 figure)",
         "algorithmic_ops_per_launch": float(ops[dom]), "cell_instr_per_launch": float(cinstr[dom]),

@@ -478,7 +478,8 @@ __device__ __forceinline__ void walk_lanes(const uint64_t* tape, uint32_t n, int
 // empty or a leaf without evaluating them.
 //
 // Up to 32 consecutive items of one node are prepared together, one per lane
-// (the same forward pass and backward walk as cells, one box per lane); each
+// (the same forward pass and backward walk as cells, one box per lane, in the
+// first 256 bytes of each slot row: lane_base = row base + 8 * lane); each
 // item's tape goes to the warp's item scratch, on a 16-word boundary, while
 // it fits. Returns per lane (one item) a packed plan: bits 0-1 the mode, 0 =
 // run the node's tape, 1 = run the item tape, 2 = every cell empty, 3 = every
@@ -721,7 +722,8 @@ interval_level_kernel(LevelLaunch p) {
                         const uint32_t g = min(min(32u, groups - grp), got - it);
                         p_plan = prepare_items<ROUND, KI>(
                             tape, n_node, ItemNode{dim, T.dim_sh, ncx, ncy, ncz, cs, T.lx, T.ly, T.lz, T.tt}, grp, g,
-                            lane_base, stage, keep, mmb, items, p.mm_cap, p.n_slots, p.item_cap);
+                            smem_addr(wbase) + lane * 8u, stage, keep, mmb, items, p.mm_cap, p.n_slots,
+                            p.item_cap);
                         pg_first = item;
                         pg_g = g;
                     }
