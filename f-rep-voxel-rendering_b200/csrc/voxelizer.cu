@@ -1300,6 +1300,9 @@ __device__ __forceinline__ void pt_exec(const uint4 d, FK<K>& r, uint32_t lane_b
     }
 }
 
+// (inside namespace frep::dev: the generated loop uses FK<K>)
+#include "point_dispatch.cuh"
+
 template <int WARPS, int K>
 __global__ void __launch_bounds__(WARPS * 32)
 point_level_kernel(LevelLaunch p) {
@@ -1378,8 +1381,34 @@ point_level_kernel(LevelLaunch p) {
                     prefetch_chunk(pre, tape, base + STAGE, n, lane);
                     __syncwarp();
                 }
-                // The decode word of j+1 is read one instruction early.
                 const uint32_t sbase = smem_addr(stage);
+                if constexpr (K == 2 || K == 4) {
+                    // the jump-table loop (point_dispatch.cuh); SIN / COS / EXP here
+                    uint32_t j = 0;
+                    while (true) {
+                        PtRun<K> run;
+                        if constexpr (K == 2) run = pt_run_2(sbase, j, m, lane_base, r);
+                        else run = pt_run_4(sbase, j, m, lane_base, r);
+                        j = run.j;
+                        r = run.r;
+                        if (j >= m) break;
+                        const uint4 d = lds_u4(sbase + j * 16);
+                        switch (d.x) {
+#define FREP_PT_CASE(OPC, FA, FB)                         \
+    case OPC | (FA ? F_FWD_A : 0u) | (FB ? F_FWD_B : 0u): \
+        pt_exec<K, OPC, FA, FB>(d, r, lane_base);         \
+        break;
+                            FREP_CASES_UNARY(FREP_PT_CASE, OP_SIN)
+                            FREP_CASES_UNARY(FREP_PT_CASE, OP_COS)
+                            FREP_CASES_UNARY(FREP_PT_CASE, OP_EXP)
+#undef FREP_PT_CASE
+                            default: break;
+                        }
+                        sts_k<K>(lane_base + d.w, r);
+                        j++;
+                    }
+                } else {
+                // The decode word of j+1 is read one instruction early.
                 uint4 dn = lds_u4(sbase);
                 for (uint32_t j = 0; j < m; j++) {
                     const uint4 d = dn;
@@ -1398,6 +1427,7 @@ point_level_kernel(LevelLaunch p) {
                         default: break;
                     }
                     sts_k<K>(lane_base + d.w, r);
+                }
                 }
             }
             staged_tape = n <= STAGE ? tape_idx : 0xFFFFFFFFu;
