@@ -1,5 +1,6 @@
 """Writes point_dispatch.cuh: the point interpreter's inner loop as inline PTX
-with a jump table (brx.idx), for 2 and 4 cells per lane.
+with a jump table (brx.idx), for 2, 4 and 8 cells per lane (8: a slot row is
+two 16-byte halves 512 bytes apart, as lds_k / sts_k lay it out).
 
 The loop in C++ is a switch over (opcode, forward-A, forward-B); the compiler
 lowers it to a tree of compares and branches (about six per tape instruction).
@@ -44,10 +45,20 @@ def body(op, k, a, b):
     raise ValueError(op)
 
 
+K8_HALF = 32 * 16  # bytes between the two halves of an 8-cell slot row
+
+
 def gen(K):
-    vec = f".v{K}" if K > 1 else ""
     regs = lambda p: ", ".join(f"%%{p}{i}" for i in range(K))
-    ld = lambda p, off: [f"add.u32 %%ad, %%lb, {off};", f"ld.shared{vec}.f32 {{{regs(p)}}}, [%%ad];"]
+
+    def half(p, h):
+        return ", ".join(f"%%{p}{i}" for i in range(4 * h, 4 * h + 4))
+
+    def ld(p, off):
+        if K == 8:
+            return [f"add.u32 %%ad, %%lb, {off};", f"ld.shared.v4.f32 {{{half(p, 0)}}}, [%%ad];",
+                    f"ld.shared.v4.f32 {{{half(p, 1)}}}, [%%ad+{K8_HALF}];"]
+        return [f"add.u32 %%ad, %%lb, {off};", f"ld.shared.v{K}.f32 {{{regs(p)}}}, [%%ad];"]
     lines = []
     lines.append("{")
     lines.append(".reg .pred %%p, %%done;")
@@ -106,7 +117,11 @@ def gen(K):
             lines.append("bra.uni $FRP_STORE;")
     lines.append("$FRP_STORE:")
     lines.append("add.u32 %%ad, %%lb, %%w;")
-    lines.append(f"st.shared{vec}.f32 [%%ad], {{{regs('q')}}};")
+    if K == 8:
+        lines.append(f"st.shared.v4.f32 [%%ad], {{{half('q', 0)}}};")
+        lines.append(f"st.shared.v4.f32 [%%ad+{K8_HALF}], {{{half('q', 1)}}};")
+    else:
+        lines.append(f"st.shared.v{K}.f32 [%%ad], {{{regs('q')}}};")
     lines.append("add.u32 %%j, %%j, 1;")
     lines.append("bra.uni $FRP_LOOP;")
     lines.append("$FRP_EXIT:")
@@ -150,7 +165,7 @@ struct PtRun {
 };
 
 '''
-    return head + emit(2) + "\n" + emit(4)
+    return head + emit(2) + "\n" + emit(4) + "\n" + emit(8)
 
 
 def main():

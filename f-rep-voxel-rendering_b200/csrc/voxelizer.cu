@@ -1382,13 +1382,14 @@ point_level_kernel(LevelLaunch p) {
                     __syncwarp();
                 }
                 const uint32_t sbase = smem_addr(stage);
-                if constexpr (K == 2 || K == 4) {
+                if constexpr (K == 2 || K == 4 || K == 8) {
                     // the jump-table loop (point_dispatch.cuh); SIN / COS / EXP here
                     uint32_t j = 0;
                     while (true) {
                         PtRun<K> run;
                         if constexpr (K == 2) run = pt_run_2(sbase, j, m, lane_base, r);
-                        else run = pt_run_4(sbase, j, m, lane_base, r);
+                        else if constexpr (K == 4) run = pt_run_4(sbase, j, m, lane_base, r);
+                        else run = pt_run_8(sbase, j, m, lane_base, r);
                         j = run.j;
                         r = run.r;
                         if (j >= m) break;

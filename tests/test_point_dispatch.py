@@ -25,7 +25,7 @@ def test_header_is_the_generator_output():
 
 def test_case_table():
     g = _gen()
-    for k in (2, 4):
+    for k in (2, 4, 8):
         lines = g.gen(k)
         tab = next(l for l in lines if ".branchtargets" in l)
         targets = tab.split(".branchtargets", 1)[1].strip(" ;").split(", ")
