@@ -62,7 +62,7 @@ def gen(K):
     lines = []
     lines.append("{")
     lines.append(".reg .pred %%p, %%done;")
-    lines.append(".reg .b32 %%j, %%m, %%sb, %%lb, %%ad, %%x, %%y, %%z, %%w;")
+    lines.append(".reg .b32 %%j, %%m, %%sb, %%lb, %%ad, %%da, %%x, %%y, %%z, %%w, %%nx, %%ny, %%nz, %%nw;")
     lines.append(f".reg .f32 {regs('q')}, {regs('a')}, {regs('b')};")
     # operands: %0 = j (in/out), %1..%K = r (in/out), then sbase, m, lane_base
     lines.append("mov.b32 %%j, %0;")
@@ -71,11 +71,14 @@ def gen(K):
     lines.append(f"mov.b32 %%sb, %{K + 1};")
     lines.append(f"mov.b32 %%m, %{K + 2};")
     lines.append(f"mov.b32 %%lb, %{K + 3};")
+    # decode word j, then each iteration loads word j + 1 before dispatching j
+    # (word m, one past the chunk, is in the staging area: it holds STAGE + 1)
+    lines.append("mad.lo.u32 %%da, %%j, 16, %%sb;")
+    lines.append("ld.shared.v4.u32 {%%x, %%y, %%z, %%w}, [%%da];")
     lines.append("$FRP_LOOP:")
     lines.append("setp.ge.u32 %%done, %%j, %%m;")
     lines.append("@%%done bra.uni $FRP_EXIT;")
-    lines.append("mad.lo.u32 %%ad, %%j, 16, %%sb;")
-    lines.append("ld.shared.v4.u32 {%%x, %%y, %%z, %%w}, [%%ad];")
+    lines.append("ld.shared.v4.u32 {%%nx, %%ny, %%nz, %%nw}, [%%da+16];")
     lines.append("and.b32 %%x, %%x, 63;")
     targets = []
     for idx in range(64):
@@ -123,6 +126,8 @@ def gen(K):
     else:
         lines.append(f"st.shared.v{K}.f32 [%%ad], {{{regs('q')}}};")
     lines.append("add.u32 %%j, %%j, 1;")
+    lines.append("add.u32 %%da, %%da, 16;")
+    lines += ["mov.b32 %%x, %%nx;", "mov.b32 %%y, %%ny;", "mov.b32 %%z, %%nz;", "mov.b32 %%w, %%nw;"]
     lines.append("bra.uni $FRP_LOOP;")
     lines.append("$FRP_EXIT:")
     lines.append("mov.b32 %0, %%j;")

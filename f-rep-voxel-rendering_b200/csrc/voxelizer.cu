@@ -462,6 +462,9 @@ __device__ __forceinline__ void walk_lanes(const uint64_t* tape, uint32_t n, int
     }
 }
 
+// The forward loop's common opcodes as inline PTX with a jump table.
+#include "interval_dispatch.cuh"
+
 // ---- item-level pruning (this library's addition) ----------------------------------
 //
 // Before the cells of a work item are evaluated, the node's tape is evaluated
@@ -822,26 +825,45 @@ interval_level_kernel(LevelLaunch p) {
             sts_iv<KI>(lane_base + 3 * 32 * ROWB, bt);
 
             // ---- forward interval pass (interval.comp:121-160) ----
+            // With two cells per lane the jump-table loop (interval_dispatch.cuh)
+            // runs every opcode but DIV / SIN / COS / EXP, which it hands back
+            // to iv_exec here.
             for (uint32_t base = 0; base < n; base += STAGE) {
                 const uint32_t m = min(STAGE, n - base);
                 __syncwarp();
                 stage_chunk<false>(stage, pre, ROWB, lane, m);
                 prefetch_chunk(pre, tape, base + STAGE, n, lane);
                 __syncwarp();
-                // The decode word of j+1 is read one instruction early.
                 const uint32_t sbase = smem_addr(stage);
-                uint4 dn = lds_u4(sbase);
-                for (uint32_t j = 0; j < m; j++) {
-                    const uint4 d = dn;
-                    dn = lds_u4(sbase + (j + 1) * 16);
-                    if (d.x == OP_CONST) {
-                        const float c = __uint_as_float(d.y);
-#pragma unroll
-                        for (int h = 0; h < KI; h++) r.v[h] = make_float2(c, c);
-                    } else {
+                if constexpr (KI == 2) {
+                    uint32_t j = 0;
+                    while (true) {
+                        IvRun run;
+                        if constexpr (ROUND == 0) run = iv_run_0_2(sbase, j, m, lane_base, mmb, mm, p.mm_cap);
+                        else run = iv_run_1_2(sbase, j, m, lane_base, mmb, mm, p.mm_cap);
+                        j = run.j;
+                        mm = run.mm;
+                        if (j >= m) break;
+                        const uint4 d = lds_u4(sbase + j * 16);
                         r = iv_exec<ROUND, KI>(d, lane_base, lane, mmb, mm, p.mm_cap);
+                        sts_iv<KI>(lane_base + d.w, r);
+                        j++;
                     }
-                    sts_iv<KI>(lane_base + d.w, r);
+                } else {
+                    // The decode word of j+1 is read one instruction early.
+                    uint4 dn = lds_u4(sbase);
+                    for (uint32_t j = 0; j < m; j++) {
+                        const uint4 d = dn;
+                        dn = lds_u4(sbase + (j + 1) * 16);
+                        if (d.x == OP_CONST) {
+                            const float c = __uint_as_float(d.y);
+#pragma unroll
+                            for (int h = 0; h < KI; h++) r.v[h] = make_float2(c, c);
+                        } else {
+                            r = iv_exec<ROUND, KI>(d, lane_base, lane, mmb, mm, p.mm_cap);
+                        }
+                        sts_iv<KI>(lane_base + d.w, r);
+                    }
                 }
             }
             }

@@ -44,3 +44,20 @@ def test_case_table():
         # every target is defined once
         for t in set(targets):
             assert sum(1 for l in lines if l == t + ":") == 1, t
+
+
+def test_interval_header_is_the_generator_output():
+    spec = importlib.util.spec_from_file_location("gen_interval_dispatch", CSRC / "gen_interval_dispatch.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    assert (CSRC / "interval_dispatch.cuh").read_text() == mod.text()
+    for rnd in (0, 1):
+        lines = mod.gen(rnd, 2)
+        tab = next(l for l in lines if ".branchtargets" in l)
+        targets = tab.split(".branchtargets", 1)[1].strip(" ;").split(", ")
+        assert len(targets) == 16
+        inline = {mod.OPS[n] for n in mod.INLINE}
+        for idx, t in enumerate(targets):
+            assert (t != "$FRI_EXIT") == (idx in inline), (idx, t)
+        for t in set(targets):
+            assert sum(1 for l in lines if l == t + ":") == 1, t
