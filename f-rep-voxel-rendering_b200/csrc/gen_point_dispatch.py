@@ -94,11 +94,27 @@ def gen(K):
             targets.append("$FRP_EXIT")
     lines.append("$FRP_TAB: .branchtargets " + ", ".join(targets) + ";")
     lines.append("brx.idx.uni %%x, $FRP_TAB;")
+
+    # Each case ends with the store of its result and the dispatch of the next
+    # instruction (a threaded loop: no jump back to a common loop head).
+    def store_next():
+        out = ["add.u32 %%ad, %%lb, %%w;"]
+        if K == 8:
+            out.append(f"st.shared.v4.f32 [%%ad], {{{half('q', 0)}}};")
+            out.append(f"st.shared.v4.f32 [%%ad+{K8_HALF}], {{{half('q', 1)}}};")
+        else:
+            out.append(f"st.shared.v{K}.f32 [%%ad], {{{regs('q')}}};")
+        out += ["add.u32 %%j, %%j, 1;", "add.u32 %%da, %%da, 16;",
+                "mov.b32 %%x, %%nx;", "mov.b32 %%y, %%ny;", "mov.b32 %%z, %%nz;", "mov.b32 %%w, %%nw;",
+                "setp.ge.u32 %%done, %%j, %%m;", "@%%done bra.uni $FRP_EXIT;",
+                "ld.shared.v4.u32 {%%nx, %%ny, %%nz, %%nw}, [%%da+16];",
+                "and.b32 %%x, %%x, 63;", "brx.idx.uni %%x, $FRP_TAB;"]
+        return out
     # CONST: the value's bits are the decode word's y
     lines.append("$FRP_CONST:")
     for i in range(K):
         lines.append(f"mov.b32 %%q{i}, %%y;")
-    lines.append("bra.uni $FRP_STORE;")
+    lines += store_next()
     for name in BINARY:
         for fa in (0, 1):
             for fb in (0, 1):
@@ -109,7 +125,7 @@ def gen(K):
                     lines += ld("b", "%%z")
                 for i in range(K):
                     lines += body(name, i, f"%%q{i}" if fa else f"%%a{i}", f"%%q{i}" if fb else f"%%b{i}")
-                lines.append("bra.uni $FRP_STORE;")
+                lines += store_next()
     for name in UNARY:
         for fa in (0, 1):
             lines.append(f"$FRP_{name}_{fa}0:")
@@ -117,18 +133,7 @@ def gen(K):
                 lines += ld("a", "%%y")
             for i in range(K):
                 lines += body(name, i, f"%%q{i}" if fa else f"%%a{i}", None)
-            lines.append("bra.uni $FRP_STORE;")
-    lines.append("$FRP_STORE:")
-    lines.append("add.u32 %%ad, %%lb, %%w;")
-    if K == 8:
-        lines.append(f"st.shared.v4.f32 [%%ad], {{{half('q', 0)}}};")
-        lines.append(f"st.shared.v4.f32 [%%ad+{K8_HALF}], {{{half('q', 1)}}};")
-    else:
-        lines.append(f"st.shared.v{K}.f32 [%%ad], {{{regs('q')}}};")
-    lines.append("add.u32 %%j, %%j, 1;")
-    lines.append("add.u32 %%da, %%da, 16;")
-    lines += ["mov.b32 %%x, %%nx;", "mov.b32 %%y, %%ny;", "mov.b32 %%z, %%nz;", "mov.b32 %%w, %%nw;"]
-    lines.append("bra.uni $FRP_LOOP;")
+            lines += store_next()
     lines.append("$FRP_EXIT:")
     lines.append("mov.b32 %0, %%j;")
     for i in range(K):
