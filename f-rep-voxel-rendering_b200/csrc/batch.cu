@@ -238,11 +238,12 @@ frep_status prepare_voxelize(frep_batch* b, const frep_tape* const* tapes, TapeS
     return r;
 }
 
-// Cells per lane of the level-0 interval pass: one. Level 0 runs every
-// tree's root tape, the longest, on one node per tree; its time is set by the
-// last warps to finish the longest items, and two cells per lane double
-// those (128 trees: 10.1 ms with one, 16.5 ms with two).
-int level0_cells(const frep_batch*) { return 1; }
+// Cells per lane of the level-0 interval pass: those of the other interval
+// passes (two where the plan's shared memory holds them). With two, the
+// passes run the jump-table loop (interval_dispatch.cuh); on a 128-scene
+// batch level 0 took 11.6 ms with two and 18.6 ms with one (with the earlier
+// C++ loop for both widths, two had been slower: 16.5 against 10.1 ms).
+int level0_cells(const frep_batch* b) { return b->plan4.interval_ki; }
 
 // Enqueues the voxelization of every tree of the set: root copy + header
 // reset, then for each level index one interval pass and up to two point

@@ -1,7 +1,7 @@
 """Writes interval_dispatch.cuh: the interval interpreter's forward loop as
 inline PTX with a jump table (brx.idx), for both roundings (0 nearest, 1
-outward) and 2 cells per lane (the passes below the root; with one cell per
-lane, the root level, the C++ loop measured faster).
+outward) and 2 cells per lane (with one cell per lane, a single tree's root
+level, the C++ loop measured faster).
 
 The C++ loop tests opcodes in frequency order (two to four compare-and-branch
 pairs per instruction); here one indexed branch dispatches each instruction.
