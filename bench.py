@@ -712,6 +712,8 @@ def serve_phase(args, ctx, scs, chosen, pools, warps):
         "failed": failed - before["failed"], "voxelized": st["voxelized"] - before["voxelized"],
         "rerendered": st["rerendered"] - before["rerendered"], "evictions": st["evictions"] - before["evictions"],
         "steps": st["steps"] - before["steps"], "max_submit_lag_ms": float(1e3 * lag.max()),
+        "max_plan_ms": st["max_plan_ms"], "max_enqueue_ms": st["max_enqueue_ms"],
+        "max_step_evictions": st["max_step_evictions"],
         "latency": "scheduled arrival -> image in pinned host memory (p50/p99_ms); server_*: submit -> image",
     }
 
@@ -973,7 +975,7 @@ def run_ours_batch(args, world, rank, local):
             r = serve_phase(a, ctx, scs, chosen, pools, tuner.warps)
             sweep.append({k: r[k] for k in ("rate_req_s", "p50_ms", "p99_ms", "max_ms", "scenes_per_s",
                                             "voxelized", "rerendered", "evictions", "failed",
-                                            "max_submit_lag_ms")})
+                                            "max_submit_lag_ms", "max_plan_ms", "max_enqueue_ms")})
         if sweep:
             line["serving_sweep"] = sweep
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

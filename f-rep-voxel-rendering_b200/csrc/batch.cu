@@ -243,7 +243,20 @@ frep_status prepare_voxelize(frep_batch* b, const frep_tape* const* tapes, TapeS
 // passes run the jump-table loop (interval_dispatch.cuh); on a 128-scene
 // batch level 0 took 11.6 ms with two and 18.6 ms with one (with the earlier
 // C++ loop for both widths, two had been slower: 16.5 against 10.1 ms).
-int level0_cells(const frep_batch* b) { return b->plan4.interval_ki; }
+// A set so small that its root items at one cell per lane all run at once
+// on the persistent grid (a serving step of a few trees) takes one: each
+// item is then shorter, and the pass lasts about one item.
+int level0_cells(const frep_batch* b) {
+    if (b->plan4.interval_ki < 2) return 1;
+    uint64_t items1 = 0;  // root items at one cell per lane
+    for (const frep_tree* t : b->trees) {
+        if (t->grid.levels < 2) continue;
+        const uint64_t d = t->grid.dims[0];
+        items1 += d * d * d / 32;
+    }
+    const uint64_t warps = (uint64_t)b->plan4.blocks * (uint64_t)b->plan4.warps_per_block;
+    return items1 <= warps ? 1 : 2;
+}
 
 // Enqueues the voxelization of every tree of the set: root copy + header
 // reset, then for each level index one interval pass and up to two point

@@ -20,6 +20,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <set>
 #include <thread>
 #include <unordered_map>
 #include <vector>
@@ -33,6 +34,10 @@ using frep::detail::fail;
 namespace {
 
 using Clock = std::chrono::steady_clock;
+
+double ms_since(Clock::time_point t) {
+    return std::chrono::duration<double, std::milli>(Clock::now() - t).count();
+}
 
 // First fit over one device allocation, with coalescing of free neighbours.
 class Arena {
@@ -57,7 +62,8 @@ class Arena {
         }
         return false;
     }
-    void release(uint64_t off, uint64_t bytes) {
+    // Returns the size of the free block that now holds [off, off + bytes).
+    uint64_t release(uint64_t off, uint64_t bytes) {
         bytes = align_up(bytes, 256);
         used_ -= bytes;
         auto it = free_.emplace(off, bytes).first;
@@ -71,8 +77,10 @@ class Arena {
             if (prev->first + prev->second == it->first) {
                 prev->second += it->second;
                 free_.erase(it);
+                return prev->second;
             }
         }
+        return it->second;
     }
     uint64_t used() const { return used_; }
     uint64_t capacity() const { return cap_; }
@@ -83,6 +91,7 @@ class Arena {
 };
 
 struct Scene {
+    uint64_t id = 0;  // index in frep_server::scenes
     frep_tape tape;
     frep_grid grid{};
     frep_voxelize_opts opts{};
@@ -147,6 +156,9 @@ struct frep_server {
     std::deque<uint64_t> pending;
     std::unordered_map<uint64_t, Request> requests;
     std::vector<std::unique_ptr<Scene>> scenes;
+    // resident scenes (a tree in the arena) by (last_used, id): the eviction
+    // order, found in O(log n) however many scenes are registered
+    std::set<std::pair<uint64_t, uint64_t>> lru;
     std::deque<Step> inflight;
     uint64_t next_request = 1, next_step = 1, tick = 0;
     bool stop = false;
@@ -155,6 +167,9 @@ struct frep_server {
 
     // statistics
     uint64_t submitted = 0, completed = 0, failed = 0, voxelized = 0, rerendered = 0, evictions = 0, steps = 0;
+    uint64_t max_step_evictions = 0;  // most evictions one step's planning made
+    double max_plan_ms = 0.0;         // longest planning of one step (the lock held)
+    double max_enqueue_ms = 0.0;      // longest host time to enqueue one step
     std::vector<double> latencies;
     bool window_open = false;
     Clock::time_point window_start, window_end;
@@ -179,12 +194,27 @@ void estimate_pools(Scene& S) {
     S.tape_words = std::max<uint64_t>(S.tape_words, S.tape.record.size() + 64);
 }
 
-void evict(frep_server* sv, Scene& S) {
+// Releases the scene's tree; returns the size of the free arena block that
+// now holds its memory.
+uint64_t drop_tree(frep_server* sv, Scene& S) {
+    sv->lru.erase({S.last_used, S.id});
     frep_tree_destroy(S.tree);
-    sv->arena.release(S.arena_off, S.arena_bytes);
+    const uint64_t merged = sv->arena.release(S.arena_off, S.arena_bytes);
     S.tree = nullptr;
     S.valid = false;
+    return merged;
+}
+
+uint64_t evict(frep_server* sv, Scene& S) {
     sv->evictions++;
+    return drop_tree(sv, S);
+}
+
+// Marks a scene used by the step being formed (its place in the LRU order).
+void touch(frep_server* sv, Scene& S) {
+    if (S.tree) sv->lru.erase({S.last_used, S.id});
+    S.last_used = sv->tick;
+    if (S.tree) sv->lru.insert({S.last_used, S.id});
 }
 
 // Places the scene's tree in the arena, evicting least recently used trees
@@ -193,12 +223,16 @@ bool admit(frep_server* sv, Scene& S, uint64_t step) {
     const uint64_t bytes = frep::detail::tree_external_bytes(S.node_words, S.tape_words);
     if (bytes > sv->arena.capacity()) return false;
     uint64_t off = 0;
-    while (!sv->arena.alloc(bytes, &off)) {
-        Scene* victim = nullptr;
-        for (auto& c : sv->scenes)
-            if (c->tree && c->step != step && (!victim || c->last_used < victim->last_used)) victim = c.get();
-        if (!victim) return false;
-        evict(sv, *victim);
+    // Evict least recently used trees until a free block holds the new one.
+    // Only the block an eviction grows can newly fit it, so first fit runs
+    // again only when that block is large enough. Trees of the step being
+    // formed carry the newest tick and come last in the order.
+    bool placed = sv->arena.alloc(bytes, &off);
+    while (!placed) {
+        auto it = sv->lru.begin();
+        while (it != sv->lru.end() && sv->scenes[it->second]->step == step) ++it;
+        if (it == sv->lru.end()) return false;
+        if (evict(sv, *sv->scenes[it->second]) >= align_up(bytes, 256)) placed = sv->arena.alloc(bytes, &off);
     }
     frep_voxelize_opts o = S.opts;
     o.node_words = S.node_words;
@@ -213,6 +247,7 @@ bool admit(frep_server* sv, Scene& S, uint64_t step) {
     S.arena_off = off;
     S.arena_bytes = bytes;
     S.valid = false;
+    sv->lru.insert({S.last_used, S.id});
     return true;
 }
 
@@ -294,9 +329,7 @@ bool plan_step(frep_server* sv, StepPlan* P) {
         Scene& S = *sv->scenes[R.req.scene];
         if (S.rebuild && S.tree && S.step != step_id) {
             // an overflowed voxelization: rebuild at the grown size
-            frep_tree_destroy(S.tree);
-            sv->arena.release(S.arena_off, S.arena_bytes);
-            S.tree = nullptr;
+            drop_tree(sv, S);
             S.rebuild = false;
         }
         const float t = R.req.tape_time;
@@ -338,7 +371,7 @@ bool plan_step(frep_server* sv, StepPlan* P) {
             R.voxelized = 1;
         }
         S.step = step_id;
-        S.last_used = sv->tick;
+        touch(sv, S);
         R.gen = S.gen;
         R.state = FREP_REQ_RUNNING;
         st.requests.push_back(rid);
@@ -431,7 +464,12 @@ void scheduler_main(frep_server* sv) {
         });
         if (sv->stop) break;
         StepPlan P;
-        if (!plan_step(sv, &P)) {
+        const auto plan_start = Clock::now();
+        const uint64_t ev_before = sv->evictions;
+        const bool planned = plan_step(sv, &P);
+        sv->max_plan_ms = std::max(sv->max_plan_ms, ms_since(plan_start));
+        sv->max_step_evictions = std::max(sv->max_step_evictions, sv->evictions - ev_before);
+        if (!planned) {
             // Nothing could be placed, although every tree outside the step
             // being formed may be evicted: the arena is exhausted for good.
             const auto now = Clock::now();
@@ -443,8 +481,11 @@ void scheduler_main(frep_server* sv) {
             continue;
         }
         lock.unlock();
+        const auto enqueue_start = Clock::now();
         const frep_status r = enqueue_step(sv, P);
+        const double enqueue_ms = ms_since(enqueue_start);
         lock.lock();
+        sv->max_enqueue_ms = std::max(sv->max_enqueue_ms, enqueue_ms);
         Step& st = P.step;
         if (r != FREP_OK) {
             // The step could not be enqueued: fail its requests, invalidate what it touched.
@@ -620,6 +661,7 @@ frep_status frep_server_add_scene(frep_server* sv, const frep_tape* tape, const 
     estimate_pools(*S);
     std::lock_guard<std::mutex> lock(sv->mu);
     *scene = sv->scenes.size();
+    S->id = *scene;
     sv->scenes.push_back(std::move(S));
     return FREP_OK;
 }
@@ -714,7 +756,7 @@ frep_status frep_server_get_stats(frep_server* sv, int reset, frep_server_stats*
     out->rerendered = sv->rerendered;
     out->evictions = sv->evictions;
     out->steps = sv->steps;
-    for (auto& S : sv->scenes) out->resident_trees += S->tree ? 1 : 0;
+    out->resident_trees = sv->lru.size();
     out->resident_bytes = sv->arena.used();
     out->arena_bytes = sv->arena.capacity();
     std::vector<double> l = sv->latencies;
@@ -736,9 +778,15 @@ frep_status frep_server_get_stats(frep_server* sv, int reset, frep_server_stats*
         const double span = std::chrono::duration<double>(sv->window_end - sv->window_start).count();
         out->scenes_per_s = span > 0.0 ? (double)sv->latencies.size() / span : 0.0;
     }
+    out->max_plan_ms = sv->max_plan_ms;
+    out->max_enqueue_ms = sv->max_enqueue_ms;
+    out->max_step_evictions = sv->max_step_evictions;
     if (reset) {
         sv->latencies.clear();
         sv->window_open = false;
+        sv->max_plan_ms = 0.0;
+        sv->max_enqueue_ms = 0.0;
+        sv->max_step_evictions = 0;
     }
     return FREP_OK;
 }

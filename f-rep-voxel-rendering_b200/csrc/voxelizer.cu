@@ -160,6 +160,53 @@ __device__ __forceinline__ void cell_xyz(uint32_t cell, uint32_t dim, uint32_t s
     }
 }
 
+// Work items of the interval passes are bricks: KI = 2 cells per lane take a
+// 4x4x4 brick of the node, KI = 1 a 2x4x4 one (x extent XS = 2 * KI), bricks
+// numbered z fastest. Lane l's h-th cell is brick cell i = 32h + l with
+// z = i & 3, y = (i >> 2) & 3, x = i >> 4: each 32-cell group is eight rows
+// of four cells along z (lanes 4r .. 4r + 3), and a row's four bits lie in
+// one mask word (dim is a multiple of 4, so a row starts on a 4-bit
+// boundary). A compact brick keeps the intervals of the item-level prepass
+// narrow, where a run of whole mask words would be a rod through the node.
+template <int KI>
+__device__ __forceinline__ void brick_origin(uint32_t grp, uint32_t dim, uint32_t sh, uint32_t* bx, uint32_t* by,
+                                             uint32_t* bz) {
+    constexpr uint32_t XS = 2 * KI;
+    if (sh != NOT_POW2) {
+        const uint32_t bs = sh - 2;  // log2(bricks along y and z)
+        *bz = (grp & ((1u << bs) - 1u)) * 4u;
+        *by = ((grp >> bs) & ((1u << bs) - 1u)) * 4u;
+        *bx = (grp >> (2 * bs)) * XS;
+    } else {
+        const uint32_t nb = dim / 4u;
+        *bz = grp % nb * 4u;
+        *by = grp / nb % nb * 4u;
+        *bx = grp / (nb * nb) * XS;
+    }
+}
+template <int KI>
+__device__ __forceinline__ uint32_t brick_cell(uint32_t bx, uint32_t by, uint32_t bz, uint32_t i, uint32_t dim,
+                                               uint32_t* cx, uint32_t* cy, uint32_t* cz) {
+    *cx = bx + (i >> 4);
+    *cy = by + ((i >> 2) & 3u);
+    *cz = bz + (i & 3u);
+    return (*cx * dim + *cy) * dim + *cz;
+}
+
+// ORs a 32-cell brick group's leaf and interior ballots into the node's mask
+// words: the first lane of each row of four issues one atomic per mask with
+// the row's four bits. The node's mask words start at zero (written when the
+// node was created).
+__device__ __forceinline__ void or_group_masks(uint32_t* leaf_words, uint32_t* interior_words, uint32_t cell,
+                                               uint32_t leaf_w, uint32_t interior_w, uint32_t lane) {
+    if ((lane & 3u) == 0u) {
+        const uint32_t w = cell >> 5, s = cell & 31u;
+        const uint32_t lf = (leaf_w >> lane) & 0xFu, in = (interior_w >> lane) & 0xFu;
+        if (lf) atomicOr(&leaf_words[w], lf << s);
+        if (in) atomicOr(&interior_words[w], in << s);
+    }
+}
+
 // What a level pass needs of one tree, read from its header when a warp
 // moves on to that tree.
 struct LevelTree {
@@ -168,6 +215,7 @@ struct LevelTree {
     uint64_t* tapes;
     unsigned long long tape_cap, ofs_l, ofs_next, child_cap;
     uint32_t dim, dim_sh, node_size, node_size_next, shorten, share;
+    uint32_t next_mask_words;  // mask words a new child needs zeroed (its level is an interval level), else 0
     float cs, lx, ly, lz, tt;
 };
 
@@ -193,10 +241,13 @@ __device__ __forceinline__ LevelTree load_tree(TreeHeader* H, uint32_t L, bool p
         t.ofs_next = H->node_ofs[L + 1];  // written by the scan kernel
         const unsigned long long cap = H->node_cap;
         t.child_cap = cap > t.ofs_next ? (cap - t.ofs_next) / t.node_size_next : 0ull;
+        const uint32_t dn = H->dims[L + 1];
+        t.next_mask_words = L + 2 < H->levels ? dn * dn * dn / 16u : 0u;
     } else {
         t.node_size_next = 1;
         t.ofs_next = 0;
         t.child_cap = 0;
+        t.next_mask_words = 0;
     }
     return t;
 }
@@ -502,20 +553,10 @@ __device__ __noinline__ uint32_t prepare_items(const uint64_t* tape, uint32_t n,
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t dim = T.dim, ncx = T.ncx, ncy = T.ncy, ncz = T.ncz;
     const bool valid = lane < g;
-    // the item's cells are 32 * KI consecutive bit indices: their bounding box
-    const uint32_t c0 = (grp + (valid ? lane : 0u)) * 32u * KI, c1 = c0 + 32u * KI - 1u;
-    uint32_t x0, y0, z0, x1, y1, z1;
-    cell_xyz(c0, dim, T.dim_sh, &x0, &y0, &z0);
-    cell_xyz(c1, dim, T.dim_sh, &x1, &y1, &z1);
-    if (x0 != x1) {
-        y0 = 0;
-        y1 = dim - 1;
-        z0 = 0;
-        z1 = dim - 1;
-    } else if (y0 != y1) {
-        z0 = 0;
-        z1 = dim - 1;
-    }
+    // the item is a brick (brick_origin): its cells' bounding box
+    uint32_t x0, y0, z0;
+    brick_origin<KI>(grp + (valid ? lane : 0u), dim, T.dim_sh, &x0, &y0, &z0);
+    const uint32_t x1 = x0 + 2u * KI - 1u, y1 = y0 + 3u, z1 = z0 + 3u;
     // the cells' own box formula (voxelizer/main.comp:113-126), so the item box
     // contains each of them exactly
     const float cs = T.cs;
@@ -717,6 +758,20 @@ interval_level_kernel(LevelLaunch p) {
             const uint32_t n_node = (uint32_t)__ldcg(&T.tapes[tape_idx]);
             uint32_t n = n_node;  // length of the tape the cells run (the item's, when pruned)
             const float cs = T.cs;
+            // the item's brick: this lane's cells, their bit indices in the node
+            uint32_t cell[KI], gx[KI], gy[KI], gz[KI];
+            {
+                uint32_t ox, oy, oz;
+                brick_origin<KI>(grp, dim, T.dim_sh, &ox, &oy, &oz);
+#pragma unroll
+                for (int h = 0; h < KI; h++) {
+                    uint32_t cx, cy, cz;
+                    cell[h] = brick_cell<KI>(ox, oy, oz, h * 32u + lane, dim, &cx, &cy, &cz);
+                    gx[h] = ncx * dim + cx;
+                    gy[h] = ncy * dim + cy;
+                    gz[h] = ncz * dim + cz;
+                }
+            }
 
             if constexpr (ROUND < 2) {
                 if (items && 32u * KI < dim * dim * dim) {
@@ -738,11 +793,8 @@ interval_level_kernel(LevelLaunch p) {
                     } else if (mode >= 2) {  // every cell empty (2) or a leaf (3): no evaluation
 #pragma unroll
                         for (int h = 0; h < KI; h++) {
-                            rec[4 + 2 * words + grp * 32 * KI + h * 32 + lane] = 0xFFFFFFFFu;
-                            if (lane == 0) {
-                                rec[4 + grp * KI + h] = mode == 3 ? 0xFFFFFFFFu : 0u;
-                                rec[4 + words + grp * KI + h] = 0u;
-                            }
+                            rec[4 + 2 * words + cell[h]] = 0xFFFFFFFFu;
+                            if (mode == 3) or_group_masks(rec + 4, rec + 4 + words, cell[h], 0xFFFFFFFFu, 0u, lane);
                         }
                         stat_work += 32ull * KI * n_node;
                         continue;
@@ -750,16 +802,9 @@ interval_level_kernel(LevelLaunch p) {
                 }
             }
 
-            uint32_t cell[KI], gx[KI], gy[KI], gz[KI];
             IVK<KI> bx, by, bz, bt;
 #pragma unroll
             for (int h = 0; h < KI; h++) {
-                cell[h] = grp * 32 * KI + h * 32 + lane;
-                uint32_t cx, cy, cz;
-                cell_xyz(cell[h], dim, T.dim_sh, &cx, &cy, &cz);
-                gx[h] = ncx * dim + cx;
-                gy[h] = ncy * dim + cy;
-                gz[h] = ncz * dim + cz;
                 // voxelizer/main.comp:113-116, :124-126
                 const float lox = __fadd_rn(T.lx, __fmul_rn((float)gx[h], cs));
                 const float loy = __fadd_rn(T.ly, __fmul_rn((float)gy[h], cs));
@@ -892,6 +937,18 @@ interval_level_kernel(LevelLaunch p) {
             if (n_amb) {
                 if (lane == 0) child_base = atomicAdd(&T.H->node_count[L + 1], n_amb);
                 child_base = __shfl_sync(0xFFFFFFFFu, child_base, 0);
+                // The children (ids child_base .. child_base + n_amb - 1, those
+                // below child_cap are created) of an interval level get their
+                // mask words zeroed here: their own pass ORs bricks into them.
+                if (T.next_mask_words) {
+                    const unsigned long long c_end = min(child_base + n_amb, T.child_cap);
+                    const uint32_t made = c_end > child_base ? (uint32_t)(c_end - child_base) : 0u;
+                    const uint32_t mw = T.next_mask_words;
+                    for (uint32_t k = lane; k < made * mw; k += 32) {
+                        const uint32_t c = k / mw;
+                        T.nodes[T.ofs_next + (child_base + c) * T.node_size_next + 4 + (k - c * mw)] = 0u;
+                    }
+                }
             }
             bool any_ok = false, lost = false;
 #pragma unroll
@@ -1216,10 +1273,7 @@ interval_level_kernel(LevelLaunch p) {
                     stat_max = max(stat_max, child_len[h]);
                 }
                 rec[4 + 2 * words + cell[h]] = ok[h] ? (uint32_t)my_child[h] : 0xFFFFFFFFu;
-                if (lane == 0) {
-                    rec[4 + grp * KI + h] = leaf_w[h];
-                    rec[4 + words + grp * KI + h] = ok_w[h];
-                }
+                or_group_masks(rec + 4, rec + 4 + words, cell[h], leaf_w[h], ok_w[h], lane);
             }
         }
     }
@@ -1518,6 +1572,15 @@ level_scan_kernel(TreeHeader* const* trees, uint32_t n, uint32_t L, int point, i
     if (t == 0) *cursor = 0ull;
 }
 
+// A root at an interval level (more than one level) starts with zeroed mask
+// words: the level pass ORs its bricks into them.
+__device__ __forceinline__ void zero_root_masks(TreeHeader* H, uint32_t t, uint32_t nt) {
+    if (H->levels < 2) return;
+    const uint32_t d = H->dims[0];
+    const uint32_t mw = d * d * d / 16u;
+    for (uint32_t w = t; w < mw; w += nt) H->nodes[4 + w] = 0u;
+}
+
 // Resets the headers and writes the root nodes (Voxelizer::Voxelize sets
 // interiorNodeCount[0] = 1 and relies on a zeroed root, voxelizer.cpp:432-435).
 // One block per tree; each tree's root tape is already at word 0 of its pool.
@@ -1546,6 +1609,7 @@ __global__ void tree_init_kernel(TreeHeader* const* trees, uint32_t n, const flo
             root[2] = 0;
             root[3] = 0;
         }
+        zero_root_masks(H, t, blockDim.x);
     }
 }
 
@@ -1582,6 +1646,7 @@ __global__ void tree_init_staged_kernel(TreeHeader* const* trees, uint32_t n, co
             root[2] = 0;
             root[3] = 0;
         }
+        zero_root_masks(H, t, blockDim.x);
         __syncthreads();
     }
 }

@@ -90,7 +90,9 @@ class ServerStats(C.Structure):
     _fields_ = [(k, C.c_uint64) for k in ("submitted", "completed", "failed", "voxelized", "rerendered",
                                           "evictions", "steps", "resident_trees", "resident_bytes",
                                           "arena_bytes")] + \
-               [(k, C.c_double) for k in ("p50_ms", "p99_ms", "mean_ms", "max_ms", "scenes_per_s")]
+               [(k, C.c_double) for k in ("p50_ms", "p99_ms", "mean_ms", "max_ms", "scenes_per_s",
+                                          "max_plan_ms", "max_enqueue_ms")] + \
+               [("max_step_evictions", C.c_uint64)]
 
 
 class LightsStruct(C.Structure):

@@ -662,6 +662,11 @@ typedef struct frep_server_stats {
     uint64_t resident_trees, resident_bytes, arena_bytes;
     double p50_ms, p99_ms, mean_ms, max_ms;  /* latency of requests completed since the last reset */
     double scenes_per_s;      /* completed / (last completion - first submit), since the reset  */
+    /* Since the last reset: the longest time the scheduler held the server's
+     * lock to form one step (submits wait for it), the longest host time to
+     * enqueue one step, and the most trees evicted while forming one step. */
+    double max_plan_ms, max_enqueue_ms;
+    uint64_t max_step_evictions;
 } frep_server_stats;
 
 /* lights: used for every request (NULL = frep_lights_default). */

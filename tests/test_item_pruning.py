@@ -1,7 +1,8 @@
 """Exactness of item-level pruning, on the CPU oracle.
 
 Below the root, the device's interval passes evaluate a node's tape once over
-the bounding box of each work item (32 * KI consecutive cells of the node)
+the bounding box of each work item (a 4x4x4 brick of the node's cells, 2x4x4
+with one cell per lane)
 and, when the tape is algebraic (no SIN / COS / EXP) and every interval of
 that evaluation is finite, let the item's cells run the node tape shortened
 over the item box; an item box that is empty or inside decides its cells
@@ -50,20 +51,20 @@ def _scene(name):
     return scenes.Scene(name, shape, [8, 8, 4], (-1, -1, -1), 2.0, cam, 64, 48)
 
 
-def _item_box(low, cs, node_xyz, dim, c0, c1):
-    """The kernel's item box: the cells' own box formula at the item's
-    smallest and largest coordinates (full y / z ranges where the item's
-    cells span several x planes / y rows)."""
-    def xyz(c):
-        return c // (dim * dim), (c // dim) % dim, c % dim
-    x0, y0, z0 = xyz(c0)
-    x1, y1, z1 = xyz(c1)
-    if x0 != x1:
-        y0, y1, z0, z1 = 0, dim - 1, 0, dim - 1
-    elif y0 != y1:
-        z0, z1 = 0, dim - 1
-    g0 = np.array(node_xyz) * dim + np.array([x0, y0, z0])
-    g1 = np.array(node_xyz) * dim + np.array([x1, y1, z1])
+def _brick_cells(dim, item, xs=4):
+    """The kernel's work item `item` of a node (bricks numbered z fastest,
+    x extent xs): its cells' (x, y, z) in the node, brick cell order."""
+    nb = dim // 4
+    ox, oy, oz = item // (nb * nb) * xs, item // nb % nb * 4, item % nb * 4
+    return [(ox + (i >> 4), oy + ((i >> 2) & 3), oz + (i & 3)) for i in range(16 * xs)]
+
+
+def _item_box(low, cs, node_xyz, dim, cells):
+    """The kernel's item box: the cells' own box formula at the brick's
+    smallest and largest coordinates."""
+    c = np.array(cells)
+    g0 = np.array(node_xyz) * dim + c.min(axis=0)
+    g1 = np.array(node_xyz) * dim + c.max(axis=0)
     lo = np.array([F32(F32(low[k]) + F32(F32(g0[k]) * cs)) for k in range(3)], F32)
     hi = np.array([F32(F32(F32(low[k]) + F32(F32(g1[k]) * cs)) + cs) for k in range(3)], F32)
     return lo, hi
@@ -113,8 +114,8 @@ def _check_scene(sc, rounding, cells_per_item=64, nodes_per_level=6, items_per_n
             node_xyz = [int(v) for v in rec[1:4]]
             for item in rng.choice(n_items, size=min(n_items, items_per_node), replace=False):
                 stats["items"] += 1
-                c0 = int(item) * cells_per_item
-                lo, hi = _item_box(sc.low_vertex, cs, node_xyz, dim, c0, c0 + cells_per_item - 1)
+                cells = _brick_cells(dim, int(item), xs=cells_per_item // 16)
+                lo, hi = _item_box(sc.low_vertex, cs, node_xyz, dim, cells)
                 trace = oracle.eval_interval_trace(node_tape, ns, lo, hi, 0.0, rounding)
                 ops = node_tape & np.uint64(0xFF)
                 if np.isin(ops, (OP_SIN, OP_COS, OP_EXP)).any() or not np.isfinite(trace).all():
@@ -125,8 +126,8 @@ def _check_scene(sc, rounding, cells_per_item=64, nodes_per_level=6, items_per_n
                 decided = iv_item[0] > 0 or iv_item[1] < 0
                 stats["decided"] += int(decided)
                 stats["pruned"] += int(not decided and len(item_tape) < n_node)
-                for c in range(c0, c0 + cells_per_item):
-                    g = np.array(node_xyz) * dim + np.array([c // (dim * dim), (c // dim) % dim, c % dim])
+                for c in cells:
+                    g = np.array(node_xyz) * dim + np.array(c)
                     clo, chi = _cell_box(sc.low_vertex, cs, g)
                     iv_n, ch_n = oracle.eval_interval(node_tape, ns, clo, chi, 0.0, rounding)
                     stats["cells"] += 1
