@@ -563,8 +563,8 @@ def cpu_sample_order(n: int):
 # dram__bytes_read.sum + dram__bytes_write.sum (one pass per launch) of
 #   python bench.py --steps 2 --warmup 3 --no-cpu-baseline --serve-seconds 0 --serve-sweep '' --plain-steps 1
 # summarised in profiles/batch_512scenes_dram_per_launch.txt.
-NCU_DRAM_BYTES_512 = {(0, 0): 7.851e9, (1, 0): 23.974e9, (1, 1): 1.222e9, (1, 2): 0.514e9,
-                      (2, 1): 0.377e9, (2, 2): 13.204e9}
+NCU_DRAM_BYTES_512 = {(0, 0): 9.666e9, (1, 0): 18.210e9, (1, 1): 1.195e9, (1, 2): 0.513e9,
+                      (2, 1): 0.337e9, (2, 2): 11.455e9}
 
 
 def tuning_table():

@@ -106,15 +106,13 @@ struct Sample {
     std::vector<uint32_t> ks;
 };
 
-// Device ms per scene of batched voxelize + render of `s` (graph replay): the
-// median of `reps` timed runs after one captured run.
-frep_status time_sample(frep_ctx* ctx, const Sample& s, const frep_lights* lights, uint32_t iw, uint32_t pw,
-                        uint32_t reps, uint32_t W, uint32_t H, float margin_pools, float* ms_out) {
+// One timing of `s` with the given pools; `overflowed[i]` = tree i's
+// overflow flags (1 nodes, 2 tapes) when the result is FREP_ERR_CAPACITY.
+frep_status time_sample_with(frep_ctx* ctx, const Sample& s, const frep_lights* lights, uint32_t iw, uint32_t pw,
+                             uint32_t reps, uint32_t W, uint32_t H, const std::vector<uint64_t>& nw,
+                             const std::vector<uint64_t>& tw, std::vector<uint32_t>* overflowed, float* ms_out) {
     const uint32_t n = (uint32_t)s.tapes.size();
-    std::vector<uint64_t> nw(n), tw(n);
-    frep_status st = frep_fit_pools(ctx, s.tapes.data(), s.grids.data(), nullptr, n, margin_pools, nw.data(),
-                                    tw.data());
-    if (st != FREP_OK) return st;
+    frep_status st = FREP_OK;
     Trial tr;
     for (uint32_t i = 0; i < n; i++) {
         frep_voxelize_opts o{};
@@ -161,14 +159,42 @@ frep_status time_sample(frep_ctx* ctx, const Sample& s, const frep_lights* light
         FREP_CUDA(cudaEventElapsedTime(&ms, tr.ev[0], tr.ev[1]));
         runs.push_back(ms);
     }
-    for (frep_tree* t : tr.trees) {
+    overflowed->assign(n, 0u);
+    frep_status worst = FREP_OK;
+    for (uint32_t i = 0; i < n; i++) {
         frep_tree_info info{};
-        st = frep_tree_sync(t, &info);
-        if (st != FREP_OK) return st;  // a pool that overflowed would time a partial tree
+        st = frep_tree_sync(tr.trees[i], &info);
+        if (st == FREP_ERR_CAPACITY) (*overflowed)[i] = info.overflow;
+        else if (st != FREP_OK) return st;
+        if (st != FREP_OK) worst = st;  // a pool that overflowed would time a partial tree
     }
+    if (worst != FREP_OK) return worst;
     std::sort(runs.begin(), runs.end());
     *ms_out = runs[runs.size() / 2] / (float)n;
     return FREP_OK;
+}
+
+// Device ms per scene of batched voxelize + render of `s` (graph replay): the
+// median of `reps` timed runs after one captured run. Pools are fitted from
+// one voxelization of each scene alone plus `margin_pools`; a tree whose
+// pool still overflows in the batched run gets that pool doubled and the
+// sample is timed again (at most 4 times).
+frep_status time_sample(frep_ctx* ctx, const Sample& s, const frep_lights* lights, uint32_t iw, uint32_t pw,
+                        uint32_t reps, uint32_t W, uint32_t H, float margin_pools, float* ms_out) {
+    const uint32_t n = (uint32_t)s.tapes.size();
+    std::vector<uint64_t> nw(n), tw(n);
+    frep_status st = frep_fit_pools(ctx, s.tapes.data(), s.grids.data(), nullptr, n, margin_pools, nw.data(),
+                                    tw.data());
+    if (st != FREP_OK) return st;
+    std::vector<uint32_t> over;
+    for (int attempt = 0;; attempt++) {
+        st = time_sample_with(ctx, s, lights, iw, pw, reps, W, H, nw, tw, &over, ms_out);
+        if (st != FREP_ERR_CAPACITY || attempt == 4) return st;
+        for (uint32_t i = 0; i < n; i++) {
+            if (over[i] & 1u) nw[i] *= 2;
+            if (over[i] & 2u) tw[i] *= 2;
+        }
+    }
 }
 
 // ---- JSON of the tuning cache (the fixed schema frep/autotune.py writes) ----

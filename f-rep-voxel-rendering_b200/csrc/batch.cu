@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstring>
 #include <vector>
 
@@ -70,6 +71,12 @@ struct frep_batch {
     uint32_t profiled_levels = 0;
     cudaEvent_t ev[2 + 3 * FREP_MAX_LEVELS] = {};
     cudaEvent_t rev[2] = {};
+    // pinned halves of upload areas that grew, freed at destruction
+    std::vector<void*> retired_host;
+    // host time of the last voxelize call, ms: plans + prefix + scratch
+    // (growing them waits for the device), the upload area (waiting for its
+    // previous use, growing it), staging + launches
+    double host_ms[3] = {};
     // what the last call enqueued
     uint64_t last_upload = 0;
     uint32_t last_launches = 0;
@@ -105,8 +112,13 @@ Layout make_layout(uint32_t n, uint32_t nf, const frep_tape* const* tapes) {
 }
 
 // Takes the next upload area, waiting until the call that used it last is
-// done with it on the device, and grows it to `bytes`.
-frep_status acquire_area(frep_batch* b, size_t bytes, int* which) {
+// done with it on the device, and grows it to `bytes`. Growing waits for
+// nothing else: the device half is released and allocated in stream order
+// (cudaFreeAsync / cudaMallocAsync on `s`; its last use is complete), and the
+// pinned host half is kept until the batch is destroyed (freeing pinned
+// memory waits for the whole device: in a serving loop that stalled a step's
+// enqueue behind the step before it, up to half a second).
+frep_status acquire_area(frep_batch* b, size_t bytes, int* which, cudaStream_t s) {
     const int i = b->next_area;
     UploadArea& A = b->area[i];
     if (A.pending) {
@@ -120,8 +132,8 @@ frep_status acquire_area(frep_batch* b, size_t bytes, int* which) {
             A.graph = nullptr;
             A.graph_key.clear();
         }
-        if (A.h) cudaFreeHost(A.h);
-        if (A.d) cudaFree(A.d);
+        if (A.h) b->retired_host.push_back(A.h);
+        if (A.d) FREP_CUDA(cudaFreeAsync(A.d, s));
         b->ctx->used -= std::min<uint64_t>(b->ctx->used, A.bytes);
         b->bytes -= std::min<uint64_t>(b->bytes, A.bytes);
         A.h = nullptr;
@@ -131,7 +143,7 @@ frep_status acquire_area(frep_batch* b, size_t bytes, int* which) {
         const size_t cap = align_up(std::max(bytes + bytes / 4, 2 * prev), 4096);
         if (b->ctx->used + cap > b->ctx->budget) return fail(FREP_ERR_OOM, "frep_batch: upload area exceeds the budget");
         FREP_CUDA(cudaMallocHost(&A.h, cap));
-        FREP_CUDA(cudaMalloc(&A.d, cap));
+        FREP_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&A.d), cap, s));
         A.bytes = cap;
         b->bytes += cap;
         b->ctx->used += cap;
@@ -226,6 +238,8 @@ frep_status ensure_plans(frep_batch* b, const TapeStats& st) {
     return FREP_OK;
 }
 
+frep::WarpScratch batch_scratch(const frep_batch* b, const TapeStats& st);
+
 // Plans, work prefix and scratch for voxelizing the current tree set.
 frep_status prepare_voxelize(frep_batch* b, const frep_tape* const* tapes, TapeStats* st) {
     frep_status r = check_tapes(b, tapes, st);
@@ -234,7 +248,7 @@ frep_status prepare_voxelize(frep_batch* b, const frep_tape* const* tapes, TapeS
     if (r == FREP_OK)
         r = ensure_keep(b, (uint64_t)std::max(b->plan4.blocks * b->plan4.warps_per_block,
                                               b->plan2.blocks * b->plan2.warps_per_block) *
-                               frep::warp_scratch(st->longest, st->mm, (uint32_t)b->plan4.interval_ki, b->rounding != 2).stride);
+                               batch_scratch(b, *st).stride);
     return r;
 }
 
@@ -258,6 +272,11 @@ int level0_cells(const frep_batch* b) {
     return items1 <= warps ? 1 : 2;
 }
 
+// The interval passes' per-warp scratch for the current set.
+frep::WarpScratch batch_scratch(const frep_batch* b, const TapeStats& st) {
+    return frep::warp_scratch(st.longest, st.mm, (uint32_t)b->plan4.interval_ki, b->rounding != 2);
+}
+
 // Enqueues the voxelization of every tree of the set: root copy + header
 // reset, then for each level index one interval pass and up to two point
 // passes, each a single launch over the whole set. The level passes walk the
@@ -279,7 +298,7 @@ frep_status enqueue_voxelize(frep_batch* b, const uint8_t* d_area, const TapeSta
     a.cursor = b->d_cursor;
     a.n_trees = n;
     a.keep_scratch = b->keep;
-    const frep::WarpScratch ws = frep::warp_scratch(st.longest, st.mm, (uint32_t)b->plan4.interval_ki, b->rounding != 2);
+    const frep::WarpScratch ws = batch_scratch(b, st);
     a.keep_stride = ws.stride;
     a.mm_ofs = ws.mm_ofs;
     a.item_ofs = ws.item_ofs;
@@ -402,6 +421,14 @@ frep_status check_trees(frep_ctx* ctx, frep_tree* const* trees, uint32_t n, int*
 
 }  // namespace
 
+namespace frep {
+namespace detail {
+void batch_host_ms(const frep_batch* b, double out[3]) {
+    for (int i = 0; i < 3; i++) out[i] = b ? b->host_ms[i] : 0.0;
+}
+}  // namespace detail
+}  // namespace frep
+
 extern "C" {
 
 frep_status frep_batch_create(frep_ctx* ctx, frep_tree* const* trees, uint32_t n, frep_batch** out) {
@@ -439,6 +466,7 @@ void frep_batch_destroy(frep_batch* b) {
         if (A.d) cudaFree(A.d);
         if (A.done) cudaEventDestroy(A.done);
     }
+    for (void* h : b->retired_host) cudaFreeHost(h);
     cudaFree(b->d_prefix);
     cudaFree(b->keep);
     if (b->capture_stream) cudaStreamDestroy(b->capture_stream);
@@ -469,19 +497,30 @@ frep_status frep_batch_voxelize(frep_batch* b, const frep_tape* const* tapes, co
     FREP_CUDA(cudaSetDevice(b->ctx->device));
     cudaStream_t s = (cudaStream_t)stream_ptr;
     TapeStats st;
+    const auto t0 = std::chrono::steady_clock::now();
     frep_status r = prepare_voxelize(b, tapes, &st);
     if (r != FREP_OK) return r;
+    const auto t1 = std::chrono::steady_clock::now();
     const Layout L = make_layout((uint32_t)b->trees.size(), 0, tapes);
     int ai = 0;
-    r = acquire_area(b, L.total, &ai);
+    r = acquire_area(b, L.total, &ai, s);
     if (r != FREP_OK) return r;
+    const auto t2 = std::chrono::steady_clock::now();
     UploadArea& A = b->area[ai];
     stage_inputs(b, A.h, tapes, tape_times, L);
     FREP_CUDA(cudaMemcpyAsync(A.d, A.h, L.total, cudaMemcpyHostToDevice, s));
     r = enqueue_voxelize(b, A.d, st, L, s, b->profile);
     if (r != FREP_OK) return r;
     mark_voxelized(b, tapes, s);
-    return release_area(b, ai, s);
+    r = release_area(b, ai, s);
+    const auto t3 = std::chrono::steady_clock::now();
+    auto ms = [](std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point c) {
+        return std::chrono::duration<double, std::milli>(c - a).count();
+    };
+    b->host_ms[0] = ms(t0, t1);
+    b->host_ms[1] = ms(t1, t2);
+    b->host_ms[2] = ms(t2, t3);
+    return r;
 }
 
 frep_status frep_batch_render_frames(frep_batch* b, const frep_tree* const* frame_trees, uint32_t n_frames,
@@ -497,7 +536,7 @@ frep_status frep_batch_render_frames(frep_batch* b, const frep_tree* const* fram
     cudaStream_t s = (cudaStream_t)stream_ptr;
     const Layout L = make_layout(0, n_frames, nullptr);
     int ai = 0;
-    frep_status r = acquire_area(b, L.total, &ai);
+    frep_status r = acquire_area(b, L.total, &ai, s);
     if (r != FREP_OK) return r;
     UploadArea& A = b->area[ai];
     FrameDims fd;
@@ -533,7 +572,7 @@ frep_status frep_batch_run(frep_batch* b, const frep_tape* const* tapes, const f
     if (r != FREP_OK) return r;
     const Layout L = make_layout(n, n, tapes);
     int ai = 0;
-    r = acquire_area(b, L.total, &ai);
+    r = acquire_area(b, L.total, &ai, s);
     if (r != FREP_OK) return r;
     UploadArea& A = b->area[ai];
     // Fill the whole upload area (the graph's copy node reads it when it
@@ -588,6 +627,7 @@ frep_status frep_batch_get_info(const frep_batch* b, frep_batch_info* info) {
     info->device_bytes = b->bytes;
     info->interval_warps_per_block = b->plan_valid ? (uint32_t)b->plan4.warps_per_block : 0;
     info->point_warps_per_block = b->plan_valid ? (uint32_t)b->plan4.point_warps_per_block : 0;
+    info->root_cells_per_lane = b->plan_valid ? (uint32_t)level0_cells(b) : 0;
     return FREP_OK;
 }
 

@@ -44,6 +44,9 @@ frep_status fill_render_args(const frep_tree* tree, const frep_camera* cam, cons
 // The frame part alone (camera basis, lights, outputs): resets *args first.
 frep_status fill_view_args(const frep_camera* cam, const frep_lights* lights, float tape_time,
                            const frep_image* out, RenderArgs* args);
+// Host time of a batch's last frep_batch_voxelize, ms: plans, prefix and
+// scratch; the upload area; staging and launches.
+void batch_host_ms(const frep_batch* b, double out[3]);
 }  // namespace detail
 }  // namespace frep
 

@@ -15,6 +15,8 @@
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -170,6 +172,7 @@ struct frep_server {
     uint64_t max_step_evictions = 0;  // most evictions one step's planning made
     double max_plan_ms = 0.0;         // longest planning of one step (the lock held)
     double max_enqueue_ms = 0.0;      // longest host time to enqueue one step
+    double slow_ms = 0.0;             // FREP_SERVER_SLOW_MS: log steps slower to enqueue (0 = off)
     std::vector<double> latencies;
     bool window_open = false;
     Clock::time_point window_start, window_end;
@@ -251,16 +254,24 @@ bool admit(frep_server* sv, Scene& S, uint64_t step) {
     return true;
 }
 
-frep_status ensure_frames(frep_server* sv, uint64_t bytes) {
+// Grows the frame area in stream order: the old area is released after the
+// steps already enqueued on the server's stream (cudaFreeAsync) and the new
+// one allocated on that stream, so a growth waits for no step (a cudaFree here
+// waited for the whole device: up to 280 ms at 2000 requests/s). The first
+// area holds max_batch frames of the step's largest frame (at most 1 GB), so
+// that later steps of that frame size never grow it (a growth in the middle
+// of a serving run still took 288 ms to allocate at 2000 requests/s).
+frep_status ensure_frames(frep_server* sv, uint64_t bytes, uint64_t largest_frame) {
     if (bytes <= sv->frames_bytes) return FREP_OK;
     const uint64_t prev = sv->frames_bytes;
-    FREP_CUDA(cudaStreamSynchronize(sv->stream));
-    cudaFree(sv->d_frames);
+    if (sv->d_frames) FREP_CUDA(cudaFreeAsync(sv->d_frames, sv->stream));
     sv->d_frames = nullptr;
     sv->frames_bytes = 0;
-    // (growing waits for the stream: at least double)
-    const uint64_t cap = align_up(std::max<uint64_t>(bytes + bytes / 4, 2 * prev), 1 << 20);
-    FREP_CUDA(cudaMalloc(&sv->d_frames, cap));
+    // at least double, and at least max_batch of the largest frame (up to 1 GB)
+    const uint64_t presize = std::min<uint64_t>((uint64_t)sv->cfg.max_batch * largest_frame, 1ull << 30);
+    const uint64_t cap = align_up(std::max<uint64_t>(std::max<uint64_t>(bytes + bytes / 4, 2 * prev), presize),
+                                  1 << 20);
+    FREP_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&sv->d_frames), cap, sv->stream));
     sv->frames_bytes = cap;
     return FREP_OK;
 }
@@ -397,10 +408,15 @@ frep_status enqueue_step(frep_server* sv, StepPlan& P) {
     frep_status r = FREP_OK;
     cudaStream_t s = sv->stream;
     Step& st = P.step;
+    // phase marks for the slow-step log (FREP_SERVER_SLOW_MS)
+    Clock::time_point mark[6];
+    double vox_ms[3] = {};
+    mark[0] = Clock::now();
     // headers of the trees admitted while the step was planned (under the
     // lock, where nothing is enqueued: a launch can wait for queue space)
     for (frep_tree* t : P.vtrees)
         if (r == FREP_OK) r = frep::detail::write_tree_header(t, s);
+    mark[1] = Clock::now();
     if (r == FREP_OK && !P.vtrees.empty()) {
         if (!sv->batch) {
             r = frep_batch_create(sv->ctx, P.vtrees.data(), (uint32_t)P.vtrees.size(), &sv->batch);
@@ -410,16 +426,21 @@ frep_status enqueue_step(frep_server* sv, StepPlan& P) {
             r = frep_batch_set_trees(sv->batch, P.vtrees.data(), (uint32_t)P.vtrees.size());
         }
         if (r == FREP_OK) r = frep_batch_voxelize(sv->batch, P.vtapes.data(), P.vtimes.data(), s);
+        frep::detail::batch_host_ms(sv->batch, vox_ms);
     }
+    mark[2] = Clock::now();
     const uint32_t nf = (uint32_t)P.cams.size();
     std::vector<frep_image> imgs(nf);
     std::vector<uint64_t> ofs(nf);
-    uint64_t total = 0;
+    uint64_t total = 0, largest = 0;
     for (uint32_t i = 0; i < nf; i++) {
         ofs[i] = total;
-        total += align_up((uint64_t)P.cams[i].width * P.cams[i].height * 4, 256);
+        const uint64_t fb = align_up((uint64_t)P.cams[i].width * P.cams[i].height * 4, 256);
+        total += fb;
+        largest = std::max(largest, fb);
     }
-    if (r == FREP_OK) r = ensure_frames(sv, total);
+    if (r == FREP_OK) r = ensure_frames(sv, total, largest);
+    mark[3] = Clock::now();
     if (r == FREP_OK && !sv->batch) r = fail(FREP_ERR_INVALID_ARG, "frep_server: no voxelized tree to render");
     if (r == FREP_OK) {
         for (uint32_t i = 0; i < nf; i++) {
@@ -429,6 +450,7 @@ frep_status enqueue_step(frep_server* sv, StepPlan& P) {
         r = frep_batch_render_frames(sv->batch, P.ftrees.data(), nf, P.cams.data(), &sv->lights, P.ftimes.data(),
                                      imgs.data(), s);
     }
+    mark[4] = Clock::now();
     // pool use of the voxelized trees, read back in the step
     if (r == FREP_OK) r = ensure_ring(sv, (uint32_t)P.vtrees.size());
     if (r == FREP_OK && !P.vtrees.empty()) {
@@ -451,6 +473,17 @@ frep_status enqueue_step(frep_server* sv, StepPlan& P) {
         cudaError_t e = cudaEventCreateWithFlags(&st.done, cudaEventDisableTiming | cudaEventBlockingSync);
         if (e == cudaSuccess) e = cudaEventRecord(st.done, s);
         if (e != cudaSuccess) r = cuda_fail(e, "frep_server: step event");
+    }
+    mark[5] = Clock::now();
+    if (sv->slow_ms > 0.0) {
+        auto d = [&](int a, int b) { return std::chrono::duration<double, std::milli>(mark[b] - mark[a]).count(); };
+        if (d(0, 5) >= sv->slow_ms)
+            std::fprintf(stderr,
+                         "frep_server: step %llu enqueued in %.1f ms: headers %.1f, voxelize %.1f (plans/scratch %.1f, "
+                         "upload area %.1f, staging/launches %.1f), frame area %.1f, render %.1f, read-backs %.1f; "
+                         "%zu trees, %u frames\n",
+                         (unsigned long long)st.id, d(0, 5), d(0, 1), d(1, 2), vox_ms[0], vox_ms[1], vox_ms[2],
+                         d(2, 3), d(3, 4), d(4, 5), P.vtrees.size(), nf);
     }
     return r;
 }
@@ -505,6 +538,9 @@ void scheduler_main(frep_server* sv) {
 void completer_main(frep_server* sv) {
     cudaSetDevice(sv->ctx->device);
     std::unique_lock<std::mutex> lock(sv->mu);
+    // the previous step's event, destroyed outside the lock (a CUDA call
+    // under the lock could make submits wait behind the driver)
+    cudaEvent_t spent = nullptr;
     while (true) {
         sv->cv_steps.wait(lock, [&] { return sv->stop || !sv->inflight.empty(); });
         if (sv->inflight.empty()) {
@@ -513,12 +549,14 @@ void completer_main(frep_server* sv) {
         }
         const cudaEvent_t ev = sv->inflight.front().done;
         lock.unlock();
+        if (spent) cudaEventDestroy(spent);
+        spent = nullptr;
         const cudaError_t e = cudaEventSynchronize(ev);
         const auto now = Clock::now();
         lock.lock();
         Step st = std::move(sv->inflight.front());
         sv->inflight.pop_front();
-        cudaEventDestroy(st.done);
+        spent = st.done;
         // Overflowed voxelizations: grow the scene's pools and run its
         // requests again (the tree is rebuilt at the new size).
         std::unordered_map<uint64_t, bool> overflowed;
@@ -567,6 +605,8 @@ void completer_main(frep_server* sv) {
         sv->cv_done.notify_all();
         sv->cv_work.notify_all();
     }
+    lock.unlock();
+    if (spent) cudaEventDestroy(spent);
 }
 
 }  // namespace
@@ -579,6 +619,7 @@ frep_status frep_server_create(frep_ctx* ctx, const frep_server_config* config, 
     FREP_CUDA(cudaSetDevice(ctx->device));
     auto sv = std::make_unique<frep_server>();
     sv->ctx = ctx;
+    if (const char* v = std::getenv("FREP_SERVER_SLOW_MS")) sv->slow_ms = std::atof(v);
     if (config) sv->cfg = *config;
     if (!sv->cfg.max_batch) sv->cfg.max_batch = 512;
     if (!sv->cfg.max_inflight) sv->cfg.max_inflight = 2;

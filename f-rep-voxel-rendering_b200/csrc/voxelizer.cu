@@ -723,6 +723,8 @@ interval_level_kernel(LevelLaunch p) {
     };
 
     // item pruning: the prepared group of items (one node, lanes = items)
+    // (not at level 0: with bricks, a batch's root level pruned per brick, a
+    // dozen bricks per fetch, took 74.7 ms against 43.0 ms without)
     uint64_t* items = nullptr;
     if constexpr (ROUND < 2)
         if (p.item_cap && L > 0) items = reinterpret_cast<uint64_t*>(keep + p.item_ofs);

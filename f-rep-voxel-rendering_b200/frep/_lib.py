@@ -47,7 +47,7 @@ class Grid(C.Structure):
 class BatchInfo(C.Structure):
     _fields_ = [("n_trees", C.c_uint32), ("voxelize_launches", C.c_uint32), ("upload_bytes", C.c_uint64),
                 ("device_bytes", C.c_uint64), ("interval_warps_per_block", C.c_uint32),
-                ("point_warps_per_block", C.c_uint32)]
+                ("point_warps_per_block", C.c_uint32), ("root_cells_per_lane", C.c_uint32)]
 
 
 class VoxelizeOpts(C.Structure):

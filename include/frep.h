@@ -529,6 +529,9 @@ typedef struct frep_batch_info {
     uint64_t device_bytes;             /* the batch's own scratch + upload area          */
     uint32_t interval_warps_per_block; /* the plan in use (0 before the first run)       */
     uint32_t point_warps_per_block;
+    /* cells per lane of the root level's pass for the current tree set: 2 when
+     * its root cells fill the grid, else 1 (0 before the first run) */
+    uint32_t root_cells_per_lane;
 } frep_batch_info;
 frep_status frep_batch_get_info(const frep_batch* batch, frep_batch_info* info);
 
@@ -628,6 +631,11 @@ frep_status frep_batch_timings(frep_batch* batch, float ms[3 * FREP_MAX_LEVELS +
  * frep_voxelize_opts when given, else estimated and then refitted from the
  * scene's measured use; a voxelization that overflows its pools is retried
  * with doubled pools (at most 4 times, then FREP_ERR_CAPACITY).
+ * Diagnostics: with the environment variable FREP_SERVER_SLOW_MS set to a
+ * number of milliseconds when the server is created, every step whose host
+ * enqueue takes at least that long prints one line to stderr with the time
+ * of each phase (tree headers, voxelization: plans and scratch, upload area,
+ * staging and launches; frame area, render, read-backs).
  * ------------------------------------------------------------------------- */
 
 typedef struct frep_server frep_server;

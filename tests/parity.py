@@ -170,7 +170,7 @@ def compare_trees_fast(a, b, max_report: int = 3):
             diffs.append(f"level {lvl}: node sets differ")
             continue
         for name, x, y in (("leaf", la, lb), ("interior", ia, ib), ("tape length", na, nb), ("tape", ha, hb)):
-            if x is None:
+            if x is None or len(x) == 0:  # (a level without nodes: nothing to compare)
                 continue
             bad = np.nonzero(np.any((x != y).reshape(len(x), -1), axis=1))[0]
             if len(bad):

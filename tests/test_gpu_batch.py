@@ -188,3 +188,33 @@ def test_set_trees_and_render_frames(ctx):
                                  exp.nodes)
         np.testing.assert_array_equal(cells, want[i][2])
     batch.close()
+
+
+def test_root_level_of_a_large_batch(ctx):
+    """A set whose root cells fill the grid (160 trees with 32^3 roots): the
+    root level runs two cells per lane over 4x4x4 bricks (batch info), and
+    every tree equals the same scene voxelized alone (one root: one cell per
+    lane, 2x4x4 bricks) and, for two of them, the oracle's."""
+    from parity import compare_trees_fast, oracle_tree
+    scs = [scenes.random_csg(10 + 7 * (i % 6), seed=500 + i, grid_dims=[32, 4]) for i in range(160)]
+    pools = dict(node_words=1 << 19, tape_words=1 << 21)  # 2 MB of nodes, 16 MB of tapes per tree
+    alone = []
+    for sc in scs:
+        vs = frep.VoxelStorage(sc.grid_dims, sc.low_vertex, sc.world_size, **pools).init(ctx, sc.shape)
+        frep.Voxelizer(ctx, vs).voxelize(0.0)
+        alone.append(vs.export())
+        vs.cleanup()
+    storages = [frep.VoxelStorage(sc.grid_dims, sc.low_vertex, sc.world_size, **pools).init(ctx, sc.shape)
+                for sc in scs]
+    batch = frep.Batch(ctx, storages)
+    for rep in range(2):  # the second run starts on the first one's scratch
+        batch.voxelize()
+        assert batch.info().root_cells_per_lane == 2
+        for i, vs in enumerate(storages):
+            assert compare_trees_fast(vs.export(), alone[i]) == [], f"tree {i} (run {rep})"
+    for i in (0, 5):
+        orc = oracle_tree(scs[i], frep.Tape(scs[i].shape))
+        assert compare_trees_fast(storages[i].export(), orc) == [], f"tree {i}"
+    batch.close()
+    for vs in storages:
+        vs.cleanup()
