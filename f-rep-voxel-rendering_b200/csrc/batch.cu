@@ -133,13 +133,14 @@ frep_status acquire_area(frep_batch* b, size_t bytes, int* which, cudaStream_t s
             A.graph_key.clear();
         }
         if (A.h) b->retired_host.push_back(A.h);
-        if (A.d) FREP_CUDA(cudaFreeAsync(A.d, s));
+        A.h = nullptr;
+        uint8_t* old_d = A.d;
+        A.d = nullptr;
         b->ctx->used -= std::min<uint64_t>(b->ctx->used, A.bytes);
         b->bytes -= std::min<uint64_t>(b->bytes, A.bytes);
-        A.h = nullptr;
-        A.d = nullptr;
         A.bytes = 0;
-        // (freeing waits for the device: grow at least twofold)
+        if (old_d) FREP_CUDA(cudaFreeAsync(old_d, s));
+        // (each growth costs allocations and a new graph capture: at least twofold)
         const size_t cap = align_up(std::max(bytes + bytes / 4, 2 * prev), 4096);
         if (b->ctx->used + cap > b->ctx->budget) return fail(FREP_ERR_OOM, "frep_batch: upload area exceeds the budget");
         FREP_CUDA(cudaMallocHost(&A.h, cap));

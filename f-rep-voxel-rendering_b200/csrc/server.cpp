@@ -27,11 +27,14 @@
 #include <unordered_map>
 #include <vector>
 
+#include "arena.h"
 #include "capi_internal.h"
 
 using frep::detail::align_up;
 using frep::detail::cuda_fail;
 using frep::detail::fail;
+using frep::serving::Arena;
+using frep::serving::LruOrder;
 
 namespace {
 
@@ -40,57 +43,6 @@ using Clock = std::chrono::steady_clock;
 double ms_since(Clock::time_point t) {
     return std::chrono::duration<double, std::milli>(Clock::now() - t).count();
 }
-
-// First fit over one device allocation, with coalescing of free neighbours.
-class Arena {
-   public:
-    void reset(uint64_t bytes) {
-        free_.clear();
-        free_[0] = bytes;
-        cap_ = bytes;
-        used_ = 0;
-    }
-    bool alloc(uint64_t bytes, uint64_t* off) {
-        bytes = align_up(bytes, 256);
-        for (auto it = free_.begin(); it != free_.end(); ++it) {
-            if (it->second < bytes) continue;
-            *off = it->first;
-            const uint64_t rest = it->second - bytes;
-            const uint64_t at = it->first + bytes;
-            free_.erase(it);
-            if (rest) free_[at] = rest;
-            used_ += bytes;
-            return true;
-        }
-        return false;
-    }
-    // Returns the size of the free block that now holds [off, off + bytes).
-    uint64_t release(uint64_t off, uint64_t bytes) {
-        bytes = align_up(bytes, 256);
-        used_ -= bytes;
-        auto it = free_.emplace(off, bytes).first;
-        auto next = std::next(it);
-        if (next != free_.end() && it->first + it->second == next->first) {
-            it->second += next->second;
-            free_.erase(next);
-        }
-        if (it != free_.begin()) {
-            auto prev = std::prev(it);
-            if (prev->first + prev->second == it->first) {
-                prev->second += it->second;
-                free_.erase(it);
-                return prev->second;
-            }
-        }
-        return it->second;
-    }
-    uint64_t used() const { return used_; }
-    uint64_t capacity() const { return cap_; }
-
-   private:
-    std::map<uint64_t, uint64_t> free_;  // offset -> bytes
-    uint64_t cap_ = 0, used_ = 0;
-};
 
 struct Scene {
     uint64_t id = 0;  // index in frep_server::scenes
@@ -160,7 +112,7 @@ struct frep_server {
     std::vector<std::unique_ptr<Scene>> scenes;
     // resident scenes (a tree in the arena) by (last_used, id): the eviction
     // order, found in O(log n) however many scenes are registered
-    std::set<std::pair<uint64_t, uint64_t>> lru;
+    LruOrder lru;
     std::deque<Step> inflight;
     uint64_t next_request = 1, next_step = 1, tick = 0;
     bool stop = false;
@@ -226,17 +178,12 @@ bool admit(frep_server* sv, Scene& S, uint64_t step) {
     const uint64_t bytes = frep::detail::tree_external_bytes(S.node_words, S.tape_words);
     if (bytes > sv->arena.capacity()) return false;
     uint64_t off = 0;
-    // Evict least recently used trees until a free block holds the new one.
-    // Only the block an eviction grows can newly fit it, so first fit runs
-    // again only when that block is large enough. Trees of the step being
-    // formed carry the newest tick and come last in the order.
-    bool placed = sv->arena.alloc(bytes, &off);
-    while (!placed) {
-        auto it = sv->lru.begin();
-        while (it != sv->lru.end() && sv->scenes[it->second]->step == step) ++it;
-        if (it == sv->lru.end()) return false;
-        if (evict(sv, *sv->scenes[it->second]) >= align_up(bytes, 256)) placed = sv->arena.alloc(bytes, &off);
-    }
+    // Evict least recently used trees (not those of the step being formed)
+    // until a free block holds the new one.
+    const bool placed = frep::serving::place_evicting(
+        sv->arena, sv->lru, bytes, [&](uint64_t id) { return sv->scenes[id]->step == step; },
+        [&](uint64_t id) { return evict(sv, *sv->scenes[id]); }, &off);
+    if (!placed) return false;
     frep_voxelize_opts o = S.opts;
     o.node_words = S.node_words;
     o.tape_words = S.tape_words;
